@@ -1,0 +1,29 @@
+import os
+import subprocess
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, os.path.join(ROOT, "dqmc-dev_b200"))
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")
+
+
+@pytest.fixture(scope="session", autouse=True)
+def _oracle_built():
+    """Build the CPU oracle once per session (it is a few seconds of gcc)."""
+    for lib in ("liboracle_r.so", "liboracle_c.so"):
+        if not os.path.exists(os.path.join(ROOT, "oracle", lib)):
+            subprocess.run(["make", "-C", os.path.join(ROOT, "oracle")], check=True,
+                           stdout=subprocess.DEVNULL)
+            break
+
+
+@pytest.fixture
+def golden():
+    return GOLDEN
