@@ -1,0 +1,327 @@
+"""Benchmark: batched DQMC chain-sweeps/s on one node.
+
+Workload (per GPU): 256 independent chains of the single-band Hubbard model
+on a 12x12 square lattice (N = 144), t = 1, U = 4, mu = -1, beta = 6,
+dtau = 0.05 (L = 120), n_matmul = 10, n_delay = 16, equal-time measurements
+every 8 slices, FP64 throughout.  Chains differ by RNG stream (splitmix64 of
+the seed, one 2^512 jump per chain) and so by their HS fields.  A step is one
+sweep of every chain; value = chains x steps / device time.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun, one rank per GPU) each rank runs its own 256 chains
+(weak scaling, no collective on the data path); times are max over ranks.
+`--impl reference` times the reference's own C build (oracle/_ref/dqmc_1_r,
+the reference src/ compiled against OpenBLAS) on the host cores, as the
+reference deploys it: one process per two cores, two OpenMP threads each.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "dqmc-dev_b200"))
+
+CFG = dict(Nx=12, Ny=12, U=4.0, mu=-1.0, tp=0.0, dt=0.05, L=120, n_matmul=10, n_delay=16,
+           period_eqlt=8)
+CHAINS = 256
+METRIC = "chain-sweeps/s"
+WORKLOAD = ("256 chains x 12x12 square Hubbard (N=144), U=4, mu=-1, beta=6, dtau=0.05 "
+            "(L=120), n_matmul=10, n_delay=16, eqlt every 8 slices, FP64")
+
+
+def sim_dicts(n, seed, n_sweep):
+    from dqmc_b200 import gen
+    rngs = gen.chain_rngs(seed, n)
+    d0 = gen.make_sim(init_rng=rngs[0], n_sweep_warm=0, n_sweep_meas=n_sweep, **CFG)
+    out = [d0]
+    N, L = CFG["Nx"] * CFG["Ny"], CFG["L"]
+    for r in rngs[1:]:
+        hs, rng = gen.initial_hs(r, L, N)
+        d = dict(d0)
+        d["state/init_rng"], d["state/rng"], d["state/hs"] = r, rng, hs
+        out.append(d)
+    return out
+
+
+def dist_setup(gpus):
+    rank, world = int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl" if gpus > 0 else "gloo",
+                                timeout=datetime.timedelta(seconds=600))
+    return rank, world, local
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.device = device
+        self.p = None
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.device),
+                                       f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            self.p.wait()
+            self.f.close()
+
+    def summary(self):
+        if not self.p or not os.path.exists(self.path):
+            return None
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        busy = [v for v in sm if v > 0.5 * mx] or sm
+        return {"sm_mhz": float(np.median(busy)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def fp64_peak():
+    """cuBLAS DGEMM 8192^3, best of 5 (FP64 tensor roofline denominator)."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn_like(a)
+    for _ in range(2):
+        a @ b
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        a @ b
+        e.record()
+        torch.cuda.synchronize()
+        best = min(best, s.elapsed_time(e) / 1e3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2 * n ** 3 / best / 1e12
+
+
+def reference_rate(n_proc, sweeps, seed=1):
+    """Aggregate chain-sweeps/s of the reference C build: n_proc processes of
+    dqmc_1_r (2 OpenMP threads, OpenBLAS 1 thread) on independent chains."""
+    from dqmc_b200 import gen
+    exe = os.path.join(ROOT, "oracle", "_ref", "dqmc_1_r")
+    if not os.path.exists(exe):
+        raise RuntimeError(f"reference build missing: {exe}")
+    tmp = tempfile.mkdtemp()
+    cwd = os.getcwd()
+    os.chdir(tmp)
+    try:
+        paths = gen.create_batch(Nfiles=n_proc, prefix="ref", seed=seed, n_sweep_warm=0,
+                                 n_sweep_meas=sweeps, **CFG)
+        env = dict(os.environ, OPENBLAS_NUM_THREADS="1", OMP_NUM_THREADS="2")
+        t0 = time.perf_counter()
+        procs = [subprocess.Popen([exe, "-b", "-l", f"{p}.log", p], env=env,
+                                  stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+                 for p in paths]
+        rcs = [p.wait() for p in procs]
+        t = time.perf_counter() - t0
+        if any(rcs):
+            raise RuntimeError(f"reference runs failed: {rcs}")
+    finally:
+        os.chdir(cwd)
+        shutil.rmtree(tmp, ignore_errors=True)
+    return n_proc * sweeps / t, t
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    cores = os.cpu_count() or 2
+    n_proc = max(1, cores // 2)
+    sweeps = max(1, args.steps)
+    rate, t = reference_rate(n_proc, sweeps)
+    line = {
+        "metric": METRIC, "value": rate, "unit": METRIC, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t / sweeps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": WORKLOAD, "chains": n_proc, "cpu": True},
+        "cpu_baseline": {"value": rate, "unit": METRIC, "cores": n_proc * 2, "kind": "reference",
+                         "sample": f"{n_proc} dqmc_1_r processes x {sweeps} sweeps of one "
+                                   f"12x12 L=120 chain each (2 OpenMP threads, OpenBLAS 1 thread)"},
+        "e2e": {"value": rate, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--chains", type=int, default=CHAINS)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = dist_setup(args.gpus)
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    from dqmc_b200 import engine, lib
+
+    nch = args.chains
+    total = args.warmup + args.steps + 4
+    dicts = sim_dicts(nch, seed=1000 + rank, n_sweep=total)
+    sims = [engine.SimData(d) for d in dicts]
+    eng = engine.Engine(sims, device=local)
+    eng.init()
+    stream = torch.cuda.ExternalStream(eng.stream())
+
+    # warm-up (also captures the sweep graph)
+    eng.sweeps(args.warmup, sync=True)
+
+    # timed region: K sweeps, device time on the engine's stream
+    barrier(world)
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        eng.sweeps(args.steps, sync=False)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    t_dev = ev0.elapsed_time(ev1) / 1e3
+    assert eng.errors() == 0, "device error word set"
+    t_max = max_over_ranks(t_dev, world)
+    value = nch * args.steps * world / t_max
+    launches = eng.launches_per_sweep(True, False) * args.steps
+
+    # end to end through the C ABI with host buffers: per step, the chains'
+    # state goes host -> device, one sweep runs, state and measurements come back
+    L = lib.load()
+    e2e_steps = 2
+    h2d = d2h = 0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        for c, s in enumerate(sims):
+            lib.check(L.dqmc_engine_set_chain(eng.h, c, s.exp_lambda.ctypes.data,
+                                              s.del_.ctypes.data, s.rng.ctypes.data,
+                                              s.hs.ctypes.data, s.sweep), "set_chain")
+        h2d = sum(s.exp_lambda.nbytes + s.del_.nbytes + s.rng.nbytes + s.hs.nbytes for s in sims)
+        eng.sweeps(1, sync=True)
+        eng.pull()
+        d2h = sum(s.rng.nbytes + s.hs.nbytes + s.eq_acc.nbytes + 8 for s in sims)
+    t_e2e = max_over_ranks((time.perf_counter() - t0) / e2e_steps, world)
+    e2e = nch * world / t_e2e
+
+    # per-launch profile of one more sweep (eager launches with events)
+    prof = eng.profile_sweep(True, False)
+    peak = fp64_peak()
+    gm_ms, gm_n, gm_fl, gm_by = prof["gemm"]
+    eq_ms = prof["calc_eq_g"][0]
+    up_ms = prof["update"][0]
+    me_ms = prof["meas"][0]
+    tot_ms = gm_ms + eq_ms + up_ms + me_ms
+    achieved = gm_fl / (gm_ms / 1e3) / 1e12 if gm_ms > 0 else 0.0
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cores = os.cpu_count() or 2
+            n_proc = max(1, cores // 2)
+            rate, t = reference_rate(n_proc, 3)
+            cpu = {"value": rate, "unit": METRIC, "cores": 2 * n_proc, "kind": "reference",
+                   "sample": f"{n_proc} processes of the reference dqmc_1_r x 3 sweeps of one "
+                             f"12x12 L=120 chain each, {t:.1f} s"}
+        except Exception as ex:  # noqa: BLE001
+            cpu = {"value": None, "unit": METRIC, "cores": 0, "kind": "reference",
+                   "sample": f"not run: {ex}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "chains_per_gpu": nch,
+                       "l2": "inputs larger than L2 (about 2.6 MB of matrices per chain-spin)",
+                       "sweep_profile_ms": {"gemm": gm_ms, "calc_eq_g": eq_ms, "update": up_ms,
+                                            "meas": me_ms, "sum": tot_ms}},
+            "gpu_launches": launches,
+            "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "tensor", "kernel": "k_gemm (batched FP64 DMMA: wrap, "
+                                                      "cluster products, half wrap)",
+                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak if peak else None, "traffic": None,
+                         "peak_source": "cuBLAS DGEMM 8192^3 measured in this run "
+                                        "(MEASURED_PEAKS.json carries no FP64 figure)",
+                         "launches": int(gm_n)},
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    eng.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,1071 @@
+// Host side of the GPU engine: device state of a group of chains, the
+// sequencing of one sweep (reference src/dqmc.c:222-459) as batched kernel
+// launches, CUDA-graph capture per sweep kind, and the C ABI of
+// include/dqmc_b200.h.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <vector>
+
+#include "dqmc_b200.h"
+#include "gemm.cuh"
+#include "meas.cuh"
+#include "qr.cuh"
+#include "update.cuh"
+#include "uneq.cuh"
+
+namespace dq {
+
+#define CK(x)                                                                      \
+	do {                                                                           \
+		cudaError_t e_ = (x);                                                      \
+		if (e_ != cudaSuccess) {                                                   \
+			fprintf(stderr, "dqmc_b200: %s failed: %s (%s:%d)\n", #x,              \
+			        cudaGetErrorString(e_), __FILE__, __LINE__);                   \
+			return DQMC_E_CUDA;                                                    \
+		}                                                                          \
+	} while (0)
+
+static inline Addr per_item(long long stride) { return Addr{stride, 0, 1}; }
+static inline Addr per_spin(long long stride) { return Addr{0, stride, 2}; }
+
+// ------------------------------------------------------------------ launches
+
+template <typename T, int BM, int BN, int BK, int WM, int WN>
+static void launch_gemm_cfg(const GemmArgs<T> &g, cudaStream_t st)
+{
+	using Cfg = GemmCfg<T, BM, BN, BK, WM, WN>;
+	static bool attr = false;
+	if (!attr) {
+		cudaFuncSetAttribute(k_gemm<T, BM, BN, BK, WM, WN>,
+		                     cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM_BYTES);
+		attr = true;
+	}
+	dim3 grid((g.M + BM - 1) / BM, (g.N + BN - 1) / BN, g.batch);
+	k_gemm<T, BM, BN, BK, WM, WN><<<grid, Cfg::THREADS, Cfg::SMEM_BYTES, st>>>(g);
+}
+
+// tile choice: least padded area, larger tiles on ties
+template <typename T>
+void launch_gemm(const GemmArgs<T> &g, cudaStream_t st)
+{
+	auto pad = [&](int t) { return (long long)((g.M + t - 1) / t * t) * ((g.N + t - 1) / t * t); };
+	const long long p64 = pad(64), p48 = pad(48), p32 = pad(32);
+	if (p64 <= p48 && p64 <= p32) launch_gemm_cfg<T, 64, 64, 16, 2, 2>(g, st);
+	else if (p48 <= p32) launch_gemm_cfg<T, 48, 48, 16, 2, 2>(g, st);
+	else launch_gemm_cfg<T, 32, 32, 16, 2, 2>(g, st);
+}
+
+template <typename T>
+static GemmArgs<T> gargs(int M, int N, int K, int batch, const T *A, Addr aA, int lda,
+		const T *B, Addr aB, int ldb, T *C, Addr aC, int ldc, T alpha = one<T>(),
+		T beta = zero<T>(), int mode = 0)
+{
+	GemmArgs<T> g;
+	memset(&g, 0, sizeof(g));
+	g.M = M; g.N = N; g.K = K; g.batch = batch;
+	g.A = A; g.aA = aA; g.lda = lda;
+	g.B = B; g.aB = aB; g.ldb = ldb;
+	g.C = C; g.aC = aC; g.ldc = ldc;
+	g.alpha = alpha; g.beta = beta; g.mode = mode;
+	g.aD = Addr{0, 0, 1};
+	g.aG = Addr{0, 0, 1};
+	return g;
+}
+
+// register shapes for the per-matrix factorisations
+template <typename T, int RPL, int CPW, int NW>
+static int launch_qr_cfg(const QrArgs<T> &a, cudaStream_t st)
+{
+	const size_t sm = qr_smem_bytes<T>(a.N, NW);
+	static size_t attr = 0;
+	if (sm > attr) {
+		if (cudaFuncSetAttribute(k_qr<T, RPL, CPW, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		                         (int)sm) != cudaSuccess)
+			return DQMC_E_ARG;
+		attr = sm;
+	}
+	k_qr<T, RPL, CPW, NW><<<a.batch, NW * 32, sm, st>>>(a);
+	return 0;
+}
+
+template <typename T, int RPL, int CPW, int NW>
+static int launch_rec_cfg(const RecArgs<T> &a, cudaStream_t st)
+{
+	const size_t sm = rec_smem_bytes<T>(a.N);
+	static size_t attr = 0;
+	if (sm > attr) {
+		if (cudaFuncSetAttribute(k_recombine<T, RPL, CPW, NW>,
+		                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
+			return DQMC_E_ARG;
+		attr = sm;
+	}
+	k_recombine<T, RPL, CPW, NW><<<a.batch, NW * 32, sm, st>>>(a);
+	return 0;
+}
+
+// largest N the register-resident factorisations support
+template <typename T> constexpr int max_dense_n() { return is_cplx<T>::value ? 112 : 160; }
+
+// (max N, rows per lane, columns per warp, warps); complex stops at 112 so
+// that an N x N complex matrix still fits in shared memory
+#define DQ_SHAPES(X)                    \
+	X(32, 1, 8, 4)                      \
+	X(64, 2, 8, 8)                      \
+	X(96, 3, 8, 12)                     \
+	X(112, 4, 7, 16)                    \
+	X(128, 4, 8, 16)                    \
+	X(144, 5, 9, 16)                    \
+	X(160, 5, 10, 16)
+
+template <typename T>
+int launch_qr(const QrArgs<T> &a, cudaStream_t st)
+{
+	if (a.N < 1 || a.N > max_dense_n<T>()) return DQMC_E_ARG;
+#define X(NMAX, R, C, W) if (a.N <= NMAX) return launch_qr_cfg<T, R, C, W>(a, st);
+	DQ_SHAPES(X)
+#undef X
+	return DQMC_E_ARG;
+}
+
+template <typename T>
+int launch_rec(const RecArgs<T> &a, cudaStream_t st)
+{
+	if (a.N < 1 || a.N > max_dense_n<T>()) return DQMC_E_ARG;
+#define X(NMAX, R, C, W) if (a.N <= NMAX) return launch_rec_cfg<T, R, C, W>(a, st);
+	DQ_SHAPES(X)
+#undef X
+	return DQMC_E_ARG;
+}
+
+// ------------------------------------------------------- small helper kernels
+
+// d_l and 1/d_l of every slice from the fields: spin s uses exp_lambda[i + N*(h^s)]
+__global__ void k_diag_all(int N, int L, int nchain, const double *el, const int *hs,
+		double *dv, double *dvi)
+{
+	const long long total = (long long)nchain * 2 * L * N;
+	for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
+	     q += (long long)gridDim.x * blockDim.x) {
+		const int i = (int)(q % N);
+		const int l = (int)((q / N) % L);
+		const int s = (int)((q / ((long long)N * L)) % 2);
+		const int c = (int)(q / (2LL * N * L));
+		const int h = hs[((size_t)c * L + l) * N + i];
+		const double v = el[(size_t)c * 2 * N + i + N * (h ^ s)];
+		dv[q] = v;
+		dvi[q] = 1.0 / v;
+	}
+}
+
+// out[b] = in[b] * diag(d[b])  (N x N)
+template <typename T>
+__global__ void k_colscale(int N, int batch, const T *in, Addr ain, const double *d, Addr ad,
+		T *out, Addr aout)
+{
+	const long long NN = (long long)N * N;
+	for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < NN * batch;
+	     q += (long long)gridDim.x * blockDim.x) {
+		const int b = (int)(q / NN);
+		const long long e = q % NN;
+		const int c = (int)(e / N);
+		out[aout.off(b) + e] = in[ain.off(b) + e] * d[ad.off(b) + c];
+	}
+}
+
+template <typename T>
+__global__ void k_copy(long long n, const T *in, T *out)
+{
+	for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+	     q += (long long)gridDim.x * blockDim.x)
+		out[q] = in[q];
+}
+
+template <typename T>
+__global__ void k_combine_phase(int nchain, const T *phi, T *phase)
+{
+	const int c = blockIdx.x * blockDim.x + threadIdx.x;
+	if (c < nchain) phase[c] = phi[2 * c] * phi[2 * c + 1];
+}
+
+static int grid_for(long long n, int threads = 256)
+{
+	long long g = (n + threads - 1) / threads;
+	if (g > 148 * 16) g = 148 * 16;
+	return (int)(g < 1 ? 1 : g);
+}
+
+// ------------------------------------------------- calc_eq_g as launches
+
+// device buffers the stabilised G computation works in, NB items each
+template <typename T>
+struct EqWork {
+	int N, F, NB;
+	const T *Cl; long long cl_stride;  // cluster matrices: item b, cluster f at
+	                                   // Cl + b*cl_stride + f*N*N
+	T *Qm, *Tm, *Tm2, *Rs, *X, *W;     // NB x N*N each
+	double *dR;                        // NB x N
+	int *pvt;                          // NB x N
+	T *qdet;                           // NB
+	T *G; long long g_stride;          // output
+	T *phi;                            // NB output phases
+	unsigned *err;
+};
+
+template <typename T>
+static int eq_gemm(const GemmArgs<T> &g, cudaStream_t st, int *count)
+{
+	launch_gemm<T>(g, st);
+	if (count) (*count)++;
+	return 0;
+}
+
+// G = (I + C_{l0-1} ... C_{l0})^-1 over the F clusters (cyclic), grouped two
+// clusters at a time as calc_eq_g(l0, N, F, 2, C, ...) does (greens.c:69-208)
+template <typename T>
+static int run_calc_eq_g(const EqWork<T> &w, int l0, cudaStream_t st, int *count)
+{
+	const int N = w.N, F = w.F, NB = w.NB;
+	const size_t NN = (size_t)N * N;
+	const Addr aCl = Addr{w.cl_stride, 0, 1}, aI = Addr{(long long)NN, 0, 1};
+	auto clu = [&](int f) { return w.Cl + (size_t)(((f % F) + F) % F) * NN; };
+	int m = (l0 + 1 + (F - 1) % 2) % F;
+	QrArgs<T> q;
+	memset(&q, 0, sizeof(q));
+	q.N = N; q.batch = NB; q.err = w.err;
+	q.Q = w.Qm; q.q_stride = NN;
+	q.dout = w.dR; q.dout_stride = N;
+	q.qdet = w.qdet;
+	q.pvt = w.pvt; q.p_stride = N;
+	const int first = (F == 1) ? 1 : ((F - 1) % 2 == 1 ? 2 : 1);
+	if (first == 2) {
+		eq_gemm(gargs<T>(N, N, N, NB, clu(l0 + 1), aCl, N, clu(l0), aCl, N, w.X, aI, N), st, count);
+		q.X = w.X; q.x_stride = NN;
+	} else {
+		q.X = clu(l0); q.x_stride = w.cl_stride;
+	}
+	q.mode = QR_PIVOT;
+	q.Tout = w.Tm; q.t_stride = NN;
+	if (launch_qr<T>(q, st)) return DQMC_E_ARG;
+	if (count) (*count)++;
+	T *Tc = w.Tm, *Tn = w.Tm2;
+	while (m != l0) {
+		const int next = (m + 2) % F;
+		eq_gemm(gargs<T>(N, N, N, NB, clu(m + 1), aCl, N, clu(m), aCl, N, w.W, aI, N), st, count);
+		eq_gemm(gargs<T>(N, N, N, NB, w.W, aI, N, w.Qm, aI, N, w.X, aI, N), st, count);
+		m = next;
+		QrArgs<T> r = q;
+		r.mode = QR_PRESORT;
+		r.X = w.X; r.x_stride = NN;
+		r.dcol = w.dR; r.d_stride = N;
+		r.Tout = nullptr;
+		r.Rs = w.Rs; r.r_stride = NN;
+		if (launch_qr<T>(r, st)) return DQMC_E_ARG;
+		if (count) (*count)++;
+		GemmArgs<T> g = gargs<T>(N, N, N, NB, w.Rs, aI, N, Tc, aI, N, Tn, aI, N, one<T>(),
+		                         zero<T>(), GM_A_UPPER | GM_B_GATHER);
+		g.gidx = w.pvt;
+		g.aG = Addr{(long long)N, 0, 1};
+		eq_gemm(g, st, count);
+		T *t = Tc; Tc = Tn; Tn = t;
+	}
+	RecArgs<T> ra;
+	memset(&ra, 0, sizeof(ra));
+	ra.N = N; ra.batch = NB;
+	ra.Q = w.Qm; ra.q_stride = NN;
+	ra.Tm = Tc; ra.t_stride = NN;
+	ra.d = w.dR; ra.d_stride = N;
+	ra.qdet = w.qdet;
+	ra.G = w.G; ra.g_stride = w.g_stride;
+	ra.phase = w.phi;
+	ra.err = w.err;
+	if (launch_rec<T>(ra, st)) return DQMC_E_ARG;
+	if (count) (*count)++;
+	return 0;
+}
+
+// C = B_{l0+n-1} ... B_{l0} with B_l = exp_K diag(d_l) (mul_seq, greens.c:8-41,
+// over B's that are never materialised).  d_l for item b at d + b*d_stride +
+// l*N; exp_K per spin (item parity); X, W: NB x N*N scratch.
+template <typename T>
+static void run_mul_seq(int N, int n, int NB, const T *expK, Addr aK, const double *d,
+		long long d_stride, T *out, Addr aout, T *X, T *W, cudaStream_t st, int *count)
+{
+	const size_t NN = (size_t)N * N;
+	const Addr aI = Addr{(long long)NN, 0, 1};
+	T *src = (n == 1) ? out : W;
+	Addr as = (n == 1) ? aout : aI;
+	k_colscale<T><<<grid_for((long long)NB * NN), 256, 0, st>>>(N, NB, expK, aK, d,
+	        Addr{d_stride, 0, 1}, src, as);
+	if (count) (*count)++;
+	for (int m = 1; m < n; m++) {
+		const bool last = (m == n - 1);
+		T *dst = last ? out : (src == W ? X : W);
+		const Addr ad = last ? aout : aI;
+		GemmArgs<T> g = gargs<T>(N, N, N, NB, expK, aK, N, src, as, N, dst, ad, N, one<T>(),
+		                         zero<T>(), GM_B_ROWD);
+		g.d = d + (size_t)m * N;
+		g.aD = Addr{d_stride, 0, 1};
+		eq_gemm(g, st, count);
+		src = dst;
+		as = ad;
+	}
+}
+
+// -------------------------------------------------------------- the group
+
+template <typename T>
+struct DevBuf {
+	T *p = nullptr;
+	size_t n = 0;
+	int alloc(size_t count)
+	{
+		n = count;
+		if (count == 0) return 0;
+		if (cudaMalloc(&p, sizeof(T) * count) != cudaSuccess) {
+			p = nullptr;
+			return DQMC_E_NOMEM;
+		}
+		cudaMemset(p, 0, sizeof(T) * count);
+		return 0;
+	}
+	void release()
+	{
+		if (p) cudaFree(p);
+		p = nullptr;
+	}
+};
+
+// inverse of a class map: CSR offsets over classes, entries in loop order
+static void invert_map(const int *map, int n_entries, int n_class, std::vector<int> &off,
+		std::vector<int> &idx)
+{
+	off.assign(n_class + 1, 0);
+	for (int e = 0; e < n_entries; e++) off[map[e] + 1]++;
+	for (int r = 0; r < n_class; r++) off[r + 1] += off[r];
+	idx.resize(n_entries);
+	std::vector<int> fill(off.begin(), off.end() - 1);
+	for (int e = 0; e < n_entries; e++) idx[fill[map[e]]++] = e;
+}
+
+struct GroupBase {
+	virtual ~GroupBase() {}
+	virtual int set_chain(int c, const double *el, const double *del, const uint64_t *rng,
+	                      const int *hs, int sweep) = 0;
+	virtual int set_acc(int c, int eqn, const void *eq, int uen, const void *ue) = 0;
+	virtual int init() = 0;
+	virtual int sweeps(int n, int sync) = 0;
+	virtual int get_chain(int c, uint64_t *rng, int *hs, int *sweep) = 0;
+	virtual int get_acc(int c, int *eqn, void *eq, int *uen, void *ue) = 0;
+	virtual int get_g(int c, void *gu, void *gd, void *phase) = 0;
+	virtual int accepts(int c, long long *n) = 0;
+	virtual unsigned errors() = 0;
+	virtual int sync() = 0;
+	virtual cudaStream_t stream() = 0;
+	virtual int launches(int meq, int mue) = 0;
+	virtual int profile(int meq, int mue, double *out, int ncls) = 0;
+};
+
+template <typename T>
+struct Group : GroupBase {
+	dqmc_params p;
+	int C;        // chains
+	int NB;       // items = 2 C
+	int N, L, F, nmul;
+	int sweep = 0;
+	int kd = 0, ldp = 0;   // delayed-update flush period and panel ld
+	int eq_size = 0, ue_size = 0;
+	cudaStream_t st = nullptr;
+	std::map<int, cudaGraphExec_t> graphs;
+	std::map<int, int> graph_launches;
+	int launch_count = 0;
+
+	// parameters
+	DevBuf<T> expK, iexpK, ehK, iehK, peu, ped;
+	DevBuf<int> i_off, i_idx, ij_off, ij_idx, bb_off, bb_idx, bonds;
+	// chains
+	DevBuf<double> el, del, dv, dvi;
+	DevBuf<uint64_t> rng;
+	DevBuf<int> hs, nacc, n_eq, n_ue;
+	DevBuf<T> phase, G, Cl, Qm, Tm, Tm2, Rs, X, W, Gh, acc_eq, acc_ue, phi, qdet;
+	DevBuf<double> dR;
+	DevBuf<int> pvt;
+	DevBuf<unsigned> err;
+	UneqState<T> ue;
+
+	~Group() override
+	{
+		for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
+		DevBuf<T> *tb[] = {&expK, &iexpK, &ehK, &iehK, &peu, &ped, &phase, &G, &Cl, &Qm, &Tm,
+		                   &Tm2, &Rs, &X, &W, &Gh, &acc_eq, &acc_ue, &phi, &qdet};
+		for (auto *b : tb) b->release();
+		DevBuf<int> *ib[] = {&i_off, &i_idx, &ij_off, &ij_idx, &bb_off, &bb_idx, &bonds, &hs,
+		                     &nacc, &n_eq, &n_ue, &pvt};
+		for (auto *b : ib) b->release();
+		el.release(); del.release(); dv.release(); dvi.release(); dR.release();
+		rng.release(); err.release();
+		ue.release();
+		if (st) cudaStreamDestroy(st);
+	}
+
+	int create(const dqmc_params &pp, int nchain)
+	{
+		p = pp;
+		C = nchain;
+		NB = 2 * C;
+		N = p.N; L = p.L; F = p.F; nmul = p.n_matmul;
+		if (N < 1 || L < 1 || F < 1 || nmul < 1 || L != F * nmul || N > max_dense_n<T>() ||
+		    N > 512 || C < 1)
+			return DQMC_E_ARG;
+		if (p.period_uneqlt > 0 && !UneqState<T>::supported(N, F)) return DQMC_E_ARG;
+		CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+		const size_t NN = (size_t)N * N;
+		int rc = 0;
+		rc |= expK.alloc(2 * NN); rc |= iexpK.alloc(2 * NN);
+		rc |= ehK.alloc(2 * NN); rc |= iehK.alloc(2 * NN);
+		rc |= peu.alloc(NN); rc |= ped.alloc(NN);
+		rc |= el.alloc((size_t)C * 2 * N); rc |= del.alloc((size_t)C * 2 * N);
+		rc |= dv.alloc((size_t)C * 2 * L * N); rc |= dvi.alloc((size_t)C * 2 * L * N);
+		rc |= rng.alloc((size_t)C * 17); rc |= hs.alloc((size_t)C * L * N);
+		rc |= nacc.alloc(C); rc |= n_eq.alloc(C); rc |= n_ue.alloc(C);
+		rc |= phase.alloc(C); rc |= phi.alloc(NB); rc |= qdet.alloc(NB);
+		rc |= G.alloc(NB * NN); rc |= Cl.alloc((size_t)NB * F * NN);
+		rc |= Qm.alloc(NB * NN); rc |= Tm.alloc(NB * NN); rc |= Tm2.alloc(NB * NN);
+		rc |= Rs.alloc(NB * NN); rc |= X.alloc(NB * NN); rc |= W.alloc(NB * NN);
+		rc |= Gh.alloc(NB * NN); rc |= dR.alloc((size_t)NB * N); rc |= pvt.alloc((size_t)NB * N);
+		rc |= err.alloc(1);
+		eq_size = eq_acc_size(p.num_i, p.num_ij);
+		ue_size = p.period_uneqlt > 0 ? ue_acc_size(p.num_ij, p.num_bb, L, p.meas_bond_corr) : 0;
+		rc |= acc_eq.alloc((size_t)C * eq_size);
+		if (ue_size) rc |= acc_ue.alloc((size_t)C * ue_size);
+		if (rc) return DQMC_E_NOMEM;
+		if (p.period_uneqlt > 0 && ue.alloc(N, L, F, NB)) return DQMC_E_NOMEM;
+		// parameter matrices, per spin
+		auto up2 = [&](DevBuf<T> &dst, const void *u, const void *d) {
+			cudaMemcpy(dst.p, u, sizeof(T) * NN, cudaMemcpyHostToDevice);
+			cudaMemcpy(dst.p + NN, d, sizeof(T) * NN, cudaMemcpyHostToDevice);
+		};
+		up2(expK, p.exp_Ku, p.exp_Kd);
+		up2(iexpK, p.inv_exp_Ku, p.inv_exp_Kd);
+		up2(ehK, p.exp_halfKu, p.exp_halfKd);
+		up2(iehK, p.inv_exp_halfKu, p.inv_exp_halfKd);
+		if (p.peierlsu) cudaMemcpy(peu.p, p.peierlsu, sizeof(T) * NN, cudaMemcpyHostToDevice);
+		if (p.peierlsd) cudaMemcpy(ped.p, p.peierlsd, sizeof(T) * NN, cudaMemcpyHostToDevice);
+		std::vector<int> off, idx;
+		auto upv = [&](DevBuf<int> &dst, const std::vector<int> &v) -> int {
+			if (dst.alloc(v.size() ? v.size() : 1)) return DQMC_E_NOMEM;
+			if (!v.empty()) cudaMemcpy(dst.p, v.data(), sizeof(int) * v.size(), cudaMemcpyHostToDevice);
+			return 0;
+		};
+		invert_map(p.map_i, N, p.num_i, off, idx);
+		if (upv(i_off, off) || upv(i_idx, idx)) return DQMC_E_NOMEM;
+		invert_map(p.map_ij, N * N, p.num_ij, off, idx);
+		if (upv(ij_off, off) || upv(ij_idx, idx)) return DQMC_E_NOMEM;
+		if (p.meas_bond_corr && p.num_b > 0) {
+			invert_map(p.map_bb, p.num_b * p.num_b, p.num_bb, off, idx);
+			if (upv(bb_off, off) || upv(bb_idx, idx)) return DQMC_E_NOMEM;
+			std::vector<int> bv(p.bonds, p.bonds + 2 * p.num_b);
+			if (upv(bonds, bv)) return DQMC_E_NOMEM;
+		}
+		// delayed-update panels: the file's n_delay unless shared memory is short
+		kd = p.n_delay < 1 ? 1 : p.n_delay;
+		ldp = (N + 15) / 16 * 16 + 4;
+		while (kd > 1 && update_smem_bytes<T>(N, kd, ldp) > 200 * 1024) kd /= 2;
+		cudaFuncSetAttribute(k_update<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		                     (int)update_smem_bytes<T>(N, kd, ldp));
+		CK(cudaDeviceSynchronize());
+		return 0;
+	}
+
+	int set_chain(int c, const double *e, const double *d, const uint64_t *r, const int *h,
+	              int sw) override
+	{
+		if (c < 0 || c >= C) return DQMC_E_ARG;
+		CK(cudaMemcpy(el.p + (size_t)c * 2 * N, e, sizeof(double) * 2 * N, cudaMemcpyHostToDevice));
+		CK(cudaMemcpy(del.p + (size_t)c * 2 * N, d, sizeof(double) * 2 * N, cudaMemcpyHostToDevice));
+		CK(cudaMemcpy(rng.p + (size_t)c * 17, r, sizeof(uint64_t) * 17, cudaMemcpyHostToDevice));
+		CK(cudaMemcpy(hs.p + (size_t)c * L * N, h, sizeof(int) * L * N, cudaMemcpyHostToDevice));
+		sweep = sw;
+		return 0;
+	}
+
+	int set_acc(int c, int eqn, const void *eq, int uen, const void *uea) override
+	{
+		if (c < 0 || c >= C) return DQMC_E_ARG;
+		CK(cudaMemcpy(n_eq.p + c, &eqn, sizeof(int), cudaMemcpyHostToDevice));
+		if (eq) CK(cudaMemcpy(acc_eq.p + (size_t)c * eq_size, eq, sizeof(T) * eq_size, cudaMemcpyHostToDevice));
+		if (ue_size) {
+			CK(cudaMemcpy(n_ue.p + c, &uen, sizeof(int), cudaMemcpyHostToDevice));
+			if (uea) CK(cudaMemcpy(acc_ue.p + (size_t)c * ue_size, uea, sizeof(T) * ue_size, cudaMemcpyHostToDevice));
+		}
+		return 0;
+	}
+
+	// ------------------------------------------------------------ steps
+
+	void gemm(const GemmArgs<T> &g)
+	{
+		prof_begin(0);
+		eq_gemm<T>(g, st, &launch_count);
+		double fl = 2.0 * g.M * g.N * g.K * g.batch * (is_cplx<T>::value ? 4.0 : 1.0);
+		if (g.mode & GM_A_UPPER) fl *= 0.5;
+		prof_end(0, fl, (double)sizeof(T) * ((double)g.M * g.K + (double)g.K * g.N + (double)g.M * g.N) * g.batch);
+	}
+
+	// --- optional per-launch timing (one eager sweep, see profile())
+	bool profiling = false;
+	std::vector<cudaEvent_t> pev;
+	struct PRec { int cls; double flops, bytes; int e0, e1; };
+	std::vector<PRec> precs;
+	int cur_e0 = -1;
+	cudaEvent_t new_event()
+	{
+		cudaEvent_t e;
+		cudaEventCreate(&e);
+		pev.push_back(e);
+		return e;
+	}
+	void prof_begin(int)
+	{
+		if (!profiling) return;
+		cudaEvent_t e = new_event();
+		cudaEventRecord(e, st);
+		cur_e0 = (int)pev.size() - 1;
+	}
+	void prof_end(int cls, double flops, double bytes)
+	{
+		if (!profiling) return;
+		cudaEvent_t e = new_event();
+		cudaEventRecord(e, st);
+		precs.push_back(PRec{cls, flops, bytes, cur_e0, (int)pev.size() - 1});
+	}
+
+	// cluster C_f = B_{f n + n - 1} ... B_{f n}
+	void build_cluster(int f)
+	{
+		const size_t NN = (size_t)N * N;
+		prof_begin(0);
+		run_mul_seq<T>(N, nmul, NB, expK.p, per_spin(NN), dv.p + (size_t)f * nmul * N, (long long)L * N,
+		               Cl.p + (size_t)f * NN, per_item((long long)F * NN), X.p, W.p, st, &launch_count);
+		const double fl = 2.0 * N * NN * NB * (nmul - 1) * (is_cplx<T>::value ? 4.0 : 1.0);
+		prof_end(0, fl, 3.0 * sizeof(T) * NN * NB * (nmul - 1));
+	}
+
+	EqWork<T> eq_work()
+	{
+		EqWork<T> w;
+		w.N = N; w.F = F; w.NB = NB;
+		w.Cl = Cl.p; w.cl_stride = (long long)F * N * N;
+		w.Qm = Qm.p; w.Tm = Tm.p; w.Tm2 = Tm2.p; w.Rs = Rs.p; w.X = X.p; w.W = W.p;
+		w.dR = dR.p; w.pvt = pvt.p; w.qdet = qdet.p;
+		w.G = G.p; w.g_stride = (long long)N * N;
+		w.phi = phi.p; w.err = err.p;
+		return w;
+	}
+
+	// G = (I + C_{l0-1} ... C_{l0})^-1 (cyclic), then the chain phases
+	int calc_eq_g(int l0)
+	{
+		prof_begin(2);
+		int rc = run_calc_eq_g<T>(eq_work(), l0, st, &launch_count);
+		prof_end(2, 0.0, 0.0);
+		if (rc) return rc;
+		k_combine_phase<T><<<(C + 127) / 128, 128, 0, st>>>(C, phi.p, phase.p);
+		launch_count++;
+		return 0;
+	}
+
+	void update(int l)
+	{
+		UpdArgs<T> a;
+		a.N = N; a.L = L; a.n_delay = kd; a.nchain = C; a.slice = l; a.ldp = ldp;
+		a.del = del.p; a.exp_lambda = el.p; a.rng = rng.p; a.hs = hs.p; a.G = G.p;
+		a.phase = phase.p; a.dv = dv.p; a.dvi = dvi.p; a.n_accept = nacc.p; a.err = err.p;
+		const int np = (N + 31) / 32 * 32;
+		prof_begin(1);
+		k_update<T><<<C, 2 * np, update_smem_bytes<T>(N, kd, ldp), st>>>(a);
+		prof_end(1, 0.0, 0.0);
+		launch_count++;
+	}
+
+	// G <- B_l G B_l^-1 = exp_K (D G D^-1) inv_exp_K
+	void wrap(int l)
+	{
+		const size_t NN = (size_t)N * N;
+		const Addr aI = per_item(NN);
+		GemmArgs<T> g = gargs<T>(N, N, N, NB, G.p, aI, N, iexpK.p, per_spin(NN), N, W.p, aI, N,
+		                         one<T>(), zero<T>(), GM_A_DD);
+		g.d = dv.p + (size_t)l * N;
+		g.dinv = dvi.p + (size_t)l * N;
+		g.aD = per_item((long long)L * N);
+		gemm(g);
+		gemm(gargs<T>(N, N, N, NB, expK.p, per_spin(NN), N, W.p, aI, N, G.p, aI, N));
+	}
+
+	// Gh = inv_exp_halfK (G exp_halfK)  (dqmc.c:366-380)
+	void half_wrap(const T *src, Addr as, T *dst, Addr ad, int batch_items)
+	{
+		const size_t NN = (size_t)N * N;
+		gemm(gargs<T>(N, N, N, batch_items, src, as, N, ehK.p, per_spin(NN), N, W.p, per_item(NN), N));
+		gemm(gargs<T>(N, N, N, batch_items, iehK.p, per_spin(NN), N, W.p, per_item(NN), N, dst, ad, N));
+	}
+
+	MeasArgs<T> meas_args()
+	{
+		MeasArgs<T> m;
+		memset(&m, 0, sizeof(m));
+		m.N = N; m.L = L; m.nchain = C; m.num_i = p.num_i; m.num_ij = p.num_ij;
+		m.num_b = p.num_b; m.num_bb = p.num_bb;
+		m.degen_i = p.degen_i; m.degen_ij = p.degen_ij; m.degen_bb = p.degen_bb;
+		m.phase = phase.p;
+		m.i_off = i_off.p; m.i_idx = i_idx.p; m.ij_off = ij_off.p; m.ij_idx = ij_idx.p;
+		m.bb_off = bb_off.p; m.bb_idx = bb_idx.p; m.bonds = bonds.p;
+		m.peu = peu.p; m.ped = ped.p;
+		return m;
+	}
+
+	void meas_eqlt()
+	{
+		const size_t NN = (size_t)N * N;
+		half_wrap(G.p, per_item(NN), Gh.p, per_item(NN), NB);
+		MeasArgs<T> m = meas_args();
+		m.G = Gh.p;
+		m.acc = acc_eq.p; m.acc_stride = eq_size; m.n_sample = n_eq.p;
+		prof_begin(4);
+		k_meas_eqlt<T><<<C, 256, 2 * N * sizeof(T) + 64, st>>>(m);
+		prof_end(4, 0.0, 0.0);
+		launch_count++;
+	}
+
+	int meas_uneqlt()
+	{
+		const size_t NN = (size_t)N * N;
+		int rc = ue.compute(*this);
+		if (rc) return rc;
+		// half wrap of all 3 L matrices per item (dqmc.c:415-451)
+		T *stk[3] = {ue.G0t.p, ue.Gtt.p, ue.Gt0.p};
+		for (int q = 0; q < 3; q++)
+			for (int l = 0; l < L; l++)
+				half_wrap(stk[q] + (size_t)l * NN, per_item((long long)L * NN), stk[q] + (size_t)l * NN,
+				          per_item((long long)L * NN), NB);
+		MeasArgs<T> m = meas_args();
+		m.G0t = ue.G0t.p; m.Gtt = ue.Gtt.p; m.Gt0 = ue.Gt0.p;
+		m.acc = acc_ue.p; m.acc_stride = ue_size; m.n_sample = n_ue.p;
+		m.bond = p.meas_bond_corr;
+		k_meas_uneqlt<T><<<dim3(C, L), 256, 0, st>>>(m);
+		launch_count++;
+		return 0;
+	}
+
+	int init() override
+	{
+		const long long tot = (long long)C * 2 * L * N;
+		k_diag_all<<<grid_for(tot), 256, 0, st>>>(N, L, C, el.p, hs.p, dv.p, dvi.p);
+		for (int f = 0; f < F; f++) build_cluster(f);
+		int rc = calc_eq_g(0);
+		if (rc) return rc;
+		CK(cudaStreamSynchronize(st));
+		return 0;
+	}
+
+	// queue one sweep of the given kind
+	int enqueue_sweep(bool meq, bool mue)
+	{
+		for (int l = 0; l < L; l++) {
+			update(l);
+			const int f = l / nmul;
+			const bool recalc = ((l + 1) % nmul) == 0;
+			if (recalc) {
+				build_cluster(f);
+				int rc = calc_eq_g((f + 1) % F);
+				if (rc) return rc;
+			} else {
+				wrap(l);
+			}
+			if (meq && p.period_eqlt > 0 && (l + 1) % p.period_eqlt == 0) meas_eqlt();
+		}
+		if (mue) {
+			int rc = meas_uneqlt();
+			if (rc) return rc;
+		}
+		return 0;
+	}
+
+	int sweeps(int n, int sync_after) override
+	{
+		for (int k = 0; k < n; k++) {
+			if (sweep >= p.n_sweep) break;
+			const bool meq = sweep >= p.n_sweep_warm;
+			const bool mue = meq && p.period_uneqlt > 0 && sweep % p.period_uneqlt == 0;
+			const int kind = (meq ? 1 : 0) | (mue ? 2 : 0);
+			auto it = graphs.find(kind);
+			if (it == graphs.end()) {
+				cudaGraph_t gr;
+				CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+				launch_count = 0;
+				int rc = enqueue_sweep(meq, mue);
+				cudaError_t ce = cudaStreamEndCapture(st, &gr);
+				if (rc) return rc;
+				if (ce != cudaSuccess) {
+					fprintf(stderr, "dqmc_b200: graph capture failed: %s\n", cudaGetErrorString(ce));
+					return DQMC_E_CUDA;
+				}
+				cudaGraphExec_t ex;
+				CK(cudaGraphInstantiate(&ex, gr, 0));
+				cudaGraphDestroy(gr);
+				graphs[kind] = ex;
+				graph_launches[kind] = launch_count;
+				it = graphs.find(kind);
+			}
+			CK(cudaGraphLaunch(it->second, st));
+			sweep++;
+		}
+		if (sync_after) return sync();
+		return 0;
+	}
+
+	// One eager (not graph) sweep of the given kind with CUDA events around
+	// every launch.  out[cls*4 + {0,1,2,3}] = {total ms, launches, flops, bytes}
+	// for classes 0 gemm, 1 update, 2 calc_eq_g (all its launches, gemms
+	// included), 4 measurement.  Advances the chains by one sweep.
+	int profile(int meq, int mue, double *out, int ncls) override
+	{
+		if (sweep >= p.n_sweep) return DQMC_E_ARG;
+		profiling = true;
+		precs.clear();
+		int rc = enqueue_sweep(meq, mue);
+		profiling = false;
+		if (rc) return rc;
+		CK(cudaStreamSynchronize(st));
+		sweep++;
+		for (int i = 0; i < ncls * 4; i++) out[i] = 0.0;
+		// calc_eq_g records nest the gemm records: count gemms inside a
+		// calc_eq_g window only under class 2
+		for (size_t i = 0; i < precs.size(); i++) {
+			const PRec &r = precs[i];
+			float ms = 0.f;
+			cudaEventElapsedTime(&ms, pev[r.e0], pev[r.e1]);
+			if (r.cls < ncls) {
+				out[r.cls * 4 + 0] += ms;
+				out[r.cls * 4 + 1] += 1;
+				out[r.cls * 4 + 2] += r.flops;
+				out[r.cls * 4 + 3] += r.bytes;
+			}
+		}
+		for (cudaEvent_t e : pev) cudaEventDestroy(e);
+		pev.clear();
+		precs.clear();
+		return 0;
+	}
+
+	int sync() override
+	{
+		CK(cudaStreamSynchronize(st));
+		unsigned e = 0;
+		CK(cudaMemcpy(&e, err.p, sizeof(unsigned), cudaMemcpyDeviceToHost));
+		return e ? DQMC_E_DEVICE : 0;
+	}
+
+	unsigned errors() override
+	{
+		unsigned e = 0;
+		cudaStreamSynchronize(st);
+		cudaMemcpy(&e, err.p, sizeof(unsigned), cudaMemcpyDeviceToHost);
+		return e;
+	}
+
+	int launches(int meq, int mue) override
+	{
+		const int kind = (meq ? 1 : 0) | (mue ? 2 : 0);
+		auto it = graph_launches.find(kind);
+		if (it != graph_launches.end()) return it->second;
+		return -1;
+	}
+
+	cudaStream_t stream() override { return st; }
+
+	int get_chain(int c, uint64_t *r, int *h, int *sw) override
+	{
+		if (c < 0 || c >= C) return DQMC_E_ARG;
+		CK(cudaStreamSynchronize(st));
+		if (r) CK(cudaMemcpy(r, rng.p + (size_t)c * 17, sizeof(uint64_t) * 17, cudaMemcpyDeviceToHost));
+		if (h) CK(cudaMemcpy(h, hs.p + (size_t)c * L * N, sizeof(int) * L * N, cudaMemcpyDeviceToHost));
+		if (sw) *sw = sweep;
+		return 0;
+	}
+
+	int get_acc(int c, int *eqn, void *eq, int *uen, void *uea) override
+	{
+		if (c < 0 || c >= C) return DQMC_E_ARG;
+		CK(cudaStreamSynchronize(st));
+		if (eqn) CK(cudaMemcpy(eqn, n_eq.p + c, sizeof(int), cudaMemcpyDeviceToHost));
+		if (eq) CK(cudaMemcpy(eq, acc_eq.p + (size_t)c * eq_size, sizeof(T) * eq_size, cudaMemcpyDeviceToHost));
+		if (ue_size) {
+			if (uen) CK(cudaMemcpy(uen, n_ue.p + c, sizeof(int), cudaMemcpyDeviceToHost));
+			if (uea) CK(cudaMemcpy(uea, acc_ue.p + (size_t)c * ue_size, sizeof(T) * ue_size, cudaMemcpyDeviceToHost));
+		}
+		return 0;
+	}
+
+	int get_g(int c, void *gu, void *gd, void *ph) override
+	{
+		if (c < 0 || c >= C) return DQMC_E_ARG;
+		CK(cudaStreamSynchronize(st));
+		const size_t NN = (size_t)N * N;
+		if (gu) CK(cudaMemcpy(gu, G.p + (size_t)(2 * c) * NN, sizeof(T) * NN, cudaMemcpyDeviceToHost));
+		if (gd) CK(cudaMemcpy(gd, G.p + (size_t)(2 * c + 1) * NN, sizeof(T) * NN, cudaMemcpyDeviceToHost));
+		if (ph) CK(cudaMemcpy(ph, phase.p + c, sizeof(T), cudaMemcpyDeviceToHost));
+		return 0;
+	}
+
+	int accepts(int c, long long *n) override
+	{
+		if (c < 0 || c >= C) return DQMC_E_ARG;
+		int v = 0;
+		CK(cudaStreamSynchronize(st));
+		CK(cudaMemcpy(&v, nacc.p + c, sizeof(int), cudaMemcpyDeviceToHost));
+		*n = v;
+		return 0;
+	}
+};
+
+}  // namespace dq
+
+using namespace dq;
+
+struct dqmc_engine {
+	GroupBase *g;
+	int cplx;
+};
+
+extern "C" {
+
+int dqmc_acc_sizes(const dqmc_params *p, int *eq_size, int *ue_size)
+{
+	if (!p) return DQMC_E_ARG;
+	if (eq_size) *eq_size = eq_acc_size(p->num_i, p->num_ij);
+	if (ue_size)
+		*ue_size = p->period_uneqlt > 0 ? ue_acc_size(p->num_ij, p->num_bb, p->L, p->meas_bond_corr) : 0;
+	return 0;
+}
+
+int dqmc_engine_create(const dqmc_params *p, int n_chain, int device, dqmc_engine **out)
+{
+	if (!p || !out || n_chain < 1) return DQMC_E_ARG;
+	*out = nullptr;
+	int ndev = 0;
+	if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+		fprintf(stderr, "dqmc_b200: no CUDA device\n");
+		return DQMC_E_CUDA;
+	}
+	if (device >= 0 && cudaSetDevice(device) != cudaSuccess) return DQMC_E_CUDA;
+	GroupBase *g = nullptr;
+	int rc;
+	if (p->cplx) {
+		auto *gg = new Group<zd>();
+		rc = gg->create(*p, n_chain);
+		g = gg;
+	} else {
+		auto *gg = new Group<double>();
+		rc = gg->create(*p, n_chain);
+		g = gg;
+	}
+	if (rc) {
+		delete g;
+		return rc;
+	}
+	*out = new dqmc_engine{g, p->cplx};
+	return 0;
+}
+
+void dqmc_engine_destroy(dqmc_engine *e)
+{
+	if (!e) return;
+	delete e->g;
+	delete e;
+}
+
+int dqmc_engine_set_chain(dqmc_engine *e, int chain, const double *exp_lambda, const double *del,
+		const uint64_t *rng, const int *hs, int sweep)
+{
+	if (!e || !exp_lambda || !del || !rng || !hs) return DQMC_E_ARG;
+	return e->g->set_chain(chain, exp_lambda, del, rng, hs, sweep);
+}
+
+int dqmc_engine_set_acc(dqmc_engine *e, int chain, int eq_n_sample, const void *eq_acc,
+		int ue_n_sample, const void *ue_acc)
+{
+	if (!e) return DQMC_E_ARG;
+	return e->g->set_acc(chain, eq_n_sample, eq_acc, ue_n_sample, ue_acc);
+}
+
+int dqmc_engine_init(dqmc_engine *e) { return e ? e->g->init() : DQMC_E_ARG; }
+
+int dqmc_engine_sweeps(dqmc_engine *e, int n, int sync)
+{
+	return e ? e->g->sweeps(n, sync) : DQMC_E_ARG;
+}
+
+int dqmc_engine_sync(dqmc_engine *e) { return e ? e->g->sync() : DQMC_E_ARG; }
+
+unsigned dqmc_engine_errors(dqmc_engine *e) { return e ? e->g->errors() : 0u; }
+
+int dqmc_engine_get_chain(dqmc_engine *e, int chain, uint64_t *rng, int *hs, int *sweep)
+{
+	return e ? e->g->get_chain(chain, rng, hs, sweep) : DQMC_E_ARG;
+}
+
+int dqmc_engine_get_acc(dqmc_engine *e, int chain, int *eq_n_sample, void *eq_acc,
+		int *ue_n_sample, void *ue_acc)
+{
+	return e ? e->g->get_acc(chain, eq_n_sample, eq_acc, ue_n_sample, ue_acc) : DQMC_E_ARG;
+}
+
+int dqmc_engine_get_g(dqmc_engine *e, int chain, void *gu, void *gd, void *phase)
+{
+	return e ? e->g->get_g(chain, gu, gd, phase) : DQMC_E_ARG;
+}
+
+int dqmc_engine_accepts(dqmc_engine *e, int chain, long long *n)
+{
+	return (e && n) ? e->g->accepts(chain, n) : DQMC_E_ARG;
+}
+
+void *dqmc_engine_stream(dqmc_engine *e) { return e ? (void *)e->g->stream() : nullptr; }
+
+int dqmc_engine_launches_per_sweep(dqmc_engine *e, int meas_eq, int meas_ue)
+{
+	return e ? e->g->launches(meas_eq, meas_ue) : DQMC_E_ARG;
+}
+
+int dqmc_engine_profile_sweep(dqmc_engine *e, int meas_eq, int meas_ue, double *out, int n_class)
+{
+	return (e && out && n_class > 0) ? e->g->profile(meas_eq, meas_ue, out, n_class) : DQMC_E_ARG;
+}
+
+
+}  // extern "C"
+
+// ------------------------------------------------------------ kernel seams
+
+template <typename T>
+struct Scratch {
+	std::vector<void *> ptrs;
+	~Scratch() { for (void *p : ptrs) cudaFree(p); }
+	template <typename U>
+	U *get(size_t n)
+	{
+		void *p = nullptr;
+		if (cudaMalloc(&p, sizeof(U) * (n ? n : 1)) != cudaSuccess) return nullptr;
+		ptrs.push_back(p);
+		return (U *)p;
+	}
+};
+
+template <typename T>
+static int seam_calc_eq_g(int batch, int N, int F, int l, const void *C, void *G, void *phase,
+		cudaStream_t st)
+{
+	if (batch < 1 || N < 1 || N > max_dense_n<T>() || F < 1 || l < 0 || l >= F || !C || !G || !phase)
+		return DQMC_E_ARG;
+	const size_t NN = (size_t)N * N;
+	Scratch<T> sc;
+	EqWork<T> w;
+	w.N = N; w.F = F; w.NB = batch;
+	w.Cl = (const T *)C; w.cl_stride = (long long)F * NN;
+	w.Qm = sc.template get<T>(batch * NN); w.Tm = sc.template get<T>(batch * NN);
+	w.Tm2 = sc.template get<T>(batch * NN); w.Rs = sc.template get<T>(batch * NN);
+	w.X = sc.template get<T>(batch * NN); w.W = sc.template get<T>(batch * NN);
+	w.dR = sc.template get<double>((size_t)batch * N); w.pvt = sc.template get<int>((size_t)batch * N);
+	w.qdet = sc.template get<T>(batch);
+	w.G = (T *)G; w.g_stride = NN;
+	w.phi = (T *)phase;
+	w.err = sc.template get<unsigned>(1);
+	if (!w.Qm || !w.Tm || !w.Tm2 || !w.Rs || !w.X || !w.W || !w.dR || !w.pvt || !w.qdet || !w.err)
+		return DQMC_E_NOMEM;
+	CK(cudaMemsetAsync(w.err, 0, sizeof(unsigned), st));
+	int rc = run_calc_eq_g<T>(w, l, st, nullptr);
+	if (rc) return rc;
+	unsigned e = 0;
+	CK(cudaMemcpyAsync(&e, w.err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+	CK(cudaStreamSynchronize(st));
+	CK(cudaGetLastError());
+	return e ? DQMC_E_DEVICE : 0;
+}
+
+template <typename T>
+static int seam_update(int batch, int N, int n_delay, const double *del, uint64_t *rng, int *hs,
+		void *G, void *phase, cudaStream_t st)
+{
+	if (batch < 1 || N < 1 || N > 512 || n_delay < 1 || !del || !rng || !hs || !G || !phase)
+		return DQMC_E_ARG;
+	int kd = n_delay;
+	const int ldp = (N + 15) / 16 * 16 + 4;
+	while (kd > 1 && update_smem_bytes<T>(N, kd, ldp) > 200 * 1024) kd /= 2;
+	CK(cudaFuncSetAttribute(k_update<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+	                        (int)update_smem_bytes<T>(N, kd, ldp)));
+	UpdArgs<T> a;
+	memset(&a, 0, sizeof(a));
+	a.N = N; a.L = 1; a.n_delay = kd; a.nchain = batch; a.slice = 0; a.ldp = ldp;
+	a.del = del; a.rng = rng; a.hs = hs; a.G = (T *)G; a.phase = (T *)phase;
+	const int np = (N + 31) / 32 * 32;
+	k_update<T><<<batch, 2 * np, update_smem_bytes<T>(N, kd, ldp), st>>>(a);
+	CK(cudaGetLastError());
+	CK(cudaStreamSynchronize(st));
+	return 0;
+}
+
+template <typename T>
+static int seam_mul_seq(int batch, int N, int n, int spin, const void *expK, const double *el,
+		const int *hs, void *C, cudaStream_t st)
+{
+	if (batch < 1 || N < 1 || n < 1 || (spin != 0 && spin != 1) || !expK || !el || !hs || !C)
+		return DQMC_E_ARG;
+	const size_t NN = (size_t)N * N;
+	Scratch<T> sc;
+	double *dv = sc.template get<double>((size_t)batch * n * N);
+	double *dvi = sc.template get<double>((size_t)batch * n * N);
+	T *X = sc.template get<T>(batch * NN), *W = sc.template get<T>(batch * NN);
+	if (!dv || !dvi || !X || !W) return DQMC_E_NOMEM;
+	// the d_l of the requested spin only: k_diag_all writes both spins of
+	// each chain, so run it with spin-major strides and keep spin `spin`
+	double *dv2 = sc.template get<double>((size_t)batch * 2 * n * N);
+	double *dvi2 = sc.template get<double>((size_t)batch * 2 * n * N);
+	if (!dv2 || !dvi2) return DQMC_E_NOMEM;
+	k_diag_all<<<grid_for((long long)batch * 2 * n * N), 256, 0, st>>>(N, n, batch, el, hs, dv2, dvi2);
+	run_mul_seq<T>(N, n, batch, (const T *)expK, Addr{0, 0, 1}, dv2 + (size_t)spin * n * N,
+	               2LL * n * N, (T *)C, Addr{(long long)NN, 0, 1}, X, W, st, nullptr);
+	CK(cudaGetLastError());
+	CK(cudaStreamSynchronize(st));
+	return 0;
+}
+
+extern "C" {
+
+int dqmc_gpu_calc_eq_g(int batch, int N, int F, int l, int cplx, const void *C, void *G,
+		void *phase, void *stream)
+{
+	cudaStream_t st = (cudaStream_t)stream;
+	return cplx ? seam_calc_eq_g<zd>(batch, N, F, l, C, G, phase, st)
+	            : seam_calc_eq_g<double>(batch, N, F, l, C, G, phase, st);
+}
+
+int dqmc_gpu_update_delayed(int batch, int N, int n_delay, int cplx, const double *del,
+		uint64_t *rng, int *hs, void *G, void *phase, void *stream)
+{
+	cudaStream_t st = (cudaStream_t)stream;
+	return cplx ? seam_update<zd>(batch, N, n_delay, del, rng, hs, G, phase, st)
+	            : seam_update<double>(batch, N, n_delay, del, rng, hs, G, phase, st);
+}
+
+int dqmc_gpu_mul_seq(int batch, int N, int n, int spin, int cplx, const void *exp_K,
+		const double *exp_lambda, const int *hs, void *C, void *stream)
+{
+	cudaStream_t st = (cudaStream_t)stream;
+	return cplx ? seam_mul_seq<zd>(batch, N, n, spin, exp_K, exp_lambda, hs, C, st)
+	            : seam_mul_seq<double>(batch, N, n, spin, exp_K, exp_lambda, hs, C, st);
+}
+
+}  // extern "C"

@@ -1,0 +1,627 @@
+/*
+ * Host lifecycle of a simulation: the drop-in dqmc_wrapper and its batched
+ * form.  Follows the reference's src/dqmc.c:525-671 (dqmc_wrapper), with
+ * the signal/time-limit handling of src/sig.c, the checkpoint cadence of
+ * dqmc.c:233-244, the data layer of src/data.c:345-789 (read, save with the
+ * partial_write guard) and a profile table in the spirit of src/prof.c.
+ * The sweeps themselves run on the GPU through the engine (engine.cu).
+ */
+#define _GNU_SOURCE
+#include <math.h>
+#include <signal.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <sys/stat.h>
+#include <time.h>
+
+#include "dqmc_b200.h"
+#include "simfile.h"
+
+#ifndef DQMC_GIT_ID
+#define DQMC_GIT_ID "dqmc-b200"
+#endif
+#define DQMC_REPO "dqmc-b200"
+
+#define WRAP_FAIL -1
+#define WRAP_INCOMPLETE 1
+
+/* ----------------------------------------------------------- time, signals */
+
+static int64_t time_wall(void)
+{
+	struct timespec t;
+	clock_gettime(CLOCK_MONOTONIC, &t);
+	return (int64_t)t.tv_sec * 1000000000LL + t.tv_nsec;
+}
+
+/* sig.c:7-59: SIGUSR1/INT/TERM/HUP set a stop flag checked once per sweep */
+static volatile sig_atomic_t stop_flag = 0;
+static void on_stop(int signum) { stop_flag = signum; }
+
+static void sig_init(void)
+{
+	static int called = 0;
+	if (called) return;
+	called = 1;
+	struct sigaction sa;
+	memset(&sa, 0, sizeof(sa));
+	sa.sa_handler = on_stop;
+	sigaction(SIGUSR1, &sa, NULL);
+	sigaction(SIGINT, &sa, NULL);
+	sigaction(SIGTERM, &sa, NULL);
+	sigaction(SIGHUP, &sa, NULL);
+}
+
+struct stopper {
+	FILE *log;
+	int64_t wall_start, max_time, t_first;
+	int first;
+};
+
+/* sig.c:70-127: -1 when max_time is reached, the signal number on a signal */
+static int check_stop(struct stopper *s, int sweep, int n_sweep_warm, int n_sweep)
+{
+	const int64_t now = time_wall();
+	if (s->max_time > 0 && now >= s->wall_start + s->max_time * 1000000000LL) stop_flag = -1;
+	if (s->t_first == 0) {
+		s->first = sweep;
+		s->t_first = now;
+	}
+	if (stop_flag) {
+		const double el = (now - s->wall_start) * 1e-9;
+		const double done = (now - s->t_first) * 1e-9;
+		const int sd = sweep - s->first;
+		const double left = sd > 0 ? done / sd * (n_sweep - sweep) : 0.0;
+		fprintf(s->log, "%d/%d sweeps completed (%s)\n", sweep, n_sweep,
+		        sweep >= n_sweep_warm ? "measuring" : "warming up");
+		fprintf(s->log, "\telapsed: %.3f%c\n", el < 3600 ? el : el / 3600, el < 3600 ? 's' : 'h');
+		fprintf(s->log, "\tremaining%s: %.3f%c\n",
+		        (s->first < n_sweep_warm) ? " (ignoring measurement cost)" : "",
+		        left < 3600 ? left : left / 3600, left < 3600 ? 's' : 'h');
+		fprintf(s->log, "stop_flag = %d, stopping\n", (int)stop_flag);
+		fflush(s->log);
+	}
+	if (sweep == n_sweep_warm) {
+		s->first = sweep;
+		s->t_first = now;
+	}
+	return stop_flag;
+}
+
+/* ------------------------------------------------------------- profiling */
+
+enum { PR_WALL, PR_READ, PR_INIT, PR_SWEEPS, PR_CHECKPOINT, PR_SAVE, PR_N };
+static const char *pr_name[PR_N] = {"wall", "read", "init_g", "sweeps", "checkpoint", "save"};
+struct prof {
+	int64_t t[PR_N];
+	int n[PR_N];
+};
+
+static void prof_print(FILE *log, const struct prof *p)
+{
+	fprintf(log, "region___________|_%% of all_|___total (s)_|___us per call_|___# calls\n");
+	for (int i = 0; i < PR_N; i++) {
+		if (!p->n[i]) continue;
+		fprintf(log, "%16s |%9.3f |%12.3f |%14.3f |%10d\n", pr_name[i],
+		        100.0 * p->t[i] / (p->t[PR_WALL] ? p->t[PR_WALL] : 1), p->t[i] * 1e-9,
+		        1e-3 * p->t[i] / p->n[i], p->n[i]);
+	}
+	fprintf(log, "---------------------------------------------------------------------\n");
+}
+
+/* ------------------------------------------------------------- sim data */
+
+struct sim {
+	const char *file;
+	dqmc_params p;
+	int cplx, n_sweep_meas, checkpoint_every, num_b_alloc;
+	int *map_i, *map_ij, *bonds, *map_bb;
+	double *peierlsu, *peierlsd;
+	double *mats[8];
+	double *exp_lambda, *del;
+	uint64_t rng[17];
+	int sweep;
+	int *hs;
+	int eq_n, ue_n;
+	double *eq_acc, *ue_acc;      /* num arrays in the engine's layout */
+	int eq_size, ue_size;
+};
+
+static const char *mat_names[8] = {
+	"params/exp_Ku", "params/exp_Kd", "params/inv_exp_Ku", "params/inv_exp_Kd",
+	"params/exp_halfKu", "params/exp_halfKd", "params/inv_exp_halfKu", "params/inv_exp_halfKd"};
+
+static const char *eq_i_names[4] = {"density", "density_u", "density_d", "double_occ"};
+static const char *eq_ij_names[7] = {"g00", "g00_u", "g00_d", "nn", "xx", "zz", "pair_sw"};
+static const char *ue_ij_names[7] = {"gt0", "gt0_u", "gt0_d", "nn", "xx", "zz", "pair_sw"};
+static const char *ue_bb_names[5] = {"pair_bb", "jj", "jsjs", "kk", "ksks"};
+
+static void sim_free(struct sim *s)
+{
+	free(s->map_i); free(s->map_ij); free(s->bonds); free(s->map_bb);
+	free(s->peierlsu); free(s->peierlsd);
+	for (int i = 0; i < 8; i++) free(s->mats[i]);
+	free(s->exp_lambda); free(s->del); free(s->hs);
+	free(s->eq_acc); free(s->ue_acc);
+	memset(s, 0, sizeof(*s));
+}
+
+static int rd_num(dqsf_file *f, const char *name, double *dst, size_t n, int cplx)
+{
+	return cplx ? dqsf_read_c128(f, name, dst, n) : dqsf_read_f64(f, name, dst, n);
+}
+
+static int wr_num(dqsf_file *f, const char *name, const double *src, size_t n, int cplx)
+{
+	return cplx ? dqsf_write_c128(f, name, src, n) : dqsf_write_f64(f, name, src, n);
+}
+
+#define TRY(x) do { int rc_ = (x); if (rc_) { dqsf_close(f); sim_free(s); return rc_ < 0 ? rc_ : DQSF_RW_FAIL; } } while (0)
+
+/* data.c:345-658 for the datasets this engine carries */
+static int sim_read(struct sim *s)
+{
+	dqsf_file *f;
+	int rc = dqsf_open(s->file, 0, &f);
+	if (rc) return rc;
+	int pw = 0;
+	TRY(dqsf_read_int(f, "state/partial_write", &pw, 1));
+	if (pw) {
+		fprintf(stderr, "Last checkpoint in %s contained partial write\n", s->file);
+		dqsf_close(f);
+		return DQSF_CORRUPT_FAIL;
+	}
+	dqmc_params *p = &s->p;
+	struct { const char *n; int *d; } sc[] = {
+		{"params/N", &p->N}, {"params/L", &p->L}, {"params/n_matmul", &p->n_matmul},
+		{"params/n_delay", &p->n_delay}, {"params/F", &p->F},
+		{"params/n_sweep_warm", &p->n_sweep_warm}, {"params/n_sweep", &p->n_sweep},
+		{"params/n_sweep_meas", &s->n_sweep_meas},
+		{"params/period_eqlt", &p->period_eqlt}, {"params/period_uneqlt", &p->period_uneqlt},
+		{"params/meas_bond_corr", &p->meas_bond_corr}, {"params/num_i", &p->num_i},
+		{"params/num_ij", &p->num_ij}, {"params/num_b", &p->num_b}, {"params/num_bb", &p->num_bb},
+		{"params/degen_i", &p->degen_i}, {"params/degen_ij", &p->degen_ij},
+		{"params/degen_bb", &p->degen_bb}, {"params/checkpoint_every", &s->checkpoint_every},
+		{"state/sweep", &s->sweep},
+	};
+	for (size_t i = 0; i < sizeof(sc) / sizeof(sc[0]); i++) TRY(dqsf_read_int(f, sc[i].n, sc[i].d, 1));
+	/* toggles this engine does not carry are refused, as a reference build
+	 * without them would mis-read the file */
+	const char *unsupported[] = {"params/meas_thermal", "params/meas_2bond_corr",
+		"params/meas_energy_corr", "params/meas_nematic_corr", "params/meas_chiral",
+		"params/meas_local_JQ", "params/meas_gen_suscept", "params/meas_pair_bb_only"};
+	for (size_t i = 0; i < sizeof(unsupported) / sizeof(unsupported[0]); i++) {
+		int v = 0;
+		if (dqsf_has(f, unsupported[i])) TRY(dqsf_read_int(f, unsupported[i], &v, 1));
+		if (v) {
+			fprintf(stderr, "%s = %d is not supported by this engine\n", unsupported[i], v);
+			dqsf_close(f);
+			sim_free(s);
+			return DQSF_RW_FAIL;
+		}
+	}
+	int dt;
+	size_t cnt;
+	TRY(dqsf_info(f, "params/exp_Ku", &dt, &cnt));
+	s->cplx = p->cplx = (dt == DQSF_C128);
+	const size_t N = p->N, L = p->L, NN = N * N, w = s->cplx ? 2 : 1;
+	s->map_i = calloc(N, sizeof(int));
+	s->map_ij = calloc(NN, sizeof(int));
+	TRY(dqsf_read_int(f, "params/map_i", s->map_i, N));
+	TRY(dqsf_read_int(f, "params/map_ij", s->map_ij, NN));
+	s->num_b_alloc = p->num_b > 0 ? p->num_b : 1;
+	s->bonds = calloc(2 * (size_t)s->num_b_alloc, sizeof(int));
+	s->map_bb = calloc((size_t)s->num_b_alloc * s->num_b_alloc, sizeof(int));
+	if (p->meas_bond_corr && p->num_b > 0) {
+		TRY(dqsf_read_int(f, "params/bonds", s->bonds, 2 * (size_t)p->num_b));
+		TRY(dqsf_read_int(f, "params/map_bb", s->map_bb, (size_t)p->num_b * p->num_b));
+	}
+	s->peierlsu = calloc(NN * w, sizeof(double));
+	s->peierlsd = calloc(NN * w, sizeof(double));
+	TRY(rd_num(f, "params/peierlsu", s->peierlsu, NN, s->cplx));
+	TRY(rd_num(f, "params/peierlsd", s->peierlsd, NN, s->cplx));
+	for (int i = 0; i < 8; i++) {
+		s->mats[i] = calloc(NN * w, sizeof(double));
+		TRY(rd_num(f, mat_names[i], s->mats[i], NN, s->cplx));
+	}
+	s->exp_lambda = calloc(2 * N, sizeof(double));
+	s->del = calloc(2 * N, sizeof(double));
+	TRY(dqsf_read_f64(f, "params/exp_lambda", s->exp_lambda, 2 * N));
+	TRY(dqsf_read_f64(f, "params/del", s->del, 2 * N));
+	TRY(dqsf_read_u64(f, "state/rng", s->rng, 17));
+	s->hs = calloc(N * L, sizeof(int));
+	TRY(dqsf_read_int(f, "state/hs", s->hs, N * L));
+	p->map_i = s->map_i; p->map_ij = s->map_ij; p->bonds = s->bonds; p->map_bb = s->map_bb;
+	p->peierlsu = s->peierlsu; p->peierlsd = s->peierlsd;
+	p->exp_Ku = s->mats[0]; p->exp_Kd = s->mats[1]; p->inv_exp_Ku = s->mats[2];
+	p->inv_exp_Kd = s->mats[3]; p->exp_halfKu = s->mats[4]; p->exp_halfKd = s->mats[5];
+	p->inv_exp_halfKu = s->mats[6]; p->inv_exp_halfKd = s->mats[7];
+	dqmc_acc_sizes(p, &s->eq_size, &s->ue_size);
+	s->eq_acc = calloc((size_t)s->eq_size * w, sizeof(double));
+	s->ue_acc = calloc((size_t)(s->ue_size ? s->ue_size : 1) * w, sizeof(double));
+	char name[128];
+	const size_t ni = p->num_i, nij = p->num_ij, nbb = p->num_bb;
+	TRY(dqsf_read_int(f, "meas_eqlt/n_sample", &s->eq_n, 1));
+	TRY(rd_num(f, "meas_eqlt/sign", s->eq_acc, 1, s->cplx));
+	for (int k = 0; k < 4; k++) {
+		snprintf(name, sizeof(name), "meas_eqlt/%s", eq_i_names[k]);
+		TRY(rd_num(f, name, s->eq_acc + w * (1 + k * ni), ni, s->cplx));
+	}
+	for (int k = 0; k < 7; k++) {
+		snprintf(name, sizeof(name), "meas_eqlt/%s", eq_ij_names[k]);
+		TRY(rd_num(f, name, s->eq_acc + w * (1 + 4 * ni + k * nij), nij, s->cplx));
+	}
+	if (p->period_uneqlt > 0) {
+		TRY(dqsf_read_int(f, "meas_uneqlt/n_sample", &s->ue_n, 1));
+		TRY(rd_num(f, "meas_uneqlt/sign", s->ue_acc, 1, s->cplx));
+		for (int k = 0; k < 7; k++) {
+			snprintf(name, sizeof(name), "meas_uneqlt/%s", ue_ij_names[k]);
+			TRY(rd_num(f, name, s->ue_acc + w * (1 + k * nij * L), nij * L, s->cplx));
+		}
+		if (p->meas_bond_corr)
+			for (int k = 0; k < 5; k++) {
+				snprintf(name, sizeof(name), "meas_uneqlt/%s", ue_bb_names[k]);
+				TRY(rd_num(f, name, s->ue_acc + w * (1 + 7 * nij * L + k * nbb * L), nbb * L, s->cplx));
+			}
+	}
+	return dqsf_close(f);
+}
+
+#undef TRY
+#define TRYW(x) do { if ((x) != 0) { dqsf_close(f); return DQSF_RW_FAIL; } } while (0)
+
+/* data.c:667-789: partial_write set, state and accumulators, partial_write clear */
+static int sim_save(const struct sim *s)
+{
+	dqsf_file *f;
+	int rc = dqsf_open(s->file, 1, &f);
+	if (rc) return rc;
+	int pw = 0;
+	TRYW(dqsf_read_int(f, "state/partial_write", &pw, 1));
+	if (pw) {
+		dqsf_close(f);
+		return DQSF_CORRUPT_FAIL;
+	}
+	pw = 1;
+	TRYW(dqsf_write_int(f, "state/partial_write", &pw, 1));
+	fflush(NULL);
+	const dqmc_params *p = &s->p;
+	const size_t L = p->L, w = s->cplx ? 2 : 1;
+	const size_t ni = p->num_i, nij = p->num_ij, nbb = p->num_bb;
+	char name[128];
+	TRYW(dqsf_write_u64(f, "state/rng", s->rng, 17));
+	TRYW(dqsf_write_int(f, "state/sweep", &s->sweep, 1));
+	TRYW(dqsf_write_int(f, "state/hs", s->hs, (size_t)p->N * L));
+	TRYW(dqsf_write_int(f, "meas_eqlt/n_sample", &s->eq_n, 1));
+	TRYW(wr_num(f, "meas_eqlt/sign", s->eq_acc, 1, s->cplx));
+	for (int k = 0; k < 4; k++) {
+		snprintf(name, sizeof(name), "meas_eqlt/%s", eq_i_names[k]);
+		TRYW(wr_num(f, name, s->eq_acc + w * (1 + k * ni), ni, s->cplx));
+	}
+	for (int k = 0; k < 7; k++) {
+		snprintf(name, sizeof(name), "meas_eqlt/%s", eq_ij_names[k]);
+		TRYW(wr_num(f, name, s->eq_acc + w * (1 + 4 * ni + k * nij), nij, s->cplx));
+	}
+	if (p->period_uneqlt > 0) {
+		TRYW(dqsf_write_int(f, "meas_uneqlt/n_sample", &s->ue_n, 1));
+		TRYW(wr_num(f, "meas_uneqlt/sign", s->ue_acc, 1, s->cplx));
+		for (int k = 0; k < 7; k++) {
+			snprintf(name, sizeof(name), "meas_uneqlt/%s", ue_ij_names[k]);
+			TRYW(wr_num(f, name, s->ue_acc + w * (1 + k * nij * L), nij * L, s->cplx));
+		}
+		if (p->meas_bond_corr)
+			for (int k = 0; k < 5; k++) {
+				snprintf(name, sizeof(name), "meas_uneqlt/%s", ue_bb_names[k]);
+				TRYW(wr_num(f, name, s->ue_acc + w * (1 + 7 * nij * L + k * nbb * L), nbb * L, s->cplx));
+			}
+	}
+	fflush(NULL);
+	pw = 0;
+	TRYW(dqsf_write_int(f, "state/partial_write", &pw, 1));
+	return dqsf_close(f);
+}
+
+#undef TRYW
+
+/* data.c:69-99 */
+static int consistency_check(const char *file, FILE *log)
+{
+	dqsf_file *f;
+	if (dqsf_open(file, 0, &f) != 0) return DQSF_OPEN_FAIL;
+	char commit[256] = "";
+	int rc = dqsf_read_str(f, "metadata/commit", commit, sizeof(commit));
+	dqsf_close(f);
+	if (rc) return rc;
+	fprintf(log, "hdf5 generation script commit id %s\n", commit);
+	return strcmp(commit, DQMC_GIT_ID);
+}
+
+/* estimate of the device memory one chain of this file needs */
+static long long memory_req(const char *file)
+{
+	dqsf_file *f;
+	if (dqsf_open(file, 0, &f) != 0) return DQSF_OPEN_FAIL;
+	int N = 0, L = 0, F = 0, pu = 0, dt = 0;
+	size_t cnt;
+	if (dqsf_read_int(f, "params/N", &N, 1) || dqsf_read_int(f, "params/L", &L, 1) ||
+	    dqsf_read_int(f, "params/F", &F, 1) || dqsf_read_int(f, "params/period_uneqlt", &pu, 1) ||
+	    dqsf_info(f, "params/exp_Ku", &dt, &cnt)) {
+		dqsf_close(f);
+		return DQSF_RW_FAIL;
+	}
+	dqsf_close(f);
+	const long long sz = dt == DQSF_C128 ? 16 : 8, NN = (long long)N * N;
+	long long mats = 2 * (F + 9) * NN + 8 * NN;
+	if (pu > 0) mats += 6 * (long long)L * NN + 4 * (long long)(F + 2) * (F + 2) * NN;
+	return sz * mats + 4LL * L * N * 5;
+}
+
+/* ---------------------------------------------------------------- engine */
+
+static int engine_from(struct sim **sims, int n, dqmc_engine **out)
+{
+	int rc = dqmc_engine_create(&sims[0]->p, n, 0, out);
+	if (rc) return rc;
+	for (int c = 0; c < n; c++) {
+		struct sim *s = sims[c];
+		rc = dqmc_engine_set_chain(*out, c, s->exp_lambda, s->del, s->rng, s->hs, s->sweep);
+		if (!rc) rc = dqmc_engine_set_acc(*out, c, s->eq_n, s->eq_acc, s->ue_n, s->ue_acc);
+		if (rc) return rc;
+	}
+	return dqmc_engine_init(*out);
+}
+
+static int engine_pull(dqmc_engine *e, struct sim **sims, int n)
+{
+	for (int c = 0; c < n; c++) {
+		struct sim *s = sims[c];
+		int rc = dqmc_engine_get_chain(e, c, s->rng, s->hs, &s->sweep);
+		if (!rc) rc = dqmc_engine_get_acc(e, c, &s->eq_n, s->eq_acc, &s->ue_n, s->ue_acc);
+		if (rc) return rc;
+	}
+	return 0;
+}
+
+/* dqmc.c:222-244: per sweep, stop check then checkpoint then the sweep.
+ * Returns 0 (done), 5 (interrupted) or 6 (checkpoint failed), or < 0. */
+static int run_group(dqmc_engine *e, struct sim **sims, int n, struct stopper *stp,
+		struct prof *pr)
+{
+	const dqmc_params *p = &sims[0]->p;
+	int sweep = sims[0]->sweep;
+	while (sweep < p->n_sweep) {
+		if (check_stop(stp, sweep, p->n_sweep_warm, p->n_sweep)) return 5;
+		const int ce = sims[0]->checkpoint_every;
+		if (ce > 0 && sweep % ce == 0) {
+			const int64_t t0 = time_wall();
+			int rc = engine_pull(e, sims, n);
+			for (int c = 0; rc == 0 && c < n; c++) rc = sim_save(sims[c]);
+			pr->t[PR_CHECKPOINT] += time_wall() - t0;
+			pr->n[PR_CHECKPOINT]++;
+			if (rc) return 6;
+		}
+		const int64_t t0 = time_wall();
+		int rc = dqmc_engine_sweeps(e, 1, 1);
+		pr->t[PR_SWEEPS] += time_wall() - t0;
+		pr->n[PR_SWEEPS]++;
+		if (rc) return rc;
+		sweep++;
+	}
+	return engine_pull(e, sims, n);
+}
+
+static FILE *open_log(const char *log_file)
+{
+	return log_file ? fopen(log_file, "a") : stdout;
+}
+
+static void log_header(FILE *log, const char *sim_file)
+{
+	fprintf(log, "executable commit id %s from repo %s\n", DQMC_GIT_ID, DQMC_REPO);
+	fprintf(log, "compiled on %s %s\n", __DATE__, __TIME__);
+	fprintf(log, "hdf5 and executable versions consistent? %s\n",
+	        consistency_check(sim_file, log) ? "No" : "Yes");
+	fprintf(log, "integer size on this system: %zu bytes\n", sizeof(int));
+	fprintf(log, "measurements on the GPU (sm_100a engine)\n");
+	const long long mem = memory_req(sim_file);
+	if (mem < 0) fprintf(log, "minimum RAM check failed: %lld\n", mem);
+	else fprintf(log, "minimum device memory requirement: %.2f MB\n", mem * 1e-6);
+}
+
+int dqmc_wrapper(const char *sim_file, const char *log_file, const int64_t max_time,
+		const bool dry, const bool bench)
+{
+	const int64_t wall_start = time_wall();
+	struct prof pr;
+	memset(&pr, 0, sizeof(pr));
+	FILE *log = open_log(log_file);
+	if (log == NULL) {
+		fprintf(stderr, "fopen() failed to open: %s\n", log_file);
+		return WRAP_FAIL;
+	}
+	log_header(log, sim_file);
+	if (dry) {
+		fprintf(log, "toggled dry run for mem check only\n");
+		fprintf(log, "Not performing: read sim file, alloc mem, run core DQMC logic, or save data\n");
+		if (log != stdout) fclose(log); else fflush(log);
+		return 0;
+	}
+	sig_init();
+	struct stopper stp = {log, wall_start, max_time, 0, 0};
+	int ret = 0;
+	struct sim s;
+	memset(&s, 0, sizeof(s));
+	s.file = sim_file;
+	fprintf(log, "opening %s\n", sim_file);
+	struct stat info;
+	if (stat(sim_file, &info) == 0)
+		fprintf(log, "size of this hdf5 file: %.2f MB\n", ((double)info.st_size) * 1e-6);
+	fflush(log);
+	int64_t t0 = time_wall();
+	const int rs = sim_read(&s);
+	pr.t[PR_READ] += time_wall() - t0;
+	pr.n[PR_READ]++;
+	dqmc_engine *e = NULL;
+	if (rs) {
+		fprintf(log, "sim_data_read_alloc() failed: %d\n", rs);
+		ret = WRAP_FAIL;
+		goto cleanup;
+	}
+	if (s.checkpoint_every) fprintf(log, "checkpointing every %d sweeps\n", s.checkpoint_every);
+	else fprintf(log, "warning: running with no checkpoints\n");
+	fprintf(log, "%d/%d sweeps completed\n", s.sweep, s.p.n_sweep);
+	if (s.sweep >= s.p.n_sweep) {
+		fprintf(log, "already finished so don't do anything\n");
+		goto cleanup;
+	}
+	time_t now;
+	time(&now);
+	fprintf(log, "[%.24s] starting dqmc\n", ctime(&now));
+	fflush(log);
+	t0 = time_wall();
+	struct sim *one[1] = {&s};
+	int rc = engine_from(one, 1, &e);
+	pr.t[PR_INIT] += time_wall() - t0;
+	pr.n[PR_INIT]++;
+	if (rc) {
+		fprintf(log, "engine setup failed: %d\n", rc);
+		ret = WRAP_FAIL;
+		goto cleanup;
+	}
+	rc = run_group(e, one, 1, &stp, &pr);
+	if (rc == 5) {
+		fprintf(log, "dqmc() interrupted\n");
+		ret = WRAP_INCOMPLETE;
+		goto cleanup;
+	} else if (rc == 6) {
+		fprintf(log, "dqmc() checkpoint failed\n");
+		ret = WRAP_FAIL;
+		goto cleanup;
+	} else if (rc) {
+		fprintf(log, "dqmc() failed on the device: %d (errors 0x%x)\n", rc, dqmc_engine_errors(e));
+		ret = WRAP_FAIL;
+		goto cleanup;
+	}
+	time(&now);
+	fprintf(log, "[%.24s] %d/%d sweeps completed\n", ctime(&now), s.sweep, s.p.n_sweep);
+	if (bench) {
+		fprintf(log, "benchmark mode enabled; not saving data to disk\n");
+		goto cleanup;
+	}
+	fprintf(log, "saving data to disk\n");
+	t0 = time_wall();
+	rc = sim_save(&s);
+	pr.t[PR_SAVE] += time_wall() - t0;
+	pr.n[PR_SAVE]++;
+	if (rc < 0) {
+		fprintf(log, "sim_data_save() failed: %d\n", rc);
+		ret = WRAP_FAIL;
+		goto cleanup;
+	}
+	fprintf(log, "sim_data_save() succeeded\n");
+cleanup:
+	dqmc_engine_destroy(e);
+	sim_free(&s);
+	pr.t[PR_WALL] = time_wall() - wall_start;
+	pr.n[PR_WALL] = 1;
+	fprintf(log, "wall time: %.3f\n", pr.t[PR_WALL] * 1e-9);
+	prof_print(log, &pr);
+	if (log != stdout) fclose(log); else fflush(log);
+	return ret;
+}
+
+/* files whose parameter sets are byte-identical and whose sweep counters
+ * agree can share an engine */
+static int same_group(const struct sim *a, const struct sim *b)
+{
+	const dqmc_params *p = &a->p, *q = &b->p;
+	if (memcmp(&p->N, &q->N, sizeof(int) * 18) != 0 || a->sweep != b->sweep ||
+	    a->checkpoint_every != b->checkpoint_every)
+		return 0;
+	const size_t NN = (size_t)p->N * p->N, w = a->cplx ? 2 : 1;
+	for (int i = 0; i < 8; i++)
+		if (memcmp(a->mats[i], b->mats[i], NN * w * sizeof(double))) return 0;
+	if (memcmp(a->map_ij, b->map_ij, NN * sizeof(int)) || memcmp(a->map_i, b->map_i, p->N * sizeof(int)))
+		return 0;
+	if (memcmp(a->peierlsu, b->peierlsu, NN * w * sizeof(double))) return 0;
+	return 1;
+}
+
+int dqmc_wrapper_batch(int n_files, const char *const *sim_files, const char *log_file,
+		const int64_t max_time, const bool bench, int *status)
+{
+	if (n_files < 1 || !sim_files || !status) return WRAP_FAIL;
+	const int64_t wall_start = time_wall();
+	struct prof pr;
+	memset(&pr, 0, sizeof(pr));
+	FILE *log = open_log(log_file);
+	if (!log) return WRAP_FAIL;
+	sig_init();
+	struct stopper stp = {log, wall_start, max_time, 0, 0};
+	struct sim *sims = calloc(n_files, sizeof(struct sim));
+	int *group = calloc(n_files, sizeof(int));
+	int worst = 0;
+	for (int i = 0; i < n_files; i++) {
+		sims[i].file = sim_files[i];
+		status[i] = 0;
+		group[i] = -1;
+		const int rc = sim_read(&sims[i]);
+		if (rc) {
+			fprintf(log, "%s: read failed: %d\n", sim_files[i], rc);
+			status[i] = WRAP_FAIL;
+		}
+	}
+	/* group the readable, unfinished files */
+	int ng = 0;
+	for (int i = 0; i < n_files; i++) {
+		if (status[i] || group[i] >= 0) continue;
+		if (sims[i].sweep >= sims[i].p.n_sweep) continue;
+		group[i] = ng;
+		for (int j = i + 1; j < n_files; j++)
+			if (!status[j] && group[j] < 0 && same_group(&sims[i], &sims[j])) group[j] = ng;
+		ng++;
+	}
+	fprintf(log, "%d files in %d parameter groups\n", n_files, ng);
+	for (int gi = 0; gi < ng; gi++) {
+		int n = 0;
+		for (int i = 0; i < n_files; i++) n += group[i] == gi;
+		struct sim **members = calloc(n, sizeof(struct sim *));
+		int *idx = calloc(n, sizeof(int));
+		n = 0;
+		for (int i = 0; i < n_files; i++)
+			if (group[i] == gi) { idx[n] = i; members[n++] = &sims[i]; }
+		dqmc_engine *e = NULL;
+		int64_t t0 = time_wall();
+		int rc = engine_from(members, n, &e);
+		pr.t[PR_INIT] += time_wall() - t0;
+		pr.n[PR_INIT]++;
+		if (!rc) rc = run_group(e, members, n, &stp, &pr);
+		int st = 0;
+		if (rc == 5) st = WRAP_INCOMPLETE;
+		else if (rc) st = WRAP_FAIL;
+		if (st == 0 && !bench)
+			for (int k = 0; k < n; k++)
+				if (sim_save(members[k]) < 0) status[idx[k]] = WRAP_FAIL;
+		for (int k = 0; k < n; k++)
+			if (!status[idx[k]]) status[idx[k]] = st;
+		fprintf(log, "group %d: %d chains, status %d\n", gi, n, st);
+		dqmc_engine_destroy(e);
+		free(members);
+		free(idx);
+	}
+	for (int i = 0; i < n_files; i++) {
+		if (status[i] == WRAP_FAIL) worst = WRAP_FAIL;
+		else if (status[i] == WRAP_INCOMPLETE && worst == 0) worst = WRAP_INCOMPLETE;
+		sim_free(&sims[i]);
+	}
+	free(sims);
+	free(group);
+	pr.t[PR_WALL] = time_wall() - wall_start;
+	pr.n[PR_WALL] = 1;
+	fprintf(log, "wall time: %.3f\n", pr.t[PR_WALL] * 1e-9);
+	prof_print(log, &pr);
+	if (log != stdout) fclose(log); else fflush(log);
+	return worst;
+}

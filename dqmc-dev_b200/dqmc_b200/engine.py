@@ -1,0 +1,226 @@
+"""Python front end of the GPU engine: sim files in, chains advanced on the
+GPU through the C ABI, state and measurements back out.
+
+Mirrors what the reference's data layer and driver do for one file
+(src/data.c:345-789, src/dqmc.c:84-511) for any number of files that share a
+parameter set; the arithmetic all happens in libdqmc_b200.so.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import lib as _lib
+from . import simfile
+
+EQ_I = ["density", "density_u", "density_d", "double_occ"]
+EQ_IJ = ["g00", "g00_u", "g00_d", "nn", "xx", "zz", "pair_sw"]
+UE_IJ = ["gt0", "gt0_u", "gt0_d", "nn", "xx", "zz", "pair_sw"]
+UE_BB = ["pair_bb", "jj", "jsjs", "kk", "ksks"]
+MATS = ["exp_Ku", "exp_Kd", "inv_exp_Ku", "inv_exp_Kd", "exp_halfKu", "exp_halfKd",
+        "inv_exp_halfKu", "inv_exp_halfKd"]
+INT_PARAMS = ["N", "L", "n_matmul", "n_delay", "F", "n_sweep_warm", "n_sweep", "period_eqlt",
+              "period_uneqlt", "meas_bond_corr", "num_i", "num_ij", "num_b", "num_bb",
+              "degen_i", "degen_ij", "degen_bb"]
+
+
+def _scalar(v) -> int:
+    return int(np.asarray(v).reshape(-1)[0])
+
+
+class SimData:
+    """Parameters, state and accumulators of one sim file, as numpy arrays."""
+
+    def __init__(self, d: dict, path: str | None = None):
+        self.path = path
+        self.cplx = np.asarray(d["params/exp_Ku"]).dtype == np.complex128
+        nt = np.complex128 if self.cplx else np.float64
+        self.nt = nt
+        self.p = {k: _scalar(d["params/" + k]) for k in INT_PARAMS}
+        N, L = self.p["N"], self.p["L"]
+        self.N, self.L = N, L
+        a = lambda k, t: np.ascontiguousarray(np.asarray(d[k], dtype=t).reshape(-1))  # noqa: E731
+        self.map_i = a("params/map_i", np.int32)
+        self.map_ij = a("params/map_ij", np.int32)
+        nb = max(self.p["num_b"], 1)
+        self.bonds = a("params/bonds", np.int32) if "params/bonds" in d else np.zeros(2 * nb, np.int32)
+        self.map_bb = a("params/map_bb", np.int32) if "params/map_bb" in d else np.zeros(nb * nb, np.int32)
+        self.peierlsu = a("params/peierlsu", nt)
+        self.peierlsd = a("params/peierlsd", nt)
+        self.mats = {k: a("params/" + k, nt) for k in MATS}
+        self.exp_lambda = a("params/exp_lambda", np.float64)
+        self.del_ = a("params/del", np.float64)
+        self.rng = a("state/rng", np.uint64).copy()
+        self.sweep = _scalar(d["state/sweep"])
+        self.hs = a("state/hs", np.int32).copy()
+        ni, nij, nbb = self.p["num_i"], self.p["num_ij"], self.p["num_bb"]
+        self.eq_n = _scalar(d["meas_eqlt/n_sample"])
+        parts = [a("meas_eqlt/sign", nt)] + [a("meas_eqlt/" + k, nt) for k in EQ_I + EQ_IJ]
+        self.eq_acc = np.concatenate(parts).astype(nt)
+        self.ue_n = 0
+        self.ue_acc = np.zeros(1, nt)
+        if self.p["period_uneqlt"] > 0:
+            self.ue_n = _scalar(d["meas_uneqlt/n_sample"])
+            parts = [a("meas_uneqlt/sign", nt)] + [a("meas_uneqlt/" + k, nt) for k in UE_IJ]
+            if self.p["meas_bond_corr"]:
+                parts += [a("meas_uneqlt/" + k, nt) for k in UE_BB]
+            self.ue_acc = np.concatenate(parts).astype(nt)
+        self._sizes = (ni, nij, nbb)
+
+    @classmethod
+    def read(cls, path: str) -> "SimData":
+        d = simfile.read(path)
+        if _scalar(d["state/partial_write"]):
+            raise RuntimeError(f"Last checkpoint in {path} contained partial write")
+        return cls(d, path)
+
+    def params(self) -> tuple[_lib.Params, list]:
+        p = _lib.Params()
+        for k, v in self.p.items():
+            setattr(p, k, v)
+        p.cplx = int(self.cplx)
+        keep = [self.map_i, self.map_ij, self.bonds, self.map_bb, self.peierlsu, self.peierlsd]
+        p.map_i, p.map_ij = self.map_i.ctypes.data, self.map_ij.ctypes.data
+        p.bonds, p.map_bb = self.bonds.ctypes.data, self.map_bb.ctypes.data
+        p.peierlsu, p.peierlsd = self.peierlsu.ctypes.data, self.peierlsd.ctypes.data
+        for k, v in self.mats.items():
+            setattr(p, k, v.ctypes.data)
+            keep.append(v)
+        return p, keep
+
+    def measurements(self) -> dict:
+        """Accumulators as the datasets the reference writes (data.c:687-789)."""
+        ni, nij, nbb = self._sizes
+        L = self.L
+        out = {"meas_eqlt/n_sample": self.eq_n, "meas_eqlt/sign": self.eq_acc[0]}
+        o = 1
+        for k in EQ_I:
+            out["meas_eqlt/" + k] = self.eq_acc[o:o + ni]
+            o += ni
+        for k in EQ_IJ:
+            out["meas_eqlt/" + k] = self.eq_acc[o:o + nij]
+            o += nij
+        if self.p["period_uneqlt"] > 0:
+            out["meas_uneqlt/n_sample"] = self.ue_n
+            out["meas_uneqlt/sign"] = self.ue_acc[0]
+            o = 1
+            for k in UE_IJ:
+                out["meas_uneqlt/" + k] = self.ue_acc[o:o + nij * L]
+                o += nij * L
+            if self.p["meas_bond_corr"]:
+                for k in UE_BB:
+                    out["meas_uneqlt/" + k] = self.ue_acc[o:o + nbb * L]
+                    o += nbb * L
+        return out
+
+    def save(self, path: str | None = None):
+        """In-place update with the partial_write guard (data.c:667-789)."""
+        path = path or self.path
+        simfile.update(path, {"state/partial_write": 1})
+        vals = {"state/rng": self.rng, "state/sweep": self.sweep,
+                "state/hs": self.hs.reshape(self.L, self.N)}
+        for k, v in self.measurements().items():
+            vals[k] = v
+        simfile.update(path, vals)
+        simfile.update(path, {"state/partial_write": 0})
+
+
+class Engine:
+    """A group of chains with one parameter set, advanced on one GPU."""
+
+    def __init__(self, sims: list[SimData], device: int = 0):
+        if not sims:
+            raise ValueError("no chains")
+        self.lib = _lib.load()
+        self.sims = sims
+        s0 = sims[0]
+        self._p, self._keep = s0.params()
+        h = C.c_void_p()
+        _lib.check(self.lib.dqmc_engine_create(C.byref(self._p), len(sims), device, C.byref(h)),
+                   "dqmc_engine_create")
+        self.h = h
+        for c, s in enumerate(sims):
+            _lib.check(self.lib.dqmc_engine_set_chain(
+                h, c, s.exp_lambda.ctypes.data, s.del_.ctypes.data, s.rng.ctypes.data,
+                s.hs.ctypes.data, s.sweep), "dqmc_engine_set_chain")
+            _lib.check(self.lib.dqmc_engine_set_acc(
+                h, c, s.eq_n, s.eq_acc.ctypes.data, s.ue_n, s.ue_acc.ctypes.data),
+                "dqmc_engine_set_acc")
+
+    def init(self):
+        _lib.check(self.lib.dqmc_engine_init(self.h), "dqmc_engine_init")
+
+    def sweeps(self, n: int, sync: bool = True):
+        _lib.check(self.lib.dqmc_engine_sweeps(self.h, n, int(sync)), "dqmc_engine_sweeps")
+
+    def sync(self):
+        _lib.check(self.lib.dqmc_engine_sync(self.h), "dqmc_engine_sync")
+
+    def errors(self) -> int:
+        return int(self.lib.dqmc_engine_errors(self.h))
+
+    def launches_per_sweep(self, meas_eq: bool, meas_ue: bool) -> int:
+        return int(self.lib.dqmc_engine_launches_per_sweep(self.h, int(meas_eq), int(meas_ue)))
+
+    def profile_sweep(self, meas_eq: bool, meas_ue: bool = False, n_class: int = 5):
+        """One eagerly launched sweep with per-launch CUDA events; returns
+        {class: (ms, launches, flops, bytes)}."""
+        out = (C.c_double * (4 * n_class))()
+        _lib.check(self.lib.dqmc_engine_profile_sweep(self.h, int(meas_eq), int(meas_ue), out,
+                                                      n_class), "dqmc_engine_profile_sweep")
+        names = ["gemm", "update", "calc_eq_g", "uneqlt_g", "meas"]
+        return {names[c]: tuple(out[4 * c:4 * c + 4]) for c in range(n_class)}
+
+    def stream(self) -> int:
+        return int(self.lib.dqmc_engine_stream(self.h) or 0)
+
+    def pull(self):
+        """Copy every chain's state and accumulators back into its SimData."""
+        for c, s in enumerate(self.sims):
+            sw = C.c_int()
+            _lib.check(self.lib.dqmc_engine_get_chain(self.h, c, s.rng.ctypes.data,
+                                                      s.hs.ctypes.data, C.byref(sw)),
+                       "dqmc_engine_get_chain")
+            s.sweep = sw.value
+            en, un = C.c_int(), C.c_int()
+            _lib.check(self.lib.dqmc_engine_get_acc(self.h, c, C.byref(en), s.eq_acc.ctypes.data,
+                                                    C.byref(un), s.ue_acc.ctypes.data),
+                       "dqmc_engine_get_acc")
+            s.eq_n, s.ue_n = en.value, un.value
+
+    def g(self, c: int):
+        s = self.sims[c]
+        gu = np.zeros(s.N * s.N, s.nt)
+        gd = np.zeros_like(gu)
+        ph = np.zeros(1, s.nt)
+        _lib.check(self.lib.dqmc_engine_get_g(self.h, c, gu.ctypes.data, gd.ctypes.data,
+                                              ph.ctypes.data), "dqmc_engine_get_g")
+        return gu.reshape(s.N, s.N).T, gd.reshape(s.N, s.N).T, ph[0]
+
+    def accepts(self, c: int) -> int:
+        n = C.c_longlong()
+        _lib.check(self.lib.dqmc_engine_accepts(self.h, c, C.byref(n)), "dqmc_engine_accepts")
+        return n.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.dqmc_engine_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def run_file(path: str, n_sweeps: int | None = None, device: int = 0) -> SimData:
+    """Run one sim file to n_sweep (or n_sweeps more) and return its data."""
+    s = SimData.read(path)
+    e = Engine([s], device)
+    e.init()
+    e.sweeps((s.p["n_sweep"] - s.sweep) if n_sweeps is None else n_sweeps)
+    e.pull()
+    e.close()
+    return s

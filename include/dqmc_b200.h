@@ -1,0 +1,151 @@
+/*
+ * dqmc_b200: B200-native DQMC sweep engine -- C ABI.
+ *
+ * Drop-in for the sweep of katherineding/dqmc-dev.  Plain pointers, sizes and
+ * int status codes; no CUDA, C++ or torch types in any signature.  Matrices
+ * are column-major (element (i, j) at [i + N*j]) exactly as the reference
+ * stores them; `num` arrays are double, or interleaved (re, im) double pairs
+ * when the parameter set is complex (cplx = 1), like C99 double complex.
+ *
+ * Status codes: 0 success, negative on failure (DQMC_E_*).
+ */
+#ifndef DQMC_B200_H
+#define DQMC_B200_H
+
+#include <stdbool.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+	DQMC_OK = 0,
+	DQMC_E_ARG = -10,      /* invalid argument or unsupported size */
+	DQMC_E_CUDA = -11,     /* CUDA runtime error (no device, launch failure) */
+	DQMC_E_NOMEM = -12,    /* device allocation failed */
+	DQMC_E_DEVICE = -13,   /* a kernel reported an error (see dqmc_engine_errors) */
+};
+
+/* ---------------------------------------------------------------------------
+ * Drop-in entry point.  Replaces
+ *   int dqmc_wrapper(const char *sim_file, const char *log_file,
+ *                    const int64_t max_time, const bool dry, const bool bench);
+ * of the reference (src/dqmc.h:9-10, body src/dqmc.c:525-671): same
+ * arguments, same log lines, same return codes (-1 failure, 0 complete,
+ * 1 partial: stopped by signal or max_time), same checkpoint and
+ * partial_write protocol.  The sim file is the DQSF container written by the
+ * generator (dqmc_b200/gen.py or the reference generator under the DQSF
+ * h5py stand-in).
+ * ------------------------------------------------------------------------ */
+int dqmc_wrapper(const char *sim_file, const char *log_file,
+		const int64_t max_time, const bool dry, const bool bench);
+
+/* Batched drop-in: runs every file of a list as chains of one engine (files
+ * with equal parameters share kernel launches).  status[i] receives what
+ * dqmc_wrapper would have returned for file i.  Returns the worst status.
+ * No reference counterpart; the reference runs such lists one file per
+ * process through its stack job board (src/main_stack.c:399-479). */
+int dqmc_wrapper_batch(int n_files, const char *const *sim_files,
+		const char *log_file, const int64_t max_time, const bool bench,
+		int *status);
+
+/* ---------------------------------------------------------------------------
+ * Engine: a group of chains sharing one parameter set (struct params,
+ * src/data.h:7-38) advanced together on one GPU.
+ * ------------------------------------------------------------------------ */
+typedef struct dqmc_engine dqmc_engine;
+
+typedef struct {
+	int N, L, n_matmul, n_delay, F;
+	int n_sweep_warm, n_sweep, period_eqlt, period_uneqlt, meas_bond_corr;
+	int num_i, num_ij, num_b, num_bb, degen_i, degen_ij, degen_bb;
+	int cplx;                         /* 0 real, 1 complex */
+	const int *map_i, *map_ij;        /* [N], [N*N] */
+	const int *bonds, *map_bb;        /* [2*num_b], [num_b*num_b] */
+	const void *peierlsu, *peierlsd;  /* num[N*N] */
+	const void *exp_Ku, *exp_Kd, *inv_exp_Ku, *inv_exp_Kd;
+	const void *exp_halfKu, *exp_halfKd, *inv_exp_halfKu, *inv_exp_halfKd;
+} dqmc_params;
+
+/* Accumulator sizes in num elements per chain (layout documented in
+ * dqmc-dev_b200/csrc/meas.cuh: sign, then the datasets in data.h order). */
+int dqmc_acc_sizes(const dqmc_params *p, int *eq_size, int *ue_size);
+
+int dqmc_engine_create(const dqmc_params *p, int n_chain, int device,
+		dqmc_engine **out);
+void dqmc_engine_destroy(dqmc_engine *e);
+
+/* Per-chain state (host arrays, copied): exp_lambda[2N], del[2N] as in the
+ * sim file, rng[17], hs[L*N] (hs[i + N*l]), and the sweep counter (equal
+ * for every chain of an engine). */
+int dqmc_engine_set_chain(dqmc_engine *e, int chain, const double *exp_lambda,
+		const double *del, const uint64_t *rng, const int *hs, int sweep);
+int dqmc_engine_set_acc(dqmc_engine *e, int chain, int eq_n_sample,
+		const void *eq_acc, int ue_n_sample, const void *ue_acc);
+
+/* Computes the initial G of every chain (dqmc.c:188-220). */
+int dqmc_engine_init(dqmc_engine *e);
+
+/* Advances every chain by n sweeps (dqmc.c:222-459), measuring as the
+ * parameters and the sweep counter say.  Stream-ordered; returns after the
+ * work is queued unless sync != 0. */
+int dqmc_engine_sweeps(dqmc_engine *e, int n, int sync);
+int dqmc_engine_sync(dqmc_engine *e);
+/* OR of the device error words since creation (0 = none) */
+unsigned dqmc_engine_errors(dqmc_engine *e);
+
+int dqmc_engine_get_chain(dqmc_engine *e, int chain, uint64_t *rng, int *hs,
+		int *sweep);
+int dqmc_engine_get_acc(dqmc_engine *e, int chain, int *eq_n_sample, void *eq_acc,
+		int *ue_n_sample, void *ue_acc);
+/* G of both spins (column-major) and the chain's phase */
+int dqmc_engine_get_g(dqmc_engine *e, int chain, void *gu, void *gd, void *phase);
+/* total Metropolis accepts of a chain since creation */
+int dqmc_engine_accepts(dqmc_engine *e, int chain, long long *n);
+/* CUDA stream the engine queues on, as an opaque handle (cudaStream_t) */
+void *dqmc_engine_stream(dqmc_engine *e);
+/* number of kernels one sweep of the given kind launches */
+int dqmc_engine_launches_per_sweep(dqmc_engine *e, int meas_eq, int meas_ue);
+/* Runs one sweep eagerly with CUDA events around every launch (it advances
+ * the chains like dqmc_engine_sweeps(e, 1, 1)).  out[4*c + k], c < n_class:
+ * k = 0 total ms, 1 launches, 2 algorithmic FLOPs, 3 operand bytes, for the
+ * launch classes c = 0 batched GEMM, 1 delayed update, 2 calc_eq_g (its
+ * GEMMs included), 3 unequal-time G, 4 measurements. */
+int dqmc_engine_profile_sweep(dqmc_engine *e, int meas_eq, int meas_ue, double *out,
+		int n_class);
+
+/* ---------------------------------------------------------------------------
+ * Kernel-level seams on device pointers, batched over `batch` independent
+ * problems laid out back to back.  Each mirrors one reference function.
+ * stream: a cudaStream_t passed as void* (NULL = default stream).
+ * ------------------------------------------------------------------------ */
+
+/* calc_eq_g (src/greens.c:69-208, called as calc_eq_g(l, N, F, 2, C, g, ...)
+ * by dqmc.c:202, 288): G = (I + C_{l-1} ... C_{l})^-1 from F cluster
+ * matrices per problem (C: batch x F x N*N), writing G (batch x N*N) and
+ * phase[batch] = 1/phase(det G). */
+int dqmc_gpu_calc_eq_g(int batch, int N, int F, int l, int cplx, const void *C,
+		void *G, void *phase, void *stream);
+
+/* update_delayed (src/updates.c:7-84) preceded by shuffle (src/rand.h:25-31)
+ * as dqmc.c:249-253 calls them, for `batch` chains: del[batch][2N],
+ * rng[batch][17], hs[batch][N] (this slice's fields), G[batch][2][N*N]
+ * (up, down), phase[batch]; n_delay as in the sim file. */
+int dqmc_gpu_update_delayed(int batch, int N, int n_delay, int cplx,
+		const double *del, uint64_t *rng, int *hs, void *G, void *phase,
+		void *stream);
+
+/* mul_seq (src/greens.c:8-41) for B_l = exp_K diag(exp_lambda[hs_l]):
+ * C = B_{l0+n-1} ... B_{l0} for one spin (spin 0 uses hs, 1 uses !hs) of
+ * `batch` chains: exp_K[N*N] shared, exp_lambda[batch][2N],
+ * hs[batch][n][N] (the n slices), C[batch][N*N]. */
+int dqmc_gpu_mul_seq(int batch, int N, int n, int spin, int cplx,
+		const void *exp_K, const double *exp_lambda, const int *hs, void *C,
+		void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
