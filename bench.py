@@ -39,6 +39,14 @@ WORKLOAD = ("256 chains x 12x12 square Hubbard (N=144), U=4, mu=-1, beta=6, dtau
             "(L=120), n_matmul=10, n_delay=16, eqlt every 8 slices, FP64")
 
 
+T0 = time.time()
+
+
+def log(msg):
+    """progress line on stderr (the JSON result goes to stdout)"""
+    print(f"[bench {time.time() - T0:7.1f}s] {msg}", file=sys.stderr, flush=True)
+
+
 def sim_dicts(n, seed, n_sweep):
     from dqmc_b200 import gen
     rngs = gen.chain_rngs(seed, n)
@@ -227,13 +235,17 @@ def main():
     nch = args.chains
     total = args.warmup + args.steps + 4
     dicts = sim_dicts(nch, seed=1000 + rank, n_sweep=total)
+    log(f"generated {nch} chains")
     sims = [engine.SimData(d) for d in dicts]
     eng = engine.Engine(sims, device=local)
     eng.init()
+    log("initial G done")
     stream = torch.cuda.ExternalStream(eng.stream())
 
     # warm-up (also captures the sweep graph)
-    eng.sweeps(args.warmup, sync=True)
+    for _ in range(args.warmup):
+        eng.sweeps(1, sync=True)
+        log("warm-up sweep done")
 
     # timed region: K sweeps, device time on the engine's stream
     barrier(world)
@@ -248,6 +260,7 @@ def main():
     t_dev = ev0.elapsed_time(ev1) / 1e3
     assert eng.errors() == 0, "device error word set"
     t_max = max_over_ranks(t_dev, world)
+    log(f"timed sweeps done: {1e3 * t_dev / args.steps:.1f} ms per sweep")
     value = nch * args.steps * world / t_max
     launches = eng.launches_per_sweep(True, False) * args.steps
 
@@ -256,22 +269,28 @@ def main():
     L = lib.load()
     e2e_steps = 2
     h2d = d2h = 0
+    eng.pull()          # host copies of the state the device now holds
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for _ in range(e2e_steps):
+    for k in range(e2e_steps):
         for c, s in enumerate(sims):
             lib.check(L.dqmc_engine_set_chain(eng.h, c, s.exp_lambda.ctypes.data,
                                               s.del_.ctypes.data, s.rng.ctypes.data,
                                               s.hs.ctypes.data, s.sweep), "set_chain")
+        log(f"e2e step {k}: state uploaded")
         h2d = sum(s.exp_lambda.nbytes + s.del_.nbytes + s.rng.nbytes + s.hs.nbytes for s in sims)
         eng.sweeps(1, sync=True)
+        log(f"e2e step {k}: sweep done")
         eng.pull()
+        log(f"e2e step {k}: state downloaded")
         d2h = sum(s.rng.nbytes + s.hs.nbytes + s.eq_acc.nbytes + 8 for s in sims)
     t_e2e = max_over_ranks((time.perf_counter() - t0) / e2e_steps, world)
     e2e = nch * world / t_e2e
 
+    log("e2e done")
     # per-launch profile of one more sweep (eager launches with events)
     prof = eng.profile_sweep(True, False)
+    log("profile sweep done")
     peak = fp64_peak()
     gm_ms, gm_n, gm_fl, gm_by = prof["gemm"]
     eq_ms = prof["calc_eq_g"][0]
@@ -285,9 +304,10 @@ def main():
         try:
             cores = os.cpu_count() or 2
             n_proc = max(1, cores // 2)
-            rate, t = reference_rate(n_proc, 3)
+            rate, t = reference_rate(n_proc, 30)
+            log("cpu baseline done")
             cpu = {"value": rate, "unit": METRIC, "cores": 2 * n_proc, "kind": "reference",
-                   "sample": f"{n_proc} processes of the reference dqmc_1_r x 3 sweeps of one "
+                   "sample": f"{n_proc} processes of the reference dqmc_1_r x 30 sweeps of one "
                              f"12x12 L=120 chain each, {t:.1f} s"}
         except Exception as ex:  # noqa: BLE001
             cpu = {"value": None, "unit": METRIC, "cores": 0, "kind": "reference",

@@ -80,6 +80,10 @@ __device__ inline double shfl(double v, int src) { return __shfl_sync(0xffffffff
 __device__ inline zd shfl(zd v, int src) {
 	return zd{__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src)};
 }
+__device__ inline double shfl_xor(double v, int o) { return __shfl_xor_sync(0xffffffffu, v, o); }
+__device__ inline zd shfl_xor(zd v, int o) {
+	return zd{__shfl_xor_sync(0xffffffffu, v.x, o), __shfl_xor_sync(0xffffffffu, v.y, o)};
+}
 __device__ inline double warp_sum(double v) {
 	for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
 	return v;

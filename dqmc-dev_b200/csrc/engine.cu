@@ -4,6 +4,8 @@
 // include/dqmc_b200.h.
 #include <cstdio>
 #include <cstdlib>
+#include <ctime>
+#include <unistd.h>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -33,29 +35,53 @@ static inline Addr per_spin(long long stride) { return Addr{0, stride, 2}; }
 
 // ------------------------------------------------------------------ launches
 
-template <typename T, int BM, int BN, int BK, int WM, int WN>
-static void launch_gemm_cfg(const GemmArgs<T> &g, cudaStream_t st)
+template <typename T, int BM, int BN, int BK, int WM, int WN, int ST, int MODE>
+static int launch_gemm_mode(const GemmArgs<T> &g, cudaStream_t st)
 {
-	using Cfg = GemmCfg<T, BM, BN, BK, WM, WN>;
+	using Cfg = GemmCfg<T, BM, BN, BK, WM, WN, ST>;
 	static bool attr = false;
 	if (!attr) {
-		cudaFuncSetAttribute(k_gemm<T, BM, BN, BK, WM, WN>,
-		                     cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM_BYTES);
+		if (cudaFuncSetAttribute(k_gemm<T, BM, BN, BK, WM, WN, ST, MODE>,
+		                         cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM_BYTES) != cudaSuccess)
+			return DQMC_E_ARG;
 		attr = true;
 	}
 	dim3 grid((g.M + BM - 1) / BM, (g.N + BN - 1) / BN, g.batch);
-	k_gemm<T, BM, BN, BK, WM, WN><<<grid, Cfg::THREADS, Cfg::SMEM_BYTES, st>>>(g);
+	k_gemm<T, BM, BN, BK, WM, WN, ST, MODE><<<grid, Cfg::THREADS, Cfg::SMEM_BYTES, st>>>(g);
+	return 0;
+}
+
+template <typename T, int BM, int BN, int BK, int WM, int WN, int ST>
+static int launch_gemm_cfg(const GemmArgs<T> &g, cudaStream_t st)
+{
+	switch (g.mode) {
+	case 0: return launch_gemm_mode<T, BM, BN, BK, WM, WN, ST, 0>(g, st);
+	case GM_A_DD: return launch_gemm_mode<T, BM, BN, BK, WM, WN, ST, GM_A_DD>(g, st);
+	case GM_B_ROWD: return launch_gemm_mode<T, BM, BN, BK, WM, WN, ST, GM_B_ROWD>(g, st);
+	case GM_B_COLD: return launch_gemm_mode<T, BM, BN, BK, WM, WN, ST, GM_B_COLD>(g, st);
+	case GM_B_IDENT: return launch_gemm_mode<T, BM, BN, BK, WM, WN, ST, GM_B_IDENT>(g, st);
+	case GM_A_UPPER | GM_B_GATHER:
+		return launch_gemm_mode<T, BM, BN, BK, WM, WN, ST, GM_A_UPPER | GM_B_GATHER>(g, st);
+	default: return DQMC_E_ARG;
+	}
 }
 
 // tile choice: least padded area, larger tiles on ties
 template <typename T>
-void launch_gemm(const GemmArgs<T> &g, cudaStream_t st)
+int launch_gemm(const GemmArgs<T> &g, cudaStream_t st)
 {
+	if (g.K > 512 || g.M < 1 || g.N < 1 || g.K < 1 || g.batch < 1) return DQMC_E_ARG;
 	auto pad = [&](int t) { return (long long)((g.M + t - 1) / t * t) * ((g.N + t - 1) / t * t); };
 	const long long p64 = pad(64), p48 = pad(48), p32 = pad(32);
-	if (p64 <= p48 && p64 <= p32) launch_gemm_cfg<T, 64, 64, 16, 2, 2>(g, st);
-	else if (p48 <= p32) launch_gemm_cfg<T, 48, 48, 16, 2, 2>(g, st);
-	else launch_gemm_cfg<T, 32, 32, 16, 2, 2>(g, st);
+	if constexpr (is_cplx<T>::value) {
+		if (p64 <= p48 && p64 <= p32) return launch_gemm_cfg<T, 64, 64, 8, 4, 2, 3>(g, st);
+		if (p48 <= p32) return launch_gemm_cfg<T, 48, 48, 8, 2, 2, 3>(g, st);
+		return launch_gemm_cfg<T, 32, 32, 8, 2, 2, 3>(g, st);
+	} else {
+		if (p64 <= p48 && p64 <= p32) return launch_gemm_cfg<T, 64, 64, 16, 2, 2, 3>(g, st);
+		if (p48 <= p32) return launch_gemm_cfg<T, 48, 48, 16, 2, 2, 4>(g, st);
+		return launch_gemm_cfg<T, 32, 32, 16, 2, 2, 4>(g, st);
+	}
 }
 
 template <typename T>
@@ -76,19 +102,26 @@ static GemmArgs<T> gargs(int M, int N, int K, int batch, const T *A, Addr aA, in
 }
 
 // register shapes for the per-matrix factorisations
-template <typename T, int RPL, int CPW, int NW>
-static int launch_qr_cfg(const QrArgs<T> &a, cudaStream_t st)
+template <typename T, int RPL, int CPW, int NW, int MODE>
+static int launch_qr_mode(const QrArgs<T> &a, cudaStream_t st)
 {
 	const size_t sm = qr_smem_bytes<T>(a.N, NW);
 	static size_t attr = 0;
 	if (sm > attr) {
-		if (cudaFuncSetAttribute(k_qr<T, RPL, CPW, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-		                         (int)sm) != cudaSuccess)
+		if (cudaFuncSetAttribute(k_qr<T, RPL, CPW, NW, MODE>,
+		                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
 			return DQMC_E_ARG;
 		attr = sm;
 	}
-	k_qr<T, RPL, CPW, NW><<<a.batch, NW * 32, sm, st>>>(a);
+	k_qr<T, RPL, CPW, NW, MODE><<<a.batch, NW * 32, sm, st>>>(a);
 	return 0;
+}
+
+template <typename T, int RPL, int CPW, int NW>
+static int launch_qr_cfg(const QrArgs<T> &a, cudaStream_t st)
+{
+	return a.mode == QR_PIVOT ? launch_qr_mode<T, RPL, CPW, NW, QR_PIVOT>(a, st)
+	                          : launch_qr_mode<T, RPL, CPW, NW, QR_PRESORT>(a, st);
 }
 
 template <typename T, int RPL, int CPW, int NW>
@@ -217,9 +250,9 @@ struct EqWork {
 template <typename T>
 static int eq_gemm(const GemmArgs<T> &g, cudaStream_t st, int *count)
 {
-	launch_gemm<T>(g, st);
+	const int rc = launch_gemm<T>(g, st);
 	if (count) (*count)++;
-	return 0;
+	return rc;
 }
 
 // G = (I + C_{l0-1} ... C_{l0})^-1 over the F clusters (cyclic), grouped two
@@ -381,14 +414,39 @@ struct Group : GroupBase {
 	std::map<int, cudaGraphExec_t> graphs;
 	std::map<int, int> graph_launches;
 	int launch_count = 0;
+	// DQMC_DEBUG_SYNC=1: eager launches, each polled to completion with a
+	// deadline; a kernel that does not finish is named and the process exits
+	bool debug_sync = getenv("DQMC_DEBUG_SYNC") != nullptr;
+	int watchdog(const char *what)
+	{
+		if (!debug_sync) return 0;
+		const double t0 = (double)clock() / CLOCKS_PER_SEC;
+		for (;;) {
+			const cudaError_t e = cudaStreamQuery(st);
+			if (e == cudaSuccess) return 0;
+			if (e != cudaErrorNotReady) {
+				fprintf(stderr, "dqmc_b200 watchdog: %s failed: %s\n", what, cudaGetErrorString(e));
+				fflush(stderr);
+				_exit(4);
+			}
+			if ((double)clock() / CLOCKS_PER_SEC - t0 > 10.0) {
+				fprintf(stderr, "dqmc_b200 watchdog: %s (sweep %d) did not finish in 10 s\n", what, sweep);
+				fflush(stderr);
+				_exit(3);
+			}
+		}
+	}
 
 	// parameters
 	DevBuf<T> expK, iexpK, ehK, iehK, peu, ped;
 	DevBuf<int> i_off, i_idx, ij_off, ij_idx, bb_off, bb_idx, bonds;
 	// chains
 	DevBuf<double> el, del, dv, dvi;
-	DevBuf<uint64_t> rng;
-	DevBuf<int> hs, nacc, n_eq, n_ue;
+	DevBuf<uint64_t> rng, rng_ckpt;
+	DevBuf<int> hs, nacc, n_eq, n_ue, order;
+	DevBuf<double> ubuf;
+	bool need_draws = true;
+	bool need_init = true;     // G must be recomputed from the fields before sweeping
 	DevBuf<T> phase, G, Cl, Qm, Tm, Tm2, Rs, X, W, Gh, acc_eq, acc_ue, phi, qdet;
 	DevBuf<double> dR;
 	DevBuf<int> pvt;
@@ -405,7 +463,7 @@ struct Group : GroupBase {
 		                     &nacc, &n_eq, &n_ue, &pvt};
 		for (auto *b : ib) b->release();
 		el.release(); del.release(); dv.release(); dvi.release(); dR.release();
-		rng.release(); err.release();
+		rng.release(); rng_ckpt.release(); order.release(); ubuf.release(); err.release();
 		ue.release();
 		if (st) cudaStreamDestroy(st);
 	}
@@ -417,7 +475,7 @@ struct Group : GroupBase {
 		NB = 2 * C;
 		N = p.N; L = p.L; F = p.F; nmul = p.n_matmul;
 		if (N < 1 || L < 1 || F < 1 || nmul < 1 || L != F * nmul || N > max_dense_n<T>() ||
-		    N > 512 || C < 1)
+		    N > 480 || C < 1)
 			return DQMC_E_ARG;
 		if (p.period_uneqlt > 0 && !UneqState<T>::supported(N, F)) return DQMC_E_ARG;
 		CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
@@ -428,7 +486,9 @@ struct Group : GroupBase {
 		rc |= peu.alloc(NN); rc |= ped.alloc(NN);
 		rc |= el.alloc((size_t)C * 2 * N); rc |= del.alloc((size_t)C * 2 * N);
 		rc |= dv.alloc((size_t)C * 2 * L * N); rc |= dvi.alloc((size_t)C * 2 * L * N);
-		rc |= rng.alloc((size_t)C * 17); rc |= hs.alloc((size_t)C * L * N);
+		rc |= rng.alloc((size_t)C * 17); rc |= rng_ckpt.alloc((size_t)C * 17);
+		rc |= order.alloc((size_t)C * 2 * N); rc |= ubuf.alloc((size_t)C * 2 * N);
+		rc |= hs.alloc((size_t)C * L * N);
 		rc |= nacc.alloc(C); rc |= n_eq.alloc(C); rc |= n_ue.alloc(C);
 		rc |= phase.alloc(C); rc |= phi.alloc(NB); rc |= qdet.alloc(NB);
 		rc |= G.alloc(NB * NN); rc |= Cl.alloc((size_t)NB * F * NN);
@@ -488,6 +548,8 @@ struct Group : GroupBase {
 		CK(cudaMemcpy(rng.p + (size_t)c * 17, r, sizeof(uint64_t) * 17, cudaMemcpyHostToDevice));
 		CK(cudaMemcpy(hs.p + (size_t)c * L * N, h, sizeof(int) * L * N, cudaMemcpyHostToDevice));
 		sweep = sw;
+		need_draws = true;
+		need_init = true;
 		return 0;
 	}
 
@@ -509,6 +571,7 @@ struct Group : GroupBase {
 	{
 		prof_begin(0);
 		eq_gemm<T>(g, st, &launch_count);
+		watchdog("k_gemm");
 		double fl = 2.0 * g.M * g.N * g.K * g.batch * (is_cplx<T>::value ? 4.0 : 1.0);
 		if (g.mode & GM_A_UPPER) fl *= 0.5;
 		prof_end(0, fl, (double)sizeof(T) * ((double)g.M * g.K + (double)g.K * g.N + (double)g.M * g.N) * g.batch);
@@ -549,6 +612,7 @@ struct Group : GroupBase {
 		prof_begin(0);
 		run_mul_seq<T>(N, nmul, NB, expK.p, per_spin(NN), dv.p + (size_t)f * nmul * N, (long long)L * N,
 		               Cl.p + (size_t)f * NN, per_item((long long)F * NN), X.p, W.p, st, &launch_count);
+		watchdog("mul_seq");
 		const double fl = 2.0 * N * NN * NB * (nmul - 1) * (is_cplx<T>::value ? 4.0 : 1.0);
 		prof_end(0, fl, 3.0 * sizeof(T) * NN * NB * (nmul - 1));
 	}
@@ -571,10 +635,19 @@ struct Group : GroupBase {
 		prof_begin(2);
 		int rc = run_calc_eq_g<T>(eq_work(), l0, st, &launch_count);
 		prof_end(2, 0.0, 0.0);
+		watchdog("calc_eq_g");
 		if (rc) return rc;
 		k_combine_phase<T><<<(C + 127) / 128, 128, 0, st>>>(C, phi.p, phase.p);
 		launch_count++;
 		return 0;
+	}
+
+	// the draws of slice l for every chain, from the working RNG state
+	void draws(int l)
+	{
+		k_draws<<<(C + 63) / 64, 64, 0, st>>>(N, L, C, l, del.p, rng.p, rng_ckpt.p, hs.p, order.p,
+		                                      ubuf.p);
+		launch_count++;
 	}
 
 	void update(int l)
@@ -583,11 +656,17 @@ struct Group : GroupBase {
 		a.N = N; a.L = L; a.n_delay = kd; a.nchain = C; a.slice = l; a.ldp = ldp;
 		a.del = del.p; a.exp_lambda = el.p; a.rng = rng.p; a.hs = hs.p; a.G = G.p;
 		a.phase = phase.p; a.dv = dv.p; a.dvi = dvi.p; a.n_accept = nacc.p; a.err = err.p;
+		a.rng_ckpt = rng_ckpt.p; a.order = order.p; a.u = ubuf.p;
+		// the look-ahead warp draws the next slice, except when that is this
+		// slice again (L = 1), whose fields this kernel is still changing
+		a.next_slice = (L == 1) ? -1 : (l + 1) % L;
 		const int np = (N + 31) / 32 * 32;
 		prof_begin(1);
-		k_update<T><<<C, 2 * np, update_smem_bytes<T>(N, kd, ldp), st>>>(a);
+		k_update<T><<<C, 2 * np + 32, update_smem_bytes<T>(N, kd, ldp), st>>>(a);
 		prof_end(1, 0.0, 0.0);
 		launch_count++;
+		watchdog("k_update");
+		if (L == 1) draws(0);
 	}
 
 	// G <- B_l G B_l^-1 = exp_K (D G D^-1) inv_exp_K
@@ -637,6 +716,7 @@ struct Group : GroupBase {
 		k_meas_eqlt<T><<<C, 256, 2 * N * sizeof(T) + 64, st>>>(m);
 		prof_end(4, 0.0, 0.0);
 		launch_count++;
+		watchdog("k_meas_eqlt");
 	}
 
 	int meas_uneqlt()
@@ -666,6 +746,9 @@ struct Group : GroupBase {
 		for (int f = 0; f < F; f++) build_cluster(f);
 		int rc = calc_eq_g(0);
 		if (rc) return rc;
+		draws(0);
+		need_draws = false;
+		need_init = false;
 		CK(cudaStreamSynchronize(st));
 		return 0;
 	}
@@ -695,11 +778,26 @@ struct Group : GroupBase {
 
 	int sweeps(int n, int sync_after) override
 	{
+		if (need_init) {
+			// fields were replaced: G, clusters and draws follow them again
+			const int rc = init();
+			if (rc) return rc;
+		}
+		if (need_draws) {
+			draws(0);
+			need_draws = false;
+		}
 		for (int k = 0; k < n; k++) {
 			if (sweep >= p.n_sweep) break;
 			const bool meq = sweep >= p.n_sweep_warm;
 			const bool mue = meq && p.period_uneqlt > 0 && sweep % p.period_uneqlt == 0;
 			const int kind = (meq ? 1 : 0) | (mue ? 2 : 0);
+			if (debug_sync) {
+				int rc = enqueue_sweep(meq, mue);
+				if (rc) return rc;
+				sweep++;
+				continue;
+			}
 			auto it = graphs.find(kind);
 			if (it == graphs.end()) {
 				cudaGraph_t gr;
@@ -733,6 +831,14 @@ struct Group : GroupBase {
 	int profile(int meq, int mue, double *out, int ncls) override
 	{
 		if (sweep >= p.n_sweep) return DQMC_E_ARG;
+		if (need_init) {
+			const int rc = init();
+			if (rc) return rc;
+		}
+		if (need_draws) {
+			draws(0);
+			need_draws = false;
+		}
 		profiling = true;
 		precs.clear();
 		int rc = enqueue_sweep(meq, mue);
@@ -790,7 +896,8 @@ struct Group : GroupBase {
 	{
 		if (c < 0 || c >= C) return DQMC_E_ARG;
 		CK(cudaStreamSynchronize(st));
-		if (r) CK(cudaMemcpy(r, rng.p + (size_t)c * 17, sizeof(uint64_t) * 17, cudaMemcpyDeviceToHost));
+		// the state the chain has at the sweep boundary, before the look-ahead
+		if (r) CK(cudaMemcpy(r, rng_ckpt.p + (size_t)c * 17, sizeof(uint64_t) * 17, cudaMemcpyDeviceToHost));
 		if (h) CK(cudaMemcpy(h, hs.p + (size_t)c * L * N, sizeof(int) * L * N, cudaMemcpyDeviceToHost));
 		if (sw) *sw = sweep;
 		return 0;
@@ -999,19 +1106,26 @@ template <typename T>
 static int seam_update(int batch, int N, int n_delay, const double *del, uint64_t *rng, int *hs,
 		void *G, void *phase, cudaStream_t st)
 {
-	if (batch < 1 || N < 1 || N > 512 || n_delay < 1 || !del || !rng || !hs || !G || !phase)
+	if (batch < 1 || N < 1 || N > 480 || n_delay < 1 || !del || !rng || !hs || !G || !phase)
 		return DQMC_E_ARG;
 	int kd = n_delay;
 	const int ldp = (N + 15) / 16 * 16 + 4;
 	while (kd > 1 && update_smem_bytes<T>(N, kd, ldp) > 200 * 1024) kd /= 2;
 	CK(cudaFuncSetAttribute(k_update<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
 	                        (int)update_smem_bytes<T>(N, kd, ldp)));
+	Scratch<T> sc;
+	uint64_t *ck = sc.template get<uint64_t>((size_t)batch * 17);
+	int *ord = sc.template get<int>((size_t)batch * 2 * N);
+	double *uu = sc.template get<double>((size_t)batch * 2 * N);
+	if (!ck || !ord || !uu) return DQMC_E_NOMEM;
+	k_draws<<<(batch + 63) / 64, 64, 0, st>>>(N, 1, batch, 0, del, rng, ck, hs, ord, uu);
 	UpdArgs<T> a;
 	memset(&a, 0, sizeof(a));
 	a.N = N; a.L = 1; a.n_delay = kd; a.nchain = batch; a.slice = 0; a.ldp = ldp;
-	a.del = del; a.rng = rng; a.hs = hs; a.G = (T *)G; a.phase = (T *)phase;
+	a.del = del; a.rng = rng; a.rng_ckpt = ck; a.hs = hs; a.G = (T *)G; a.phase = (T *)phase;
+	a.order = ord; a.u = uu; a.next_slice = -1;
 	const int np = (N + 31) / 32 * 32;
-	k_update<T><<<batch, 2 * np, update_smem_bytes<T>(N, kd, ldp), st>>>(a);
+	k_update<T><<<batch, 2 * np + 32, update_smem_bytes<T>(N, kd, ldp), st>>>(a);
 	CK(cudaGetLastError());
 	CK(cudaStreamSynchronize(st));
 	return 0;
@@ -1042,7 +1156,33 @@ static int seam_mul_seq(int batch, int N, int n, int spin, const void *expK, con
 	return 0;
 }
 
+template <typename T>
+static int seam_gemm(int batch, int M, int N, int K, const void *alpha, const void *A, int lda,
+		long long sA, const void *B, int ldb, long long sB, const void *beta, void *C, int ldc,
+		long long sC, cudaStream_t st)
+{
+	if (!A || !B || !C || !alpha || !beta || lda < M || ldb < K || ldc < M) return DQMC_E_ARG;
+	GemmArgs<T> g = gargs<T>(M, N, K, batch, (const T *)A, Addr{sA, 0, 1}, lda, (const T *)B,
+	                         Addr{sB, 0, 1}, ldb, (T *)C, Addr{sC, 0, 1}, ldc,
+	                         *(const T *)alpha, *(const T *)beta, 0);
+	const int rc = launch_gemm<T>(g, st);
+	if (rc) return rc;
+	CK(cudaGetLastError());
+	return 0;
+}
+
 extern "C" {
+
+int dqmc_gpu_gemm(int batch, int M, int N, int K, int cplx, const void *alpha, const void *A,
+		int lda, long long stride_a, const void *B, int ldb, long long stride_b, const void *beta,
+		void *C, int ldc, long long stride_c, void *stream)
+{
+	cudaStream_t st = (cudaStream_t)stream;
+	return cplx ? seam_gemm<zd>(batch, M, N, K, alpha, A, lda, stride_a, B, ldb, stride_b, beta, C,
+	                             ldc, stride_c, st)
+	            : seam_gemm<double>(batch, M, N, K, alpha, A, lda, stride_a, B, ldb, stride_b, beta,
+	                                C, ldc, stride_c, st);
+}
 
 int dqmc_gpu_calc_eq_g(int batch, int N, int F, int l, int cplx, const void *C, void *G,
 		void *phase, void *stream)

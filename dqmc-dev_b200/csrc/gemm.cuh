@@ -7,15 +7,20 @@
 // (b % div) * lo, which covers per-item matrices (div 1), per-spin shared
 // parameters such as exp(-dt K_sigma) (div 2, hi 0) and per-item stacks.
 //
-// Operand modes fuse the diagonal factors of B_l = exp(-dt K) diag(d_l)
-// (reference dqmc.c:29-59) into the tile loads instead of materialising B:
+// Operand modes (compile-time) fuse the diagonal factors of
+// B_l = exp(-dt K) diag(d_l) (reference dqmc.c:29-59) and the other
+// structure of the calc_eq_g products into the kernel instead of
+// materialising them:
 //   A_DD       A[r,k] * d[r] / d[k]     (G -> D G D^-1, the wrap prologue)
 //   B_ROWD     B[k,c] * d[k]            (diag(d) X, the mul_seq step)
-//   B_COLD     B[k,c] * d[c]            (X diag(d), the first factor of C_f)
-//   A_UPPER    A[r,k] = 0 for r > k     (triangular A: the trmm of calc_eq_g)
+//   B_COLD     B[k,c] * d[c]            (X diag(d))
+//   A_UPPER    A[r,k] = 0 for r > k     (triangular A, the trmm of calc_eq_g;
+//                                        k-tiles left of the diagonal skipped)
 //   B_GATHER   B[k,c] = B[idx[k],c]     (row permutation P^T T)
-// Tiles are staged through shared memory by the CTA (register double
-// buffering) with padded strides so fragment loads are bank-conflict free.
+//   B_IDENT    B = I                    (C = alpha A + beta C)
+// Tiles move global -> shared with cp.async (zero-filled outside the matrix)
+// through a STAGES-deep ring; scale vectors are staged once per CTA and
+// applied when fragments are read, so every mode keeps the same pipeline.
 #pragma once
 
 #include "common.cuh"
@@ -28,7 +33,7 @@ enum : int {
 	GM_A_UPPER = 4,
 	GM_B_GATHER = 8,
 	GM_B_COLD = 16,
-	GM_B_IDENT = 32,   // B is the identity (C = alpha A + beta C with scaling)
+	GM_B_IDENT = 32,
 };
 
 struct Addr {
@@ -49,16 +54,48 @@ struct GemmArgs {
 	const int *gidx; Addr aG;                       // row gather for B
 };
 
-template <typename T, int BM, int BN, int BK, int WM, int WN>
+__device__ inline void cp_async8(void *smem, const void *gmem, bool valid)
+{
+	const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+	asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem),
+	             "r"(valid ? 8 : 0));
+}
+__device__ inline void cp_async16(void *smem, const void *gmem, bool valid)
+{
+	const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+	asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem),
+	             "r"(valid ? 16 : 0));
+}
+__device__ inline void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int NPEND>
+__device__ inline void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(NPEND)); }
+
+template <typename T>
+__device__ inline void cp_async_el(T *smem, const T *gmem, bool valid);
+template <>
+__device__ inline void cp_async_el<double>(double *smem, const double *gmem, bool valid)
+{
+	cp_async8(smem, gmem, valid);
+}
+template <>
+__device__ inline void cp_async_el<zd>(zd *smem, const zd *gmem, bool valid)
+{
+	cp_async16(smem, gmem, valid);
+}
+
+template <typename T, int BM, int BN, int BK, int WM, int WN, int STAGES>
 struct GemmCfg {
+	static constexpr bool CX = is_cplx<T>::value;
 	static constexpr int THREADS = WM * WN * 32;
-	static constexpr int SA = BM + 4;      // As[k][r]
-	static constexpr int SB = BK + 4;      // Bs[c][k]
-	static constexpr int PLANES = is_cplx<T>::value ? 2 : 1;
-	static constexpr int SMEM_A = BK * SA;
-	static constexpr int SMEM_B = BN * SB;
-	static constexpr int STAGE = PLANES * (SMEM_A + SMEM_B);
-	static constexpr int SMEM_BYTES = 2 * STAGE * (int)sizeof(double);
+	// padded strides: fragment reads conflict-free for 8- and 16-byte elements
+	static constexpr int SA = BM + (CX ? 2 : 4);      // As[k][r]
+	static constexpr int SB = BK + (CX ? 2 : 4);      // Bs[c][k]
+	static constexpr int TILE_A = BK * SA;
+	static constexpr int TILE_B = BN * SB;
+	static constexpr int STAGE = TILE_A + TILE_B;     // elements of T
+	static constexpr int KMAX = 512;                  // largest K of the scale vectors
+	static constexpr int SMEM_BYTES = STAGES * STAGE * (int)sizeof(T)
+	                                  + (2 * KMAX + BM + BN) * (int)sizeof(double) + KMAX * 4;
 	static constexpr int WTM = BM / WM, WTN = BN / WN;
 	static constexpr int MT = WTM / 8, NT = WTN / 8;
 	static constexpr int A_PER_T = (BM * BK + THREADS - 1) / THREADS;
@@ -67,13 +104,19 @@ struct GemmCfg {
 	static_assert(BK % 4 == 0, "BK multiple of 4");
 };
 
-template <typename T, int BM, int BN, int BK, int WM, int WN>
+template <typename T, int BM, int BN, int BK, int WM, int WN, int STAGES, int MODE>
 __global__ void __launch_bounds__(WM *WN * 32)
 k_gemm(GemmArgs<T> g)
 {
-	using Cfg = GemmCfg<T, BM, BN, BK, WM, WN>;
-	constexpr bool CX = is_cplx<T>::value;
-	extern __shared__ double sm[];
+	using Cfg = GemmCfg<T, BM, BN, BK, WM, WN, STAGES>;
+	constexpr bool CX = Cfg::CX;
+	extern __shared__ __align__(16) unsigned char smraw[];
+	T *sm = (T *)smraw;
+	double *sdk = (double *)(smraw + STAGES * Cfg::STAGE * sizeof(T));   // per-k scale
+	double *sdk2 = sdk + Cfg::KMAX;                                       // per-k 1/d (A_DD)
+	double *sdr = sdk2 + Cfg::KMAX;                                       // per-row (A_DD)
+	double *sdc = sdr + BM;                                               // per-column (B_COLD)
+	int *sgi = (int *)(sdc + BN);                                         // gather rows
 	const int b = blockIdx.z;
 	const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
 	if (b >= g.batch || m0 >= g.M || n0 >= g.N) return;
@@ -82,131 +125,139 @@ k_gemm(GemmArgs<T> g)
 	const T *A = g.A + g.aA.off(b);
 	const T *B = g.B + g.aB.off(b);
 	T *Cp = g.C + g.aC.off(b);
-	const double *d = (g.mode & (GM_A_DD | GM_B_ROWD | GM_B_COLD)) ? g.d + g.aD.off(b) : nullptr;
-	const double *dinv = (g.mode & GM_A_DD) ? g.dinv + g.aD.off(b) : nullptr;
-	const int *gi = (g.mode & GM_B_GATHER) ? g.gidx + g.aG.off(b) : nullptr;
 	const int M = g.M, N = g.N, K = g.K;
 
-	double acc_r[Cfg::MT][Cfg::NT][2], acc_i[CX ? Cfg::MT : 1][CX ? Cfg::NT : 1][2];
-#pragma unroll
-	for (int i = 0; i < Cfg::MT; i++)
-#pragma unroll
-		for (int j = 0; j < Cfg::NT; j++) {
-			acc_r[i][j][0] = acc_r[i][j][1] = 0.0;
-			if (CX) acc_i[CX ? i : 0][CX ? j : 0][0] = acc_i[CX ? i : 0][CX ? j : 0][1] = 0.0;
+	// scale vectors and gather indices for this item, staged once
+	if (MODE & (GM_A_DD | GM_B_ROWD | GM_B_COLD)) {
+		const double *d = g.d + g.aD.off(b);
+		if (MODE & GM_A_DD) {
+			const double *di = g.dinv + g.aD.off(b);
+			for (int q = tid; q < K; q += Cfg::THREADS) sdk2[q] = di[q];
+			for (int q = tid; q < BM; q += Cfg::THREADS) sdr[q] = (m0 + q < M) ? d[m0 + q] : 0.0;
 		}
+		if (MODE & GM_B_ROWD)
+			for (int q = tid; q < K; q += Cfg::THREADS) sdk[q] = d[q];
+		if (MODE & GM_B_COLD)
+			for (int q = tid; q < BN; q += Cfg::THREADS) sdc[q] = (n0 + q < N) ? d[n0 + q] : 0.0;
+	}
+	if (MODE & GM_B_GATHER) {
+		const int *gi = g.gidx + g.aG.off(b);
+		for (int q = tid; q < K; q += Cfg::THREADS) sgi[q] = gi[q];
+	}
+	if (MODE & (GM_A_DD | GM_B_ROWD | GM_B_COLD | GM_B_GATHER)) __syncthreads();
 
 	int kt0 = 0;
-	if (g.mode & GM_A_UPPER) kt0 = m0 / BK;
+	if (MODE & GM_A_UPPER) kt0 = m0 / BK;
 	const int nkt = (K + BK - 1) / BK;
 
-	T ra[Cfg::A_PER_T], rb[Cfg::B_PER_T];
-	auto load = [&](int kt) {
+	auto issue = [&](int kt, int stage) {
+		T *As = sm + stage * Cfg::STAGE;
+		T *Bs = As + Cfg::TILE_A;
 		const int k0 = kt * BK;
-#pragma unroll
-		for (int q = 0; q < Cfg::A_PER_T; q++) {
-			const int idx = tid + q * Cfg::THREADS;
-			const int r = idx % BM, k = idx / BM;
-			const int gr = m0 + r, gk = k0 + k;
-			T v = zero<T>();
-			if (idx < BM * BK && gr < M && gk < K) {
-				if (!((g.mode & GM_A_UPPER) && gr > gk)) {
-					v = A[gr + (long long)gk * g.lda];
-					if (g.mode & GM_A_DD) v = v * (d[gr] * dinv[gk]);
-				}
-			}
-			ra[q] = v;
-		}
-#pragma unroll
-		for (int q = 0; q < Cfg::B_PER_T; q++) {
-			const int idx = tid + q * Cfg::THREADS;
-			const int k = idx % BK, c = idx / BK;
-			const int gk = k0 + k, gc = n0 + c;
-			T v = zero<T>();
-			if (idx < BK * BN && gk < K && gc < N) {
-				if (g.mode & GM_B_IDENT) {
-					v = (gk == gc) ? one<T>() : zero<T>();
-				} else {
-					const int row = gi ? gi[gk] : gk;
-					v = B[row + (long long)gc * g.ldb];
-				}
-				if (g.mode & GM_B_ROWD) v = v * d[gk];
-				if (g.mode & GM_B_COLD) v = v * d[gc];
-			}
-			rb[q] = v;
-		}
-	};
-	auto store = [&](int stage) {
-		double *As = sm + stage * Cfg::STAGE;
-		double *Bs = As + Cfg::PLANES * Cfg::SMEM_A;
 #pragma unroll
 		for (int q = 0; q < Cfg::A_PER_T; q++) {
 			const int idx = tid + q * Cfg::THREADS;
 			if (idx < BM * BK) {
 				const int r = idx % BM, k = idx / BM;
-				double xr, xi;
-				split(ra[q], xr, xi);
-				As[k * Cfg::SA + r] = xr;
-				if (CX) As[Cfg::SMEM_A + k * Cfg::SA + r] = xi;
+				const int gr = m0 + r, gk = k0 + k;
+				const bool ok = gr < M && gk < K;
+				cp_async_el<T>(As + k * Cfg::SA + r, ok ? A + gr + (long long)gk * g.lda : A, ok);
 			}
 		}
+		if (!(MODE & GM_B_IDENT)) {
 #pragma unroll
-		for (int q = 0; q < Cfg::B_PER_T; q++) {
-			const int idx = tid + q * Cfg::THREADS;
-			if (idx < BK * BN) {
-				const int k = idx % BK, c = idx / BK;
-				double xr, xi;
-				split(rb[q], xr, xi);
-				Bs[c * Cfg::SB + k] = xr;
-				if (CX) Bs[Cfg::SMEM_B + c * Cfg::SB + k] = xi;
+			for (int q = 0; q < Cfg::B_PER_T; q++) {
+				const int idx = tid + q * Cfg::THREADS;
+				if (idx < BK * BN) {
+					const int k = idx % BK, c = idx / BK;
+					const int gk = k0 + k, gc = n0 + c;
+					const bool ok = gk < K && gc < N;
+					int row = gk;
+					if (MODE & GM_B_GATHER) row = ok ? sgi[gk] : 0;
+					cp_async_el<T>(Bs + c * Cfg::SB + k, ok ? B + row + (long long)gc * g.ldb : B, ok);
+				}
 			}
 		}
 	};
 
-	const int gq = lane >> 2, tq = lane & 3;
-	int stage = 0;
-	if (kt0 < nkt) {
-		load(kt0);
-		store(0);
+	double acc_r[Cfg::MT][Cfg::NT][2];
+	double acc_i[CX ? Cfg::MT : 1][CX ? Cfg::NT : 1][2];
+#pragma unroll
+	for (int i = 0; i < Cfg::MT; i++)
+#pragma unroll
+		for (int j = 0; j < Cfg::NT; j++) {
+			acc_r[i][j][0] = acc_r[i][j][1] = 0.0;
+			if constexpr (CX) acc_i[i][j][0] = acc_i[i][j][1] = 0.0;
+		}
+
+	// prologue
+#pragma unroll
+	for (int sidx = 0; sidx < STAGES - 1; sidx++) {
+		if (kt0 + sidx < nkt) issue(kt0 + sidx, sidx);
+		cp_commit();
 	}
-	__syncthreads();
+	const int gq = lane >> 2, tq = lane & 3;
 	for (int kt = kt0; kt < nkt; kt++) {
-		const bool more = kt + 1 < nkt;
-		if (more) load(kt + 1);
-		const double *As = sm + stage * Cfg::STAGE;
-		const double *Bs = As + Cfg::PLANES * Cfg::SMEM_A;
+		cp_wait<STAGES - 2>();
+		__syncthreads();
+		{
+			const int nk = kt + STAGES - 1;
+			if (nk < nkt) issue(nk, (nk - kt0) % STAGES);
+			cp_commit();
+		}
+		const int stage = (kt - kt0) % STAGES;
+		const T *As = sm + stage * Cfg::STAGE;
+		const T *Bs = As + Cfg::TILE_A;
+		const int k0 = kt * BK;
 #pragma unroll
 		for (int kk = 0; kk < BK; kk += 4) {
+			const int gk = k0 + kk + tq;
 			double fa[Cfg::MT], fb[Cfg::NT], fai[CX ? Cfg::MT : 1], fbi[CX ? Cfg::NT : 1];
+			double ka = 1.0, kb = 1.0;
+			if (MODE & GM_A_DD) ka = (gk < K) ? sdk2[gk] : 0.0;
+			if (MODE & GM_B_ROWD) kb = (gk < K) ? sdk[gk] : 0.0;
 #pragma unroll
 			for (int i = 0; i < Cfg::MT; i++) {
 				const int r = wm * Cfg::WTM + i * 8 + gq;
-				fa[i] = As[(kk + tq) * Cfg::SA + r];
-				if (CX) fai[CX ? i : 0] = As[Cfg::SMEM_A + (kk + tq) * Cfg::SA + r];
+				const T v = As[(kk + tq) * Cfg::SA + r];
+				double xr, xi;
+				split(v, xr, xi);
+				double sc = ka;
+				if (MODE & GM_A_DD) sc *= sdr[r];
+				if ((MODE & GM_A_UPPER) && (m0 + r > gk)) sc = 0.0;
+				fa[i] = xr * sc;
+				if constexpr (CX) fai[i] = xi * sc;
 			}
 #pragma unroll
 			for (int j = 0; j < Cfg::NT; j++) {
 				const int c = wn * Cfg::WTN + j * 8 + gq;
-				fb[j] = Bs[c * Cfg::SB + kk + tq];
-				if (CX) fbi[CX ? j : 0] = Bs[Cfg::SMEM_B + c * Cfg::SB + kk + tq];
+				double xr, xi;
+				if (MODE & GM_B_IDENT) {
+					xr = (gk == n0 + c) ? 1.0 : 0.0;
+					xi = 0.0;
+				} else {
+					const T v = Bs[c * Cfg::SB + kk + tq];
+					split(v, xr, xi);
+				}
+				double sc = kb;
+				if (MODE & GM_B_COLD) sc *= sdc[c];
+				fb[j] = xr * sc;
+				if constexpr (CX) fbi[j] = xi * sc;
 			}
 #pragma unroll
 			for (int i = 0; i < Cfg::MT; i++)
 #pragma unroll
 				for (int j = 0; j < Cfg::NT; j++) {
 					dmma(acc_r[i][j][0], acc_r[i][j][1], fa[i], fb[j]);
-					if (CX) {
-						const int ii = CX ? i : 0, jj = CX ? j : 0;
-						dmma(acc_r[i][j][0], acc_r[i][j][1], -fai[ii], fbi[jj]);
-						dmma(acc_i[ii][jj][0], acc_i[ii][jj][1], fa[i], fbi[jj]);
-						dmma(acc_i[ii][jj][0], acc_i[ii][jj][1], fai[ii], fb[j]);
+					if constexpr (CX) {
+						dmma(acc_r[i][j][0], acc_r[i][j][1], -fai[i], fbi[j]);
+						dmma(acc_i[i][j][0], acc_i[i][j][1], fa[i], fbi[j]);
+						dmma(acc_i[i][j][0], acc_i[i][j][1], fai[i], fb[j]);
 					}
 				}
 		}
-		if (more) store(stage ^ 1);
-		__syncthreads();
-		stage ^= 1;
 	}
+	cp_wait<0>();
 
 	// epilogue: lane holds C[gq][2 tq + {0,1}] of each 8x8 tile
 	const bool use_beta = !(re(g.beta) == 0.0 && im(g.beta) == 0.0);

@@ -5,6 +5,12 @@
 //   warp w owns columns c = w + NW*q (q < CPW), lane l owns rows l + 32*p
 //   (p < RPL); Householder vectors and scalars live in shared memory.
 //
+// Every elimination step updates all CPW columns of a warp at once: the CPW
+// dot products are accumulated independently and reduced together with
+// interleaved butterfly shuffles, and columns that take no part are masked
+// arithmetically, so the work of a step is straight-line code with CPW-fold
+// instruction-level parallelism.
+//
 // k_qr      Householder QR that picks, at each step, which remaining column
 //           to eliminate next, so no columns are moved:
 //             QR_PIVOT   largest remaining partial column norm, with the norm
@@ -40,12 +46,6 @@ struct QrArgs {
 	unsigned *err;
 };
 
-template <typename T, int RPL, int CPW, int NW>
-struct QrShape {
-	static constexpr int NMAX = 32 * RPL < NW * CPW ? 32 * RPL : NW * CPW;
-	static constexpr int THREADS = NW * 32;
-};
-
 template <typename T>
 size_t qr_smem_bytes(int N, int nw)
 {
@@ -53,18 +53,28 @@ size_t qr_smem_bytes(int N, int nw)
 	       + sizeof(int) * (3 * (size_t)N + 2 * nw) + 64;
 }
 
-// select slot q of a register array with a compile-time bound
-template <typename T, int NQ>
-__device__ inline T pick(const T (&arr)[NQ], int q)
+// value of row r (uniform across the warp) from the lane that holds it
+template <typename T, int RPL>
+__device__ inline T row_of(const T (&col)[RPL], int r, int lane)
 {
-	T v = arr[0];
+	T v = zero<T>();
 #pragma unroll
-	for (int i = 1; i < NQ; i++)
-		if (i == q) v = arr[i];
-	return v;
+	for (int p = 0; p < RPL; p++)
+		if (lane + 32 * p == r) v = col[p];
+	return shfl(v, r & 31);
 }
 
-template <typename T, int RPL, int CPW, int NW>
+// CPW independent warp sums, their butterfly stages interleaved
+template <typename T, int CPW>
+__device__ inline void warp_sums(T (&s)[CPW])
+{
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+		for (int q = 0; q < CPW; q++) s[q] += shfl_xor(s[q], o);
+}
+
+template <typename T, int RPL, int CPW, int NW, int MODE>
 __global__ void __launch_bounds__(NW * 32) k_qr(QrArgs<T> a)
 {
 	const int item = blockIdx.x;
@@ -74,72 +84,101 @@ __global__ void __launch_bounds__(NW * 32) k_qr(QrArgs<T> a)
 	extern __shared__ __align__(16) unsigned char smraw[];
 	T *V = (T *)smraw;                          // N*N reflectors, column j = v_j
 	T *tau = V + (size_t)N * N;                 // N
-	double *vn1 = (double *)(tau + N);          // N partial norms
-	double *vn2 = vn1 + N;                      // N norms at last recompute
+	double *vn1 = (double *)(tau + N);          // N column norms (partial norms when pivoting)
+	double *vn2 = vn1 + N;                      // N norms at the last recompute
 	double *dsh = vn2 + N;                      // N diag(R)
 	double *vv = dsh + N;                       // N  v^H v
 	double *cval = vv + N;                      // NW candidate norms
-	int *used = (int *)(cval + NW);             // N  column eliminated?
-	int *pvt = used + N;                        // N  column chosen at step j
-	int *pos = pvt + N;                         // N  step at which column c was chosen
-	int *ccol = pos + N;                        // NW candidate columns
+	int *pvt = (int *)(cval + NW);              // N  column chosen at step j
+	int *ccol = pvt + N;                        // NW candidate columns
 	__shared__ int s_col;
 
 	const T *X = a.X + (size_t)item * a.x_stride;
 	T x[CPW][RPL];
+	int posr[CPW];    // step at which each own column is eliminated (N: not yet)
 #pragma unroll
 	for (int q = 0; q < CPW; q++) {
 		const int c = w + NW * q;
-		const double sc = (a.mode == QR_PRESORT && c < N) ? a.dcol[(size_t)item * a.d_stride + c] : 1.0;
+		const double sc = (MODE == QR_PRESORT && c < N) ? a.dcol[(size_t)item * a.d_stride + c] : 1.0;
 #pragma unroll
 		for (int p = 0; p < RPL; p++) {
 			const int r = lane + 32 * p;
 			x[q][p] = (c < N && r < N) ? X[r + (size_t)N * c] * sc : zero<T>();
 		}
+		posr[q] = N;
 	}
-	for (int c = tid; c < N; c += blockDim.x) used[c] = 0;
-	// column norms
+	// column norms (squared)
+	{
+		double s[CPW];
 #pragma unroll
-	for (int q = 0; q < CPW; q++) {
-		double s = 0.0;
+		for (int q = 0; q < CPW; q++) {
+			s[q] = 0.0;
 #pragma unroll
-		for (int p = 0; p < RPL; p++) s += abs2(x[q][p]);
-		s = warp_sum(s);
-		const int c = w + NW * q;
-		if (lane == 0 && c < N) {
-			vn1[c] = (a.mode == QR_PIVOT) ? sqrt(s) : s;
-			vn2[c] = vn1[c];
+			for (int p = 0; p < RPL; p++) s[q] += abs2(x[q][p]);
+		}
+		warp_sums(s);
+#pragma unroll
+		for (int q = 0; q < CPW; q++) {
+			const int c = w + NW * q;
+			const double v = (MODE == QR_PIVOT) ? sqrt(s[q]) : s[q];
+			if (lane == 0 && c < N) {
+				vn1[c] = v;
+				vn2[c] = v;
+			}
 		}
 	}
 	__syncthreads();
-	if (a.mode == QR_PRESORT) {
+	if (MODE == QR_PRESORT) {
 		// stable descending order of the squared norms (greens.c:123-129)
+		// (a NaN norm ranks last, so the order stays a permutation)
 		for (int c = tid; c < N; c += blockDim.x) {
-			const double v = vn1[c];
+			double v = vn1[c];
+			if (!(v >= 0.0)) {
+				v = -1.0;
+				if (a.err) atomicOr(a.err, DQ_ERR_NAN);
+			}
 			int rank = 0;
 			for (int o = 0; o < N; o++) {
-				const double u = vn1[o];
+				double u = vn1[o];
+				if (!(u >= 0.0)) u = -1.0;
 				rank += (u > v) || (u == v && o < c);
 			}
 			pvt[rank] = c;
-			pos[c] = rank;
 		}
 		__syncthreads();
+		// reload in pivot-position order: slot q of warp w holds position
+		// q*NW + w, so eliminated columns are whole slots that later steps skip
+#pragma unroll
+		for (int q = 0; q < CPW; q++) {
+			const int jq = q * NW + w;
+			const int c = jq < N ? pvt[jq] : 0;
+			const double sc = jq < N ? a.dcol[(size_t)item * a.d_stride + c] : 0.0;
+#pragma unroll
+			for (int p = 0; p < RPL; p++) {
+				const int r = lane + 32 * p;
+				x[q][p] = (jq < N && r < N) ? X[r + (size_t)N * c] * sc : zero<T>();
+			}
+			posr[q] = jq < N ? jq : N;
+		}
 	}
 
 	const double tol3z = sqrt(2.220446049250313e-16);
 	for (int j = 0; j < N; j++) {
 		int cj;
-		if (a.mode == QR_PIVOT) {
-			// warp candidates: largest partial norm among remaining columns
+		if (MODE == QR_PIVOT) {
+			// warp candidate: largest partial norm among remaining own columns
 			double best = -1.0;
 			int bc = N;
 #pragma unroll
 			for (int q = 0; q < CPW; q++) {
 				const int c = w + NW * q;
-				if (c < N && !used[c]) {
-					const double v = vn1[c];
-					if (v > best || (v == best && c < bc)) { best = v; bc = c; }
+				if (c < N && posr[q] == N) {
+					double v = vn1[c];
+					if (!(v >= 0.0)) v = -0.5;   // NaN: last choice, still a candidate
+					if (v > best || (v == best && c < bc)) {
+						best = v;
+						bc = c;
+					}
 				}
 			}
 			if (lane == 0) { cval[w] = best; ccol[w] = bc; }
@@ -149,16 +188,27 @@ __global__ void __launch_bounds__(NW * 32) k_qr(QrArgs<T> a)
 				int bcol = N;
 				for (int q = 0; q < NW; q++)
 					if (cval[q] > bb || (cval[q] == bb && ccol[q] < bcol)) { bb = cval[q]; bcol = ccol[q]; }
+				if (bcol >= N) {
+					// no finite candidate (NaN norms): take the first unused column
+					if (a.err) atomicOr(a.err, DQ_ERR_NAN);
+					for (int q = 0; q < N; q++) {
+						bool taken = false;
+						for (int jj = 0; jj < j; jj++) taken |= (pvt[jj] == q);
+						if (!taken) { bcol = q; break; }
+					}
+				}
 				s_col = bcol;
 				pvt[j] = bcol;
-				pos[bcol] = j;
-				used[bcol] = 1;
 			}
 			__syncthreads();
 			cj = s_col;
+			if (cj % NW == w) {
+#pragma unroll
+				for (int q = 0; q < CPW; q++)
+					if (q == cj / NW) posr[q] = j;
+			}
 		} else {
-			cj = pvt[j];
-			if (tid == 0) used[cj] = 1;
+			cj = j;     // position order: step j eliminates slot j / NW of warp j % NW
 		}
 		const int ow = cj % NW, oq = cj / NW;
 		if (w == ow) {
@@ -173,15 +223,13 @@ __global__ void __launch_bounds__(NW * 32) k_qr(QrArgs<T> a)
 			}
 			// alpha = row j, sigma = sum over rows > j
 			double sig = 0.0;
-			T alpha = zero<T>();
 #pragma unroll
 			for (int p = 0; p < RPL; p++) {
 				const int r = lane + 32 * p;
 				if (r > j && r < N) sig += abs2(col[p]);
-				if (r == j) alpha = col[p];
 			}
 			sig = warp_sum(sig);
-			alpha = shfl(alpha, j & 31);
+			const T alpha = row_of(col, j, lane);
 			const double anorm2 = abs2(alpha);
 			T tj, scal;
 			double beta;
@@ -219,73 +267,105 @@ __global__ void __launch_bounds__(NW * 32) k_qr(QrArgs<T> a)
 					for (int p = 0; p < RPL; p++) x[q][p] = col[p];
 		}
 		__syncthreads();
-		// apply H_j^H = I - conj(tau) v v^H to the remaining columns
+		// apply H_j^H = I - conj(tau) v v^H to every remaining own column;
+		// v is zero above row j, so row blocks p < j/32 take no part, and in
+		// position order (PRESORT) whole slots are already eliminated
 		const T ct = conjv(tau[j]);
+		const int pa = j >> 5;
 		T vr[RPL];
 #pragma unroll
 		for (int p = 0; p < RPL; p++) {
 			const int r = lane + 32 * p;
-			vr[p] = (r < N) ? V[r + (size_t)N * j] : zero<T>();
+			vr[p] = (p >= pa && r < N) ? V[r + (size_t)N * j] : zero<T>();
 		}
+		T s[CPW];
 #pragma unroll
 		for (int q = 0; q < CPW; q++) {
-			const int c = w + NW * q;
-			if (c >= N || c == cj) continue;
-			if (a.mode == QR_PIVOT ? used[c] : (pos[c] <= j)) continue;
-			T s = zero<T>();
+			s[q] = zero<T>();
 #pragma unroll
-			for (int p = 0; p < RPL; p++) s = fma_(conjv(vr[p]), x[q][p], s);
-			s = warp_sum(s);
-			const T f = ct * s;
+			for (int p = 0; p < RPL; p++) s[q] = fma_(conjv(vr[p]), x[q][p], s[q]);
+		}
+		warp_sums(s);
+#pragma unroll
+		for (int q = 0; q < CPW; q++) {
+			const bool act = (MODE == QR_PRESORT) ? (q * NW + w > j) : (posr[q] > j);
+			const T f = act ? ct * s[q] : zero<T>();
 #pragma unroll
 			for (int p = 0; p < RPL; p++) x[q][p] = x[q][p] - vr[p] * f;
-			if (a.mode == QR_PIVOT && vn1[c] != 0.0) {
-				// partial norm downdate (LAPACK dlaqp2)
-				T xj = zero<T>();
+		}
+		if (MODE == QR_PIVOT) {
+			// partial norm downdate over rows > j (LAPACK dlaqp2); the norms of
+			// a warp's columns are private to it (lane 0 writes them)
+			T xj[CPW];
+#pragma unroll
+			for (int q = 0; q < CPW; q++) {
+				T v = zero<T>();
 #pragma unroll
 				for (int p = 0; p < RPL; p++)
-					if (lane + 32 * p == j) xj = x[q][p];
-				xj = shfl(xj, j & 31);
-				double t = absv(xj) / vn1[c];
+					if (lane + 32 * p == j) v = x[q][p];
+				xj[q] = v;
+			}
+#pragma unroll
+			for (int q = 0; q < CPW; q++) xj[q] = shfl(xj[q], j & 31);
+			bool need = false;
+			double nv[CPW];
+			bool rec[CPW];
+#pragma unroll
+			for (int q = 0; q < CPW; q++) {
+				const int c = w + NW * q;
+				const double n1 = (c < N) ? vn1[c] : 0.0, n2 = (c < N) ? vn2[c] : 1.0;
+				const bool act = posr[q] == N && c < N && n1 != 0.0;
+				double t = act ? absv(xj[q]) / n1 : 0.0;
 				t = fmax(0.0, 1.0 - t * t);
-				const double t2 = t * (vn1[c] / vn2[c]) * (vn1[c] / vn2[c]);
-				double nv;
-				const bool recompute = t2 <= tol3z;
-				if (recompute) {
-					double s2 = 0.0;
+				const double t2 = act ? t * (n1 / n2) * (n1 / n2) : 1.0;
+				rec[q] = act && t2 <= tol3z;
+				need |= rec[q];
+				nv[q] = act ? n1 * sqrt(t) : n1;
+			}
+			if (need) {
+				double s2[CPW];
+#pragma unroll
+				for (int q = 0; q < CPW; q++) {
+					s2[q] = 0.0;
 #pragma unroll
 					for (int p = 0; p < RPL; p++)
-						if (lane + 32 * p > j && lane + 32 * p < N) s2 += abs2(x[q][p]);
-					s2 = warp_sum(s2);
-					nv = sqrt(s2);
-				} else {
-					nv = vn1[c] * sqrt(t);
+						if (lane + 32 * p > j && lane + 32 * p < N) s2[q] += abs2(x[q][p]);
 				}
-				__syncwarp();
-				if (lane == 0) {
-					vn1[c] = nv;
-					if (recompute) vn2[c] = nv;
-				}
-				__syncwarp();
+				warp_sums(s2);
+#pragma unroll
+				for (int q = 0; q < CPW; q++)
+					if (rec[q]) nv[q] = sqrt(s2[q]);
 			}
+			__syncwarp();
+			if (lane == 0) {
+#pragma unroll
+				for (int q = 0; q < CPW; q++) {
+					const int c = w + NW * q;
+					if (c < N && posr[q] == N) {
+						vn1[c] = nv[q];
+						if (rec[q]) vn2[c] = nv[q];
+					}
+				}
+			}
+			__syncwarp();
 		}
 	}
 	__syncthreads();
 
-	// R outputs: the register column of original index c holds R[:, pos[c]]
-	const size_t NN = (size_t)N * N;
+	// R outputs: PIVOT slots hold original columns c (R[:, posr]); PRESORT
+	// slots hold positions
 #pragma unroll
 	for (int q = 0; q < CPW; q++) {
 		const int c = w + NW * q;
 		if (c >= N) continue;
-		const int jc = pos[c];
+		const int jc = (MODE == QR_PRESORT) ? c : posr[q];
 #pragma unroll
 		for (int p = 0; p < RPL; p++) {
 			const int r = lane + 32 * p;
 			if (r >= N) continue;
 			const double dr = dsh[r] == 0.0 ? 1.0 : dsh[r];
 			const T v = (r <= jc) ? x[q][p] / dr : zero<T>();
-			if (a.mode == QR_PIVOT) a.Tout[(size_t)item * a.t_stride + r + (size_t)N * c] = v;
+			if (MODE == QR_PIVOT) a.Tout[(size_t)item * a.t_stride + r + (size_t)N * c] = v;
 			else a.Rs[(size_t)item * a.r_stride + r + (size_t)N * jc] = v;
 		}
 	}
@@ -293,7 +373,6 @@ __global__ void __launch_bounds__(NW * 32) k_qr(QrArgs<T> a)
 		a.dout[(size_t)item * a.dout_stride + r] = dsh[r] == 0.0 ? 1.0 : dsh[r];
 		if (a.pvt) a.pvt[(size_t)item * a.p_stride + r] = pvt[r];
 	}
-	(void)NN;
 
 	// explicit Q = H_0 H_1 ... H_{N-1}: columns by position, reflectors backwards
 #pragma unroll
@@ -304,21 +383,24 @@ __global__ void __launch_bounds__(NW * 32) k_qr(QrArgs<T> a)
 	}
 	for (int j = N - 1; j >= 0; j--) {
 		const T tj = tau[j];
+		const int pa = j >> 5;
 		T vr[RPL];
 #pragma unroll
 		for (int p = 0; p < RPL; p++) {
 			const int r = lane + 32 * p;
-			vr[p] = (r < N) ? V[r + (size_t)N * j] : zero<T>();
+			vr[p] = (p >= pa && r < N) ? V[r + (size_t)N * j] : zero<T>();
 		}
+		T s[CPW];
 #pragma unroll
 		for (int q = 0; q < CPW; q++) {
-			const int c = w + NW * q;
-			if (c < j || c >= N) continue;
-			T s = zero<T>();
+			s[q] = zero<T>();
 #pragma unroll
-			for (int p = 0; p < RPL; p++) s = fma_(conjv(vr[p]), x[q][p], s);
-			s = warp_sum(s);
-			const T f = tj * s;
+			for (int p = 0; p < RPL; p++) s[q] = fma_(conjv(vr[p]), x[q][p], s[q]);
+		}
+		warp_sums(s);
+#pragma unroll
+		for (int q = 0; q < CPW; q++) {
+			const T f = (w + NW * q >= j) ? tj * s[q] : zero<T>();
 #pragma unroll
 			for (int p = 0; p < RPL; p++) x[q][p] = x[q][p] - vr[p] * f;
 		}
@@ -384,6 +466,7 @@ __global__ void __launch_bounds__(NW * 32) k_recombine(RecArgs<T> a)
 		if (fabs(dr) > 1.0) { vsh[r] = 1.0 / dr; dss[r] = 1.0; }
 		else { vsh[r] = 1.0; dss[r] = dr; }
 		rused[r] = 0;
+		stepof[r] = N;
 	}
 	__syncthreads();
 	// M = diag(v) Q^H + diag(ds) T
@@ -398,6 +481,10 @@ __global__ void __launch_bounds__(NW * 32) k_recombine(RecArgs<T> a)
 			                           : zero<T>();
 		}
 	}
+	// rows of this lane still free to become pivots
+	bool freer[RPL];
+#pragma unroll
+	for (int p = 0; p < RPL; p++) freer[p] = lane + 32 * p < N;
 	// LU, implicit partial pivoting: rows stay put, prow[j] is the pivot row
 	for (int j = 0; j < N; j++) {
 		const int ow = j % NW, oq = j / NW;
@@ -416,7 +503,7 @@ __global__ void __launch_bounds__(NW * 32) k_recombine(RecArgs<T> a)
 #pragma unroll
 			for (int p = 0; p < RPL; p++) {
 				const int r = lane + 32 * p;
-				if (r < N && !rused[r]) {
+				if (freer[p]) {
 					const double m = absv(col[p]);
 					if (m > best || (m == best && r < br)) { best = m; br = r; }
 				}
@@ -426,11 +513,17 @@ __global__ void __launch_bounds__(NW * 32) k_recombine(RecArgs<T> a)
 				const int orr = __shfl_xor_sync(0xffffffffu, br, o);
 				if (ob > best || (ob == best && orr < br)) { best = ob; br = orr; }
 			}
-			T piv = zero<T>();
+			if (br >= N) {
+				// no comparable candidate (NaN column): first free row
+				if (lane == 0 && a.err) atomicOr(a.err, DQ_ERR_NAN);
+				int fr = N;
 #pragma unroll
-			for (int p = 0; p < RPL; p++)
-				if (lane + 32 * p == br) piv = col[p];
-			piv = shfl(piv, br & 31);
+				for (int p = 0; p < RPL; p++)
+					if (freer[p] && lane + 32 * p < fr) fr = lane + 32 * p;
+				for (int o = 16; o > 0; o >>= 1) fr = min(fr, __shfl_xor_sync(0xffffffffu, fr, o));
+				br = fr < N ? fr : 0;
+			}
+			T piv = row_of(col, br, lane);
 			if (re(piv) == 0.0 && im(piv) == 0.0) {
 				if (lane == 0 && a.err) atomicOr(a.err, DQ_ERR_SINGULAR);
 				piv = one<T>();
@@ -440,9 +533,10 @@ __global__ void __launch_bounds__(NW * 32) k_recombine(RecArgs<T> a)
 			for (int p = 0; p < RPL; p++) {
 				const int r = lane + 32 * p;
 				if (r < N) {
-					const T l = (!rused[r] && r != br) ? col[p] * ipiv : zero<T>();
+					const bool el = freer[p] && r != br;
+					const T l = el ? col[p] * ipiv : zero<T>();
 					lcol[r] = l;
-					if (!rused[r] && r != br) LU[r + (size_t)N * j] = l;
+					if (el) LU[r + (size_t)N * j] = l;
 				}
 			}
 			if (lane == 0) {
@@ -453,24 +547,31 @@ __global__ void __launch_bounds__(NW * 32) k_recombine(RecArgs<T> a)
 		}
 		__syncthreads();
 		const int pr = s_prow;
-		if (tid == 0) rused[pr] = 1;
+#pragma unroll
+		for (int p = 0; p < RPL; p++)
+			if (lane + 32 * p == pr) freer[p] = false;
 		T lr[RPL];
 #pragma unroll
 		for (int p = 0; p < RPL; p++) {
 			const int r = lane + 32 * p;
 			lr[p] = (r < N) ? lcol[r] : zero<T>();
 		}
+		T xp[CPW];
 #pragma unroll
 		for (int q = 0; q < CPW; q++) {
-			const int c = w + NW * q;
-			if (c <= j || c >= N) continue;
-			T xp = zero<T>();
+			T v = zero<T>();
 #pragma unroll
 			for (int p = 0; p < RPL; p++)
-				if (lane + 32 * p == pr) xp = x[q][p];
-			xp = shfl(xp, pr & 31);
+				if (lane + 32 * p == pr) v = x[q][p];
+			xp[q] = v;
+		}
 #pragma unroll
-			for (int p = 0; p < RPL; p++) x[q][p] = x[q][p] - lr[p] * xp;
+		for (int q = 0; q < CPW; q++) xp[q] = shfl(xp[q], pr & 31);
+#pragma unroll
+		for (int q = 0; q < CPW; q++) {
+			const T f = (w + NW * q > j) ? xp[q] : zero<T>();
+#pragma unroll
+			for (int p = 0; p < RPL; p++) x[q][p] = x[q][p] - lr[p] * f;
 		}
 		__syncthreads();
 	}
@@ -512,16 +613,21 @@ __global__ void __launch_bounds__(NW * 32) k_recombine(RecArgs<T> a)
 			const int r = lane + 32 * p;
 			m[p] = (r < N && sr[p] > j) ? LU[r + (size_t)N * j] : zero<T>();
 		}
+		T yp[CPW];
 #pragma unroll
 		for (int q = 0; q < CPW; q++) {
-			T yp = zero<T>();
+			T v = zero<T>();
 #pragma unroll
 			for (int p = 0; p < RPL; p++)
-				if (lane + 32 * p == pr) yp = x[q][p];
-			yp = shfl(yp, pr & 31);
-#pragma unroll
-			for (int p = 0; p < RPL; p++) x[q][p] = x[q][p] - m[p] * yp;
+				if (lane + 32 * p == pr) v = x[q][p];
+			yp[q] = v;
 		}
+#pragma unroll
+		for (int q = 0; q < CPW; q++) yp[q] = shfl(yp[q], pr & 31);
+#pragma unroll
+		for (int q = 0; q < CPW; q++)
+#pragma unroll
+			for (int p = 0; p < RPL; p++) x[q][p] = x[q][p] - m[p] * yp[q];
 	}
 	// backward: x_j = y[prow j] / U_jj, then remove it from earlier pivot rows
 	for (int j = N - 1; j >= 0; j--) {
@@ -534,19 +640,24 @@ __global__ void __launch_bounds__(NW * 32) k_recombine(RecArgs<T> a)
 			const int r = lane + 32 * p;
 			u[p] = (r < N && sr[p] < j) ? LU[r + (size_t)N * j] : zero<T>();
 		}
+		T yp[CPW];
 #pragma unroll
 		for (int q = 0; q < CPW; q++) {
-			T yp = zero<T>();
+			T v = zero<T>();
 #pragma unroll
 			for (int p = 0; p < RPL; p++)
-				if (lane + 32 * p == pr) yp = x[q][p];
-			yp = shfl(yp, pr & 31) * iu;
+				if (lane + 32 * p == pr) v = x[q][p];
+			yp[q] = v;
+		}
+#pragma unroll
+		for (int q = 0; q < CPW; q++) yp[q] = shfl(yp[q], pr & 31) * iu;
+#pragma unroll
+		for (int q = 0; q < CPW; q++)
 #pragma unroll
 			for (int p = 0; p < RPL; p++) {
-				if (lane + 32 * p == pr) x[q][p] = yp;
-				else x[q][p] = x[q][p] - u[p] * yp;
+				if (lane + 32 * p == pr) x[q][p] = yp[q];
+				else x[q][p] = x[q][p] - u[p] * yp[q];
 			}
-		}
 	}
 	T *G = a.G + (size_t)item * a.g_stride;
 #pragma unroll
@@ -573,7 +684,11 @@ __global__ void __launch_bounds__(NW * 32) k_recombine(RecArgs<T> a)
 		for (int j = 0; j < N; j++) {
 			if (rused[j]) continue;
 			int len = 0, q = j;
-			while (!rused[q]) { rused[q] = 1; q = prow[q]; len++; }
+			while (q >= 0 && q < N && !rused[q] && len <= N) { rused[q] = 1; q = prow[q]; len++; }
+			if (q < 0 || q >= N) {
+				if (a.err) atomicOr(a.err, DQ_ERR_NAN);
+				break;
+			}
 			parity ^= (len - 1) & 1;
 		}
 		if (parity) ph = ph * -1.0;

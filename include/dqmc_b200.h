@@ -78,7 +78,9 @@ void dqmc_engine_destroy(dqmc_engine *e);
 
 /* Per-chain state (host arrays, copied): exp_lambda[2N], del[2N] as in the
  * sim file, rng[17], hs[L*N] (hs[i + N*l]), and the sweep counter (equal
- * for every chain of an engine). */
+ * for every chain of an engine).  The equal-time G of every chain is
+ * recomputed from the fields before the next sweep (as the reference does
+ * when it starts from a file, dqmc.c:188-220). */
 int dqmc_engine_set_chain(dqmc_engine *e, int chain, const double *exp_lambda,
 		const double *del, const uint64_t *rng, const int *hs, int sweep);
 int dqmc_engine_set_acc(dqmc_engine *e, int chain, int eq_n_sample,
@@ -120,6 +122,15 @@ int dqmc_engine_profile_sweep(dqmc_engine *e, int meas_eq, int meas_ue, double *
  * problems laid out back to back.  Each mirrors one reference function.
  * stream: a cudaStream_t passed as void* (NULL = default stream).
  * ------------------------------------------------------------------------ */
+
+/* xgemm("N", "N", ...) (src/linalg_generic.h:23-40) for `batch` column-major
+ * problems: C_b = alpha A_b B_b + beta C_b with A_b = A + b*stride_a (M x K,
+ * leading dimension lda) and likewise B (K x N), C (M x N); K <= 512.
+ * alpha, beta: host pointers to one num.  Asynchronous on `stream`. */
+int dqmc_gpu_gemm(int batch, int M, int N, int K, int cplx, const void *alpha,
+		const void *A, int lda, long long stride_a, const void *B, int ldb,
+		long long stride_b, const void *beta, void *C, int ldc, long long stride_c,
+		void *stream);
 
 /* calc_eq_g (src/greens.c:69-208, called as calc_eq_g(l, N, F, 2, C, g, ...)
  * by dqmc.c:202, 288): G = (I + C_{l-1} ... C_{l})^-1 from F cluster

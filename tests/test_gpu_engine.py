@@ -271,3 +271,86 @@ def test_batched_chains_match_single(eng, golden, tmp_path):
         np.testing.assert_allclose(one.eq_acc, sims[k].eq_acc, rtol=1e-12, atol=1e-12)
         e1.close()
     e.close()
+
+
+# ---- larger lattices, inputs from the engine's own generator ------------------
+
+def _gen_case(tmp_path, Nx, Ny, **kw):
+    from dqmc_b200 import gen, simfile
+    d = gen.make_sim(Nx=Nx, Ny=Ny, seed=17, **kw)
+    path = str(tmp_path / f"g{Nx}x{Ny}.h5")
+    simfile.write(path, d)
+    return path
+
+
+@pytest.mark.parametrize("Nx,Ny", [(10, 10), (12, 12), (16, 10)])
+def test_calc_eq_g_seam_large(eng, Nx, Ny, tmp_path):
+    import torch
+    from dqmc_b200 import lib
+    path = _gen_case(tmp_path, Nx, Ny, U=4.0, mu=-1.0, dt=0.05, L=40, n_matmul=5, n_delay=16,
+                     period_eqlt=8)
+    o = Sim(path)
+    N, F, nmul = o.N, o.p["F"], o.p["n_matmul"]
+    for spin in (0, 1):
+        B, Cm = _clusters(o, spin, F, nmul, o.hs)
+        for l in (0, 3):
+            g_o = np.zeros(N * N, o.nt)
+            ph_o = np.zeros(1, o.nt)
+            oracle_lib(o.cplx).orc_calc_eq_g(l, N, F, 2, C.c_void_p(Cm.ctypes.data),
+                                             C.c_void_p(g_o.ctypes.data),
+                                             C.c_void_p(ph_o.ctypes.data))
+            dC = torch.from_numpy(Cm).cuda()
+            dG = torch.zeros(N * N, dtype=dC.dtype, device="cuda")
+            dph = torch.zeros(1, dtype=dC.dtype, device="cuda")
+            rc = lib.load().dqmc_gpu_calc_eq_g(1, N, F, l, int(o.cplx), dC.data_ptr(),
+                                               dG.data_ptr(), dph.data_ptr(), None)
+            assert rc == 0
+            g = dG.cpu().numpy()
+            assert np.all(np.isfinite(g))
+            assert np.max(np.abs(g - g_o)) < G_TOL
+            assert abs(dph.cpu().numpy()[0] - ph_o[0]) < 1e-12
+
+
+@pytest.mark.parametrize("Nx,Ny", [(12, 12)])
+def test_engine_large_matches_oracle(eng, Nx, Ny, tmp_path):
+    """2 sweeps of a 12x12 chain (L = 20): HS fields and RNG bit-exact, G and
+    the equal-time measurements within tolerance of the oracle."""
+    path = _gen_case(tmp_path, Nx, Ny, U=4.0, mu=-1.0, dt=0.05, L=20, n_matmul=5, n_delay=16,
+                     period_eqlt=5, n_sweep_warm=0, n_sweep_meas=2)
+    o = Sim(path)
+    gu_o, gd_o, ph_o = o.run(stop_sweep=2)
+    s, e = _run(eng, path, 2)
+    assert np.array_equal(s.hs, o.hs)
+    assert np.array_equal(s.rng, o.rng)
+    gu, gd, ph = e.g(0)
+    assert np.max(np.abs(gu - gu_o)) < G_TOL
+    assert np.max(np.abs(gd - gd_o)) < G_TOL
+    for k, v in o.eq.items():
+        mine = s.measurements()["meas_eqlt/" + k]
+        np.testing.assert_allclose(mine, v, rtol=MEAS_RTOL, atol=MEAS_RTOL * max(1, np.abs(v).max()),
+                                   err_msg=k)
+    e.close()
+
+
+def test_many_chains_stay_finite(eng, tmp_path):
+    """A batch at the benchmark shape runs several sweeps without device errors
+    and with finite Green's functions."""
+    from dqmc_b200 import gen
+    rngs = gen.chain_rngs(3, 16)
+    base = gen.make_sim(Nx=12, Ny=12, U=4.0, mu=-1.0, dt=0.05, L=40, n_matmul=10, n_delay=16,
+                        period_eqlt=8, n_sweep_warm=0, n_sweep_meas=6, init_rng=rngs[0])
+    sims = []
+    for r in rngs:
+        d = dict(base)
+        hs, rr = gen.initial_hs(r, 40, 144)
+        d["state/hs"], d["state/rng"] = hs, rr
+        sims.append(eng.SimData(d))
+    e = eng.Engine(sims)
+    e.init()
+    e.sweeps(3, sync=False)
+    e.sync()
+    assert e.errors() == 0
+    for c in range(len(sims)):
+        gu, gd, ph = e.g(c)
+        assert np.all(np.isfinite(gu)) and np.all(np.isfinite(gd))
+    e.close()
