@@ -9,6 +9,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <vector>
 
 #include "dqmc_b200.h"
@@ -1209,3 +1210,92 @@ int dqmc_gpu_mul_seq(int batch, int N, int n, int spin, int cplx, const void *ex
 }
 
 }  // extern "C"
+
+// ------------------------------------------- calc_eq_g without allocation
+//
+// Scratch of dqmc_gpu_calc_eq_g_noalloc: one array per device, created when
+// the library's module loads and held until the process exits.  Host code
+// must not pass `noalloc_scratch` itself to a kernel -- on the host that name
+// is a stand-in, not a device address; the device address comes from
+// cudaGetSymbolAddress below, once per device.
+
+static __device__ __align__(256) unsigned char noalloc_scratch[DQMC_NOALLOC_SCRATCH_BYTES];
+
+static std::mutex noalloc_mu;
+static void *noalloc_ptr[64];  // device address of the array, per device id
+
+static size_t al256(size_t n) { return (n + 255) & ~(size_t)255; }
+
+// bytes calc_eq_g needs for `batch` items of size N: six N x N work
+// matrices per item, the column norms, the pivots, det(Q) and the error word
+template <typename T>
+static size_t noalloc_bytes(int batch, int N)
+{
+	const size_t NN = (size_t)N * N;
+	return 6 * al256(sizeof(T) * batch * NN) + al256(sizeof(double) * batch * N) +
+	       al256(sizeof(int) * batch * N) + al256(sizeof(T) * batch) + al256(sizeof(unsigned));
+}
+
+static int noalloc_base(unsigned char **base)
+{
+	int dev = 0;
+	CK(cudaGetDevice(&dev));
+	if (dev < 0 || dev >= 64) return DQMC_E_ARG;
+	std::lock_guard<std::mutex> lk(noalloc_mu);
+	if (!noalloc_ptr[dev]) {
+		void *p = nullptr;
+		CK(cudaGetSymbolAddress(&p, noalloc_scratch));
+		noalloc_ptr[dev] = p;
+	}
+	*base = (unsigned char *)noalloc_ptr[dev];
+	return 0;
+}
+
+template <typename T>
+static int noalloc_calc_eq_g(int batch, int N, int F, int l, const void *C, void *G, void *phase,
+		cudaStream_t st)
+{
+	if (batch < 1 || N < 1 || N > max_dense_n<T>() || F < 1 || l < 0 || l >= F || !C || !G || !phase)
+		return DQMC_E_ARG;
+	const size_t need = noalloc_bytes<T>(batch, N);
+	if (need > (size_t)DQMC_NOALLOC_SCRATCH_BYTES) {
+		fprintf(stderr, "dqmc_gpu_calc_eq_g_noalloc: batch %d of N = %d needs %zu bytes of "
+		        "scratch, more than the %d the library holds\n", batch, N, need,
+		        (int)DQMC_NOALLOC_SCRATCH_BYTES);
+		return DQMC_E_SCRATCH;
+	}
+	unsigned char *p = nullptr;
+	const int rc0 = noalloc_base(&p);
+	if (rc0) return rc0;
+	const size_t NN = (size_t)N * N;
+	auto take = [&](size_t bytes) { unsigned char *q = p; p += al256(bytes); return (void *)q; };
+	EqWork<T> w;
+	w.N = N; w.F = F; w.NB = batch;
+	w.Cl = (const T *)C; w.cl_stride = (long long)F * NN;
+	w.Qm = (T *)take(sizeof(T) * batch * NN); w.Tm = (T *)take(sizeof(T) * batch * NN);
+	w.Tm2 = (T *)take(sizeof(T) * batch * NN); w.Rs = (T *)take(sizeof(T) * batch * NN);
+	w.X = (T *)take(sizeof(T) * batch * NN); w.W = (T *)take(sizeof(T) * batch * NN);
+	w.dR = (double *)take(sizeof(double) * batch * N);
+	w.pvt = (int *)take(sizeof(int) * batch * N);
+	w.qdet = (T *)take(sizeof(T) * batch);
+	w.err = (unsigned *)take(sizeof(unsigned));
+	w.G = (T *)G; w.g_stride = NN;
+	w.phi = (T *)phase;
+	// the error word keeps the previous call's value: clear it in stream order
+	CK(cudaMemsetAsync(w.err, 0, sizeof(unsigned), st));
+	const int rc = run_calc_eq_g<T>(w, l, st, nullptr);
+	if (rc) return rc;
+	unsigned e = 0;
+	CK(cudaMemcpyAsync(&e, w.err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+	CK(cudaStreamSynchronize(st));
+	CK(cudaGetLastError());
+	return e ? DQMC_E_DEVICE : 0;
+}
+
+extern "C" int dqmc_gpu_calc_eq_g_noalloc(int batch, int N, int F, int l, int cplx, const void *C,
+		void *G, void *phase, void *stream)
+{
+	cudaStream_t st = (cudaStream_t)stream;
+	return cplx ? noalloc_calc_eq_g<zd>(batch, N, F, l, C, G, phase, st)
+	            : noalloc_calc_eq_g<double>(batch, N, F, l, C, G, phase, st);
+}

@@ -17,6 +17,8 @@ DQMC_E_ARG = -10
 DQMC_E_CUDA = -11
 DQMC_E_NOMEM = -12
 DQMC_E_DEVICE = -13
+DQMC_E_SCRATCH = -14
+NOALLOC_SCRATCH_BYTES = 16 << 20   # DQMC_NOALLOC_SCRATCH_BYTES
 
 # every symbol include/dqmc_b200.h declares
 EXPORTS = [
@@ -27,6 +29,7 @@ EXPORTS = [
     "dqmc_engine_accepts", "dqmc_engine_stream", "dqmc_engine_launches_per_sweep",
     "dqmc_engine_profile_sweep",
     "dqmc_gpu_gemm", "dqmc_gpu_calc_eq_g", "dqmc_gpu_update_delayed", "dqmc_gpu_mul_seq",
+    "dqmc_gpu_calc_eq_g_noalloc",
 ]
 
 
@@ -82,6 +85,7 @@ def load(path: str | None = None):
         "dqmc_gpu_gemm": (i, [i, i, i, i, i, vp, vp, i, C.c_longlong, vp, i, C.c_longlong, vp,
                               vp, i, C.c_longlong, vp]),
         "dqmc_gpu_calc_eq_g": (i, [i, i, i, i, i, vp, vp, vp, vp]),
+        "dqmc_gpu_calc_eq_g_noalloc": (i, [i, i, i, i, i, vp, vp, vp, vp]),
         "dqmc_gpu_update_delayed": (i, [i, i, i, i, vp, vp, vp, vp, vp, vp]),
         "dqmc_gpu_mul_seq": (i, [i, i, i, i, i, vp, vp, vp, vp, vp]),
     }

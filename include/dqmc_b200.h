@@ -25,6 +25,7 @@ enum {
 	DQMC_E_CUDA = -11,     /* CUDA runtime error (no device, launch failure) */
 	DQMC_E_NOMEM = -12,    /* device allocation failed */
 	DQMC_E_DEVICE = -13,   /* a kernel reported an error (see dqmc_engine_errors) */
+	DQMC_E_SCRATCH = -14,  /* the problem does not fit the library's fixed scratch */
 };
 
 /* ---------------------------------------------------------------------------
@@ -154,6 +155,33 @@ int dqmc_gpu_update_delayed(int batch, int N, int n_delay, int cplx,
 int dqmc_gpu_mul_seq(int batch, int N, int n, int spin, int cplx,
 		const void *exp_K, const double *exp_lambda, const int *hs, void *C,
 		void *stream);
+
+/* Size of the fixed device scratch of dqmc_gpu_calc_eq_g_noalloc (16 MiB).
+ * A call needs 6*batch*N*N*sizeof(num) + batch*N*12 + batch*sizeof(num)
+ * bytes, each part rounded up to 256: e.g. up to 80 problems of N = 64 or
+ * 16 problems of N = 144 (real), 13 problems of N = 112 (complex). */
+#define DQMC_NOALLOC_SCRATCH_BYTES (16 << 20)
+
+/* dqmc_gpu_calc_eq_g without any device allocation; no counterpart in the
+ * reference.  Same arguments, results and status codes as
+ * dqmc_gpu_calc_eq_g, which allocates its work matrices with cudaMalloc on
+ * every call.  Some callers cannot allow that: a process whose free device
+ * memory is already reserved by another allocator (a framework's caching
+ * allocator that holds the HBM, so cudaMalloc fails), or a driver that keeps
+ * sweeps queued on other streams and cannot take the device-wide
+ * synchronisation that cudaFree implies.  This variant works in one static
+ * device array of DQMC_NOALLOC_SCRATCH_BYTES that the library holds on every
+ * device it loads on until the process exits, and returns DQMC_E_SCRATCH
+ * (with a message on stderr) when batch x N does not fit it.
+ * - The first call on a device looks up the array's device address (no
+ *   allocation); make that first call before any stream capture on it.
+ * - Every call on a device shares the one array and it keeps the previous
+ *   call's contents (the error word is cleared at the start of each call):
+ *   calls that overlap on the GPU -- from several threads, or on several
+ *   streams -- race and give wrong results.  Serialise them.
+ * Like dqmc_gpu_calc_eq_g it synchronises `stream` before it returns. */
+int dqmc_gpu_calc_eq_g_noalloc(int batch, int N, int F, int l, int cplx,
+		const void *C, void *G, void *phase, void *stream);
 
 #ifdef __cplusplus
 }
