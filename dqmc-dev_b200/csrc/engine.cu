@@ -47,8 +47,13 @@ static int launch_gemm_mode(const GemmArgs<T> &g, cudaStream_t st)
 			return DQMC_E_ARG;
 		attr = true;
 	}
-	dim3 grid((g.M + BM - 1) / BM, (g.N + BN - 1) / BN, g.batch);
-	k_gemm<T, BM, BN, BK, WM, WN, ST, MODE><<<grid, Cfg::THREADS, Cfg::SMEM_BYTES, st>>>(g);
+	// the grid's z extent is at most 65535: larger batches take several launches
+	for (int b0 = 0; b0 < g.batch; b0 += 65535) {
+		GemmArgs<T> gc = g;
+		gc.b0 = b0;
+		dim3 grid((g.M + BM - 1) / BM, (g.N + BN - 1) / BN, min(65535, g.batch - b0));
+		k_gemm<T, BM, BN, BK, WM, WN, ST, MODE><<<grid, Cfg::THREADS, Cfg::SMEM_BYTES, st>>>(gc);
+	}
 	return 0;
 }
 
@@ -71,7 +76,9 @@ static int launch_gemm_cfg(const GemmArgs<T> &g, cudaStream_t st)
 template <typename T>
 int launch_gemm(const GemmArgs<T> &g, cudaStream_t st)
 {
-	if (g.K > 512 || g.M < 1 || g.N < 1 || g.K < 1 || g.batch < 1) return DQMC_E_ARG;
+	// the scale vectors and gather indices of these modes are staged per K
+	const bool k_staged = g.mode & (GM_A_DD | GM_B_ROWD | GM_B_GATHER);
+	if ((k_staged && g.K > 512) || g.M < 1 || g.N < 1 || g.K < 1 || g.batch < 1) return DQMC_E_ARG;
 	auto pad = [&](int t) { return (long long)((g.M + t - 1) / t * t) * ((g.N + t - 1) / t * t); };
 	const long long p64 = pad(64), p48 = pad(48), p32 = pad(32);
 	if constexpr (is_cplx<T>::value) {
@@ -478,7 +485,7 @@ struct Group : GroupBase {
 		if (N < 1 || L < 1 || F < 1 || nmul < 1 || L != F * nmul || N > max_dense_n<T>() ||
 		    N > 480 || C < 1)
 			return DQMC_E_ARG;
-		if (p.period_uneqlt > 0 && !UneqState<T>::supported(N, F)) return DQMC_E_ARG;
+		if (p.period_uneqlt > 0 && !UneqState<T>::supported(N, F, L)) return DQMC_E_ARG;
 		CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
 		const size_t NN = (size_t)N * N;
 		int rc = 0;
@@ -720,23 +727,183 @@ struct Group : GroupBase {
 		watchdog("k_meas_eqlt");
 	}
 
+	// ------------------------------------------------ unequal-time G
+
+	// stack[l][item] through a table of slice indices, one entry per group
+	Addr slice_addr(int tab_off) const
+	{
+		const long long NN = (long long)N * N;
+		return Addr{(long long)NB * NN, NN, NB, ue.dtab + tab_off};
+	}
+
+	int launch_hqr(const HqrArgs<T> &h)
+	{
+		constexpr int NBK = 8, NW = 16;
+		const size_t sm = hqr_smem_bytes<T, NBK, NW>(h.M);
+		auto go = [&](auto kern) -> int {
+			CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+			kern<<<h.batch, NW * 32, sm, st>>>(h);
+			launch_count++;
+			return 0;
+		};
+		if (h.M <= 64) return go(k_hqr<T, NBK, 2, NW>);
+		if (h.M <= 128) return go(k_hqr<T, NBK, 4, NW>);
+		if (h.M <= 224) return go(k_hqr<T, NBK, 7, NW>);
+		if (h.M <= 320) return go(k_hqr<T, NBK, 10, NW>);
+		return DQMC_E_ARG;
+	}
+
+	// G(0,t), G(t,t), G(t,0) of every slice from this sweep's clusters
+	// (calc_ue_g, greens.c:471-494, with N_MUL = 2 as dqmc.c:399 calls it)
+	int calc_ue_g()
+	{
+		const size_t NN = (size_t)N * N;
+		const int E = ue.E, NE = ue.NE;
+		const long long NE2 = (long long)NE * NE, q4 = 4LL * (long long)NN;
+		const long long qstride = (long long)std::max(E - 1, 1) * q4;
+		prof_begin(3);
+		k_build_bib<T><<<grid_for((long long)L * NB * NN), 256, 0, st>>>(N, L, NB, expK.p, iexpK.p,
+		                                                               dv.p, dvi.p, ue.Bs.p, ue.iBs.p);
+		launch_count++;
+		// calc_o (greens.c:247-264): I on the diagonal, -C_{2e+1} C_{2e} at
+		// (e+1, e), the remaining clusters' product at (0, E-1)
+		CK(cudaMemsetAsync(ue.O.p, 0, sizeof(T) * NB * NE2, st));
+		if (E > 1)
+			gemm(gargs<T>(N, N, N, NB * (E - 1), Cl.p + NN, Addr{(long long)(F * NN), 2LL * (long long)NN, E - 1},
+			              N, Cl.p, Addr{(long long)(F * NN), 2LL * (long long)NN, E - 1}, N, ue.O.p + N,
+			              Addr{NE2, (long long)N * (1 + NE), E - 1}, NE, from_re<T>(-1.0), zero<T>()));
+		T *corner = ue.O.p + (size_t)(E - 1) * N * NE;
+		if (F - 2 * (E - 1) == 2)
+			gemm(gargs<T>(N, N, N, NB, Cl.p + (size_t)(F - 1) * NN, per_item((long long)F * NN), N,
+			              Cl.p + (size_t)(F - 2) * NN, per_item((long long)F * NN), N, corner,
+			              per_item(NE2), NE));
+		else {
+			k_copy2d<T><<<grid_for((long long)NB * NN), 256, 0, st>>>(N, N, NB, Cl.p + (size_t)(F - 1) * NN,
+			        (long long)F * NN, N, corner, NE2, NE, one<T>());
+			launch_count++;
+		}
+		k_add_diag<T><<<grid_for((long long)NE * NB), 256, 0, st>>>(NE, NB, ue.O.p, NE2);
+		launch_count++;
+		// bsofi (greens.c:266-337): QR of the 2N x N panels, Q^H carried to
+		// the block columns l+1 and E-1 in the same kernel
+		for (int l = 0; l + 2 < E; l++) {
+			HqrArgs<T> h;
+			memset(&h, 0, sizeof(h));
+			h.M = 2 * N; h.n = N; h.batch = NB;
+			h.A = ue.O.p + (size_t)l * N * (1 + NE); h.aA = per_item(NE2); h.lda = NE;
+			h.nx1 = N;
+			h.nx2 = N; h.X = ue.O.p + (size_t)l * N + (size_t)(E - 1) * N * NE; h.aX = per_item(NE2);
+			h.Qh = ue.Qh.p + (size_t)l * q4; h.aQ = per_item(qstride);
+			h.err = err.p;
+			if (launch_hqr(h)) return DQMC_E_ARG;
+		}
+		const int lf = std::max(E - 2, 0), wf = (E >= 2) ? 2 * N : N;
+		{
+			HqrArgs<T> h;
+			memset(&h, 0, sizeof(h));
+			h.M = wf; h.n = wf; h.batch = NB;
+			h.A = ue.O.p + (size_t)lf * N * (1 + NE); h.aA = per_item(NE2); h.lda = NE;
+			h.Qh = ue.Qh.p + (size_t)lf * q4; h.aQ = per_item(qstride);
+			h.err = err.p;
+			if (launch_hqr(h)) return DQMC_E_ARG;
+		}
+		// R^-1: diagonal blocks, then the blocks d above the diagonal,
+		// X(i, i+d) = -X(i, i) R(i, i+1..i+d) X(i+1..i+d, i+d)
+		CK(cudaMemsetAsync(ue.Gr.p, 0, sizeof(T) * NB * NE2, st));
+		{
+			TriArgs<T> t{N, NE, E, NB, ue.O.p, ue.Gr.p, err.p};
+			const size_t sm = trtri_smem_bytes<T>(N);
+			CK(cudaFuncSetAttribute(k_trtri<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+			k_trtri<T><<<NB * E, 256, sm, st>>>(t);
+			launch_count++;
+		}
+		for (int d = 1; d < E; d++) {
+			const int na = E - d;
+			const Addr dg{NE2, (long long)N * (1 + NE), na};
+			gemm(gargs<T>(N, N, d * N, NB * na, ue.O.p + (size_t)N * NE, dg, NE,
+			              ue.Gr.p + N + (size_t)d * N * NE, dg, NE, ue.Tw.p, per_item((long long)NN), N));
+			gemm(gargs<T>(N, N, N, NB * na, ue.Gr.p, dg, NE, ue.Tw.p, per_item((long long)NN), N,
+			              ue.Gr.p + (size_t)d * N * NE, dg, NE, from_re<T>(-1.0), zero<T>()));
+		}
+		// O^-1 = R^-1 Q_{E-2}^H ... Q_0^H, each on its two block columns
+		for (int l = lf; l >= 0; l--) {
+			T *cols = ue.Gr.p + (size_t)l * N * NE;
+			k_copy2d<T><<<grid_for((long long)NB * NE * wf), 256, 0, st>>>(NE, wf, NB, cols, NE2, NE,
+			        ue.Rw.p, (long long)NE * wf, NE, one<T>());
+			launch_count++;
+			gemm(gargs<T>(NE, wf, wf, NB, ue.Rw.p, per_item((long long)NE * wf), NE,
+			              ue.Qh.p + (size_t)l * q4, per_item(qstride), wf, cols, per_item(NE2), NE));
+		}
+		// expand_g (greens.c:339-469)
+		k_ue_seed<T><<<grid_for((long long)NB * E * NN), 256, 0, st>>>(N, E, NB, ue.plan.nme, ue.Gr.p,
+		                                                              ue.G0t.p, ue.Gtt.p, ue.Gt0.p);
+		launch_count++;
+		const long long sl = (long long)NB * NN;     // one slice of a stack
+		for (const UeOp &o : ue.plan.ops) {
+			T *stk = (o.kind < 2) ? ue.G0t.p : (o.kind < 4) ? ue.Gtt.p : ue.Gt0.p;
+			// operands per kind: A, B, C (and D, the second GEMM's A, for Gtt)
+			T *opA, *opB, *opD = nullptr;
+			switch (o.kind) {
+			case 0: opA = stk; opB = ue.Bs.p; break;
+			case 1: opA = stk; opB = ue.iBs.p; break;
+			case 2: opA = stk; opB = ue.Bs.p; opD = ue.iBs.p; break;
+			case 3: opA = stk; opB = ue.iBs.p; opD = ue.Bs.p; break;
+			case 4: opA = ue.iBs.p; opB = stk; break;
+			default: opA = ue.Bs.p; opB = stk; break;
+			}
+			if (!o.special) {
+				const int bt = o.nact * NB;
+				const Addr tA = slice_addr(o.tab), tB = slice_addr(o.tab + o.nact);
+				const Addr tC = slice_addr(o.tab + 2 * o.nact), tD = slice_addr(o.tab + 3 * o.nact);
+				if (opD) {
+					gemm(gargs<T>(N, N, N, bt, opA, tA, N, opB, tB, N, ue.Cw.p, per_item((long long)NN), N));
+					gemm(gargs<T>(N, N, N, bt, opD, tD, N, ue.Cw.p, per_item((long long)NN), N, stk, tC, N));
+				} else {
+					gemm(gargs<T>(N, N, N, bt, opA, tA, N, opB, tB, N, stk, tC, N));
+				}
+				continue;
+			}
+			const Addr ai = per_item((long long)NN);
+			auto at = [&](T *base, int k) { return base + UePlan::slice_of(o.kind, k, o.m, o.next) * sl; };
+			T *dst = at(stk, 2);
+			if (o.prefill) {
+				const T *src = (o.prefill == 1) ? ue.iBs.p + o.m * sl
+				             : (o.prefill == 2) ? ue.iBs.p + o.next * sl : nullptr;
+				k_copy2d<T><<<grid_for((long long)NB * NN), 256, 0, st>>>(N, N, NB, src, (long long)NN, N, dst,
+				        (long long)NN, N, one<T>());
+				launch_count++;
+			}
+			gemm(gargs<T>(N, N, N, NB, at(opA, 0), ai, N, at(opB, 1), ai, N, dst, ai, N,
+			              from_re<T>(o.alpha), from_re<T>(o.beta)));
+		}
+		prof_end(3, 0.0, 0.0);
+		watchdog("calc_ue_g");
+		return 0;
+	}
+
 	int meas_uneqlt()
 	{
 		const size_t NN = (size_t)N * N;
-		int rc = ue.compute(*this);
+		int rc = calc_ue_g();
 		if (rc) return rc;
-		// half wrap of all 3 L matrices per item (dqmc.c:415-451)
+		// half wrap of all 3 L slices per item (dqmc.c:415-451); the B stack
+		// is free again and holds the intermediate product
 		T *stk[3] = {ue.G0t.p, ue.Gtt.p, ue.Gt0.p};
-		for (int q = 0; q < 3; q++)
-			for (int l = 0; l < L; l++)
-				half_wrap(stk[q] + (size_t)l * NN, per_item((long long)L * NN), stk[q] + (size_t)l * NN,
-				          per_item((long long)L * NN), NB);
+		for (int q = 0; q < 3; q++) {
+			gemm(gargs<T>(N, N, N, L * NB, stk[q], per_item((long long)NN), N, ehK.p, per_spin((long long)NN), N,
+			              ue.Bs.p, per_item((long long)NN), N));
+			gemm(gargs<T>(N, N, N, L * NB, iehK.p, per_spin((long long)NN), N, ue.Bs.p, per_item((long long)NN),
+			              N, stk[q], per_item((long long)NN), N));
+		}
 		MeasArgs<T> m = meas_args();
 		m.G0t = ue.G0t.p; m.Gtt = ue.Gtt.p; m.Gt0 = ue.Gt0.p;
 		m.acc = acc_ue.p; m.acc_stride = ue_size; m.n_sample = n_ue.p;
 		m.bond = p.meas_bond_corr;
+		prof_begin(4);
 		k_meas_uneqlt<T><<<dim3(C, L), 256, 0, st>>>(m);
+		prof_end(4, 0.0, 0.0);
 		launch_count++;
+		watchdog("k_meas_uneqlt");
 		return 0;
 	}
 

@@ -36,10 +36,18 @@ enum : int {
 	GM_B_IDENT = 32,
 };
 
+// off(b) = q * hi + (b % div) * lo with q = b / div, or q = tab[b / div]
+// when a table is given (the slice of each group of `div` items, for the
+// unequal-time slice chains, whose slices wrap around modulo L)
 struct Addr {
 	long long hi, lo;
 	int div;
-	__host__ __device__ long long off(int b) const { return (long long)(b / div) * hi + (long long)(b % div) * lo; }
+	const int *tab;
+	__host__ __device__ long long off(int b) const
+	{
+		const int q = b / div;
+		return (long long)(tab ? tab[q] : q) * hi + (long long)(b % div) * lo;
+	}
 };
 
 template <typename T>
@@ -52,6 +60,7 @@ struct GemmArgs {
 	int mode;
 	const double *d; const double *dinv; Addr aD;   // scaling vectors (length K or M)
 	const int *gidx; Addr aG;                       // row gather for B
+	int b0;                                         // first item of this launch
 };
 
 __device__ inline void cp_async8(void *smem, const void *gmem, bool valid)
@@ -117,7 +126,7 @@ k_gemm(GemmArgs<T> g)
 	double *sdr = sdk2 + Cfg::KMAX;                                       // per-row (A_DD)
 	double *sdc = sdr + BM;                                               // per-column (B_COLD)
 	int *sgi = (int *)(sdc + BN);                                         // gather rows
-	const int b = blockIdx.z;
+	const int b = g.b0 + blockIdx.z;
 	const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
 	if (b >= g.batch || m0 >= g.M || n0 >= g.N) return;
 	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;

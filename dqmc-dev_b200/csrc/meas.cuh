@@ -127,10 +127,11 @@ __global__ void k_meas_uneqlt(MeasArgs<T> a)
 	if (c >= a.nchain || t >= a.L) return;
 	const int N = a.N, L = a.L;
 	const size_t NN = (size_t)N * N;
-	const size_t su = ((size_t)2 * c) * L * NN, sd = su + (size_t)L * NN;
-	const T *u0t = a.G0t + su + NN * t, *utt = a.Gtt + su + NN * t, *ut0 = a.Gt0 + su + NN * t;
-	const T *d0t = a.G0t + sd + NN * t, *dtt = a.Gtt + sd + NN * t, *dt0 = a.Gt0 + sd + NN * t;
-	const T *u00 = a.Gtt + su, *d00 = a.Gtt + sd;
+	// slice-major stacks: slice t of item b at (t * 2 nchain + b) N^2
+	const size_t su = ((size_t)t * 2 * a.nchain + 2 * c) * NN, sd = su + NN;
+	const T *u0t = a.G0t + su, *utt = a.Gtt + su, *ut0 = a.Gt0 + su;
+	const T *d0t = a.G0t + sd, *dtt = a.Gtt + sd, *dt0 = a.Gt0 + sd;
+	const T *u00 = a.Gtt + (size_t)2 * c * NN, *d00 = u00 + NN;
 	const T phase = a.phase[c];
 	T *acc = a.acc + (size_t)c * a.acc_stride;
 	const int nij = a.num_ij;

@@ -126,7 +126,7 @@ int dqmc_engine_profile_sweep(dqmc_engine *e, int meas_eq, int meas_ue, double *
 
 /* xgemm("N", "N", ...) (src/linalg_generic.h:23-40) for `batch` column-major
  * problems: C_b = alpha A_b B_b + beta C_b with A_b = A + b*stride_a (M x K,
- * leading dimension lda) and likewise B (K x N), C (M x N); K <= 512.
+ * leading dimension lda) and likewise B (K x N), C (M x N).
  * alpha, beta: host pointers to one num.  Asynchronous on `stream`. */
 int dqmc_gpu_gemm(int batch, int M, int N, int K, int cplx, const void *alpha,
 		const void *A, int lda, long long stride_a, const void *B, int ldb,

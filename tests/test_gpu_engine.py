@@ -96,6 +96,39 @@ def test_engine_uneqlt_matches_reference(eng, golden, case, tmp_path):
     e.close()
 
 
+def _assert_meas_oracle(s, o, rtol=MEAS_RTOL):
+    m = s.measurements()
+    groups = [("meas_eqlt/", o.eq, o.eq_sign)]
+    if s.p["period_uneqlt"] > 0:
+        groups.append(("meas_uneqlt/", o.ue, o.ue_sign))
+    for pre, d, sign in groups:
+        np.testing.assert_allclose(np.asarray(m[pre + "sign"]).reshape(-1), sign.reshape(-1),
+                                   rtol=rtol, err_msg=pre + "sign")
+        for k, r in d.items():
+            v = np.asarray(m[pre + k]).reshape(-1)
+            r = r.reshape(-1)
+            scale = max(np.max(np.abs(r)), 1.0)
+            np.testing.assert_allclose(v, r, rtol=rtol, atol=rtol * scale, err_msg=pre + k)
+
+
+# more groups E = 1 + (F-1)/2 than the reference fixtures have (E = 2, 3):
+# several panel QRs in bsofi, blocks two and more above the diagonal in
+# R^-1, and expand_g chains of uneven length; one complex case with flux
+@pytest.mark.parametrize("Nx,L,nmul,nflux", [(4, 40, 4, 0), (6, 48, 4, 0), (4, 36, 3, 0), (4, 36, 4, 0),
+                                             (4, 40, 4, 1), (4, 8, 4, 0)])
+def test_engine_uneqlt_matches_oracle_generated(eng, Nx, L, nmul, nflux, tmp_path):
+    path = _gen_case(tmp_path, Nx, Nx, U=4.0, mu=-0.5, tp=-0.2, dt=0.1, L=L, n_matmul=nmul,
+                     n_delay=4, period_eqlt=nmul, period_uneqlt=1, meas_bond_corr=1, nflux=nflux,
+                     n_sweep_warm=1, n_sweep_meas=2)
+    o = Sim(path)
+    o.run()
+    s, e = _run(eng, path)
+    assert np.array_equal(s.hs, o.hs)
+    assert s.ue_n == int(o.ue_n[0])
+    _assert_meas_oracle(s, o)
+    e.close()
+
+
 # kagome at U = 6, beta = 4 is the least well-conditioned case: two FP64
 # stabilised computations agree to a few 1e-9 there, the square cases to 1e-10
 @pytest.mark.parametrize("case,n,tol", [("c1_small", 3, G_TOL), ("sq8_small", 2, G_TOL),
