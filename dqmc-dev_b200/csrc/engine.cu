@@ -161,10 +161,45 @@ template <typename T> constexpr int max_dense_n() { return is_cplx<T>::value ? 1
 	X(144, 5, 9, 16)                    \
 	X(160, 5, 10, 16)
 
+template <typename T, int RPL>
+static int launch_qrb_rpl(const QrArgs<T> &a, cudaStream_t st)
+{
+	constexpr int NW = 16, NBK = 8;
+	const size_t sm = qrb_smem_bytes<T, NBK>(a.N);
+	static size_t attr = 0;
+	if (sm > attr) {
+		if (cudaFuncSetAttribute(k_qrb<T, NW, NBK, RPL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		                         (int)sm) != cudaSuccess)
+			return DQMC_E_ARG;
+		attr = sm;
+	}
+	k_qrb<T, NW, NBK, RPL><<<a.batch, NW * 32, sm, st>>>(a);
+	return 0;
+}
+
+// the blocked pre-sorted QR wherever its N x N matrix fits in shared memory
+template <typename T>
+static bool use_qrb(const QrArgs<T> &a)
+{
+	return a.mode == QR_PRESORT && qrb_smem_bytes<T, 8>(a.N) <= 227 * 1024;
+}
+
+template <typename T>
+static int launch_qrb(const QrArgs<T> &a, cudaStream_t st)
+{
+	if (a.N <= 32) return launch_qrb_rpl<T, 1>(a, st);
+	if (a.N <= 64) return launch_qrb_rpl<T, 2>(a, st);
+	if (a.N <= 96) return launch_qrb_rpl<T, 3>(a, st);
+	if (a.N <= 128) return launch_qrb_rpl<T, 4>(a, st);
+	if (a.N <= 160) return launch_qrb_rpl<T, 5>(a, st);
+	return DQMC_E_ARG;
+}
+
 template <typename T>
 int launch_qr(const QrArgs<T> &a, cudaStream_t st)
 {
 	if (a.N < 1 || a.N > max_dense_n<T>()) return DQMC_E_ARG;
+	if (use_qrb(a)) return launch_qrb(a, st);
 #define X(NMAX, R, C, W) if (a.N <= NMAX) return launch_qr_cfg<T, R, C, W>(a, st);
 	DQ_SHAPES(X)
 #undef X

@@ -423,6 +423,386 @@ __global__ void __launch_bounds__(NW * 32) k_qr(QrArgs<T> a)
 	}
 }
 
+// ----------------------------------------------- blocked QR, pre-sorted
+//
+// The QR_PRESORT factorisation of k_qr (greens.c:119-146: columns scaled by
+// the previous D, ordered by descending norm, then geqrf and the explicit
+// Q), with the matrix in shared memory and the reflectors taken NBK = 8 at
+// a time.  Warp 0 factors a panel of 8 columns with warp-level syncs only
+// and forms its block-reflector factor T (larft, forward columnwise); the
+// other warps meanwhile apply the previous panel's block reflector
+// I - V T^H V^H to the trailing columns (one-panel look-ahead), 8 columns
+// per warp as FP64 tensor-core (DMMA m8n8k4) tiles in the real case.  Q is
+// then accumulated backwards, block by block, in the same shared memory.
+// Outputs are those of k_qr in QR_PRESORT mode.
+
+// leading dimension: N rounded so that ld = 4 (mod 16) doubles, which keeps
+// the 8 x 4 DMMA fragment loads of neighbouring columns bank-conflict free
+__host__ __device__ inline int qrb_ld(int N) { return (N + 11) / 16 * 16 + 4; }
+
+template <typename T, int NBK>
+size_t qrb_smem_bytes(int N)
+{
+	const int np = (N + NBK - 1) / NBK, ld = qrb_ld(N);
+	return sizeof(T) * ((size_t)ld * N + (size_t)ld * NBK + N + (size_t)np * NBK * NBK)
+	       + sizeof(double) * 3 * (size_t)N + sizeof(int) * (size_t)N + 64;
+}
+
+// reflector k of a panel at global row r (< N): unit diagonal, zero above
+template <typename T>
+__device__ inline T qrb_v(const T *Vp, int ld, int r, int j0, int k, int nb)
+{
+	const int rr = r - j0;
+	return (k < nb && rr >= k) ? ((rr == k) ? one<T>() : Vp[r + (size_t)ld * k]) : zero<T>();
+}
+
+// col[j0..N-1] -= V W (V^H col), W = T^H (HERM) or T, one warp, one column
+template <typename T, int NBK, int RPL, bool HERM>
+__device__ inline void qrb_apply(T *col, const T *Vp, int ld, const T *Tp, int N, int j0, int nb,
+		int lane)
+{
+	T x[RPL], wv[NBK];
+#pragma unroll
+	for (int k = 0; k < NBK; k++) wv[k] = zero<T>();
+#pragma unroll
+	for (int q = 0; q < RPL; q++) {
+		const int r = j0 + lane + 32 * q;
+		x[q] = (r < N) ? col[r] : zero<T>();
+		if (r < N) {
+#pragma unroll
+			for (int k = 0; k < NBK; k++) wv[k] += conjv(qrb_v(Vp, ld, r, j0, k, nb)) * x[q];
+		}
+	}
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+		for (int k = 0; k < NBK; k++) wv[k] += shfl_xor(wv[k], o);
+	T wp[NBK];
+#pragma unroll
+	for (int k = 0; k < NBK; k++) {
+		T s = zero<T>();
+#pragma unroll
+		for (int m = 0; m < NBK; m++) {
+			if (m >= nb) continue;
+			if (HERM) {
+				if (m <= k) s += conjv(Tp[m + NBK * k]) * wv[m];
+			} else {
+				if (m >= k) s += Tp[k + NBK * m] * wv[m];
+			}
+		}
+		wp[k] = s;
+	}
+#pragma unroll
+	for (int q = 0; q < RPL; q++) {
+		const int r = j0 + lane + 32 * q;
+		if (r < N) {
+			T y = x[q];
+#pragma unroll
+			for (int k = 0; k < NBK; k++) y -= qrb_v(Vp, ld, r, j0, k, nb) * wp[k];
+			col[r] = y;
+		}
+	}
+}
+
+// The same for the 8 real columns c0 .. c0+7 (those < cend) on the FP64
+// tensor cores, one warp: W = V^T C, W' = op(T) W, C -= V W'.  Fragment
+// layouts of m8n8k4: lane l holds A[l/4][l%4], B[l%4][l/4] and
+// C[l/4][2(l%4) + {0,1}]; W moves from the C to the B layout by shuffles.
+template <int NBK, bool HERM>
+__device__ inline void qrb_apply8(double *A, int ld, int c0, int cend, const double *Vp,
+		const double *Tp, int N, int j0, int nb, int lane)
+{
+	static_assert(NBK == 8, "one m8n8k4 tile of reflectors");
+	const int lr = lane & 3, lq = lane >> 2;
+	double w0 = 0.0, w1 = 0.0;
+	const int cb = c0 + lq;
+	const bool cbok = cb < cend;
+	for (int r0 = j0; r0 < N; r0 += 4) {
+		const int r = r0 + lr;
+		const bool rok = r < N;
+		const double a = rok ? qrb_v(Vp, ld, r, j0, lq, nb) : 0.0;
+		const double b = (rok && cbok) ? A[r + (size_t)ld * cb] : 0.0;
+		dmma(w0, w1, a, b);
+	}
+	double u0 = 0.0, u1 = 0.0;
+#pragma unroll
+	for (int s = 0; s < 2; s++) {
+		const int kk = 4 * s + lr, src = 4 * kk + (lq >> 1);
+		const double v0 = __shfl_sync(0xffffffffu, w0, src), v1 = __shfl_sync(0xffffffffu, w1, src);
+		const double b = (lq & 1) ? v1 : v0;
+		double a;
+		if (HERM) a = (kk <= lq && lq < nb) ? Tp[kk + NBK * lq] : 0.0;
+		else a = (lq <= kk && kk < nb) ? Tp[lq + NBK * kk] : 0.0;
+		dmma(u0, u1, a, b);
+	}
+	double bw[2];
+#pragma unroll
+	for (int s = 0; s < 2; s++) {
+		const int kk = 4 * s + lr, src = 4 * kk + (lq >> 1);
+		const double v0 = __shfl_sync(0xffffffffu, u0, src), v1 = __shfl_sync(0xffffffffu, u1, src);
+		bw[s] = -((lq & 1) ? v1 : v0);
+	}
+	const int cc = c0 + 2 * lr;
+	const bool ok0 = cc < cend, ok1 = cc + 1 < cend;
+	for (int r0 = j0; r0 < N; r0 += 8) {
+		const int r = r0 + lq;
+		const bool rok = r < N;
+		double *p0 = A + r + (size_t)ld * cc;
+		double x0 = (rok && ok0) ? p0[0] : 0.0;
+		double x1 = (rok && ok1) ? p0[ld] : 0.0;
+#pragma unroll
+		for (int s = 0; s < 2; s++) {
+			const double a = rok ? qrb_v(Vp, ld, r, j0, 4 * s + lr, nb) : 0.0;
+			dmma(x0, x1, a, bw[s]);
+		}
+		if (rok && ok0) p0[0] = x0;
+		if (rok && ok1) p0[ld] = x1;
+	}
+}
+
+// columns [cfirst, N) in groups of 8 (real, tensor cores) or one by one
+// (complex), group g taken by warp `slot` when g % nslots == slot
+template <typename T, int NBK, int RPL, bool HERM>
+__device__ inline void qrb_apply_cols(T *A, int ld, int cfirst, const T *Vp, const T *Tp, int N,
+		int j0, int nb, int slot, int nslots, int lane)
+{
+	if constexpr (is_cplx<T>::value) {
+		for (int c = cfirst + slot; c < N; c += nslots)
+			qrb_apply<T, NBK, RPL, HERM>(A + (size_t)ld * c, Vp, ld, Tp, N, j0, nb, lane);
+	} else {
+		for (int c = cfirst + 8 * slot; c < N; c += 8 * nslots)
+			qrb_apply8<NBK, HERM>(A, ld, c, N, Vp, Tp, N, j0, nb, lane);
+	}
+}
+
+template <typename T, int NW, int NBK, int RPL>
+__global__ void __launch_bounds__(NW * 32) k_qrb(QrArgs<T> a)
+{
+	const int item = blockIdx.x;
+	if (item >= a.batch) return;
+	const int N = a.N, ld = qrb_ld(N);
+	const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+	const int np = (N + NBK - 1) / NBK;
+	extern __shared__ __align__(16) unsigned char smraw[];
+	T *A = (T *)smraw;                          // N columns, leading dimension ld, position order
+	T *Vb = A + (size_t)ld * N;                 // copy of one panel's V (ld x NBK)
+	T *tau = Vb + (size_t)ld * NBK;             // N
+	T *Ts = tau + N;                            // np blocks of NBK x NBK
+	double *dsh = (double *)(Ts + (size_t)np * NBK * NBK);
+	double *vv = dsh + N;                       // v^H v
+	double *vn = vv + N;                        // squared column norms
+	int *pvt = (int *)(vn + N);
+	if (N > 32 * RPL) {
+		if (tid == 0 && a.err) atomicOr(a.err, DQ_ERR_SIZE);
+		return;
+	}
+	const T *X = a.X + (size_t)item * a.x_stride;
+	const double *dc = a.dcol + (size_t)item * a.d_stride;
+
+	for (int c = w; c < N; c += NW) {
+		const double sc = dc[c];
+		double s = 0.0;
+		for (int r = lane; r < N; r += 32) s += abs2(X[r + (size_t)N * c] * sc);
+		s = warp_sum(s);
+		if (lane == 0) vn[c] = s;
+	}
+	__syncthreads();
+	// stable descending order of the squared norms (greens.c:123-129); a NaN
+	// norm ranks last so that the order stays a permutation
+	for (int c = tid; c < N; c += blockDim.x) {
+		double v = vn[c];
+		if (!(v >= 0.0)) {
+			v = -1.0;
+			if (a.err) atomicOr(a.err, DQ_ERR_NAN);
+		}
+		int rank = 0;
+		for (int o = 0; o < N; o++) {
+			double u = vn[o];
+			if (!(u >= 0.0)) u = -1.0;
+			rank += (u > v) || (u == v && o < c);
+		}
+		pvt[rank] = c;
+	}
+	__syncthreads();
+	for (int j = w; j < N; j += NW) {
+		const int c = pvt[j];
+		const double sc = dc[c];
+		for (int r = lane; r < N; r += 32) A[r + (size_t)ld * j] = X[r + (size_t)N * c] * sc;
+	}
+	__syncthreads();
+
+	// panel p by warps 0..NBK-1, warp c holding column j0 + c in registers
+	// (rows j0 + lane + 32 t).  Per reflector k: its owner (warp k) forms it
+	// (zlarfg convention) and publishes v; the later columns' warps update
+	// themselves, the earlier ones give y_c = v_c^H v_k for T (larft); two
+	// named barriers of the panel warps per reflector.  The next owner's
+	// norm below its diagonal is taken in the same pass as its update.
+	static_assert(NW == 2 * NBK, "NBK panel warps and NBK trailing warps");
+	__shared__ T ybuf[NBK];
+	auto bar_panel = []() { asm volatile("barrier.sync 1, %0;\n" ::"r"(NBK * 32) : "memory"); };
+	auto panel = [&](int p) {
+		const int j0 = p * NBK, nb = min(NBK, N - j0);
+		T *Tp = Ts + (size_t)p * NBK * NBK;
+		const int c = w, jc = j0 + c;
+		T *colc = A + (size_t)ld * jc;
+		T x[RPL];
+#pragma unroll
+		for (int t = 0; t < RPL; t++) {
+			const int r = j0 + lane + 32 * t;
+			x[t] = (c < nb && r < N) ? colc[r] : zero<T>();
+		}
+		double sig = 0.0;
+		if (c == 0) {
+#pragma unroll
+			for (int t = 0; t < RPL; t++)
+				if (j0 + lane + 32 * t > j0) sig += abs2(x[t]);
+			sig = warp_sum(sig);
+		}
+		for (int k = 0; k < nb; k++) {
+			const int j = j0 + k;
+			T tk = zero<T>();
+			if (c == k) {
+				const T alpha = shfl(x[0], k);
+				T scal;
+				double beta;
+				if (sig == 0.0 && im(alpha) == 0.0) {
+					tk = zero<T>();
+					beta = re(alpha);
+					scal = zero<T>();
+				} else {
+					beta = -copysign(sqrt(abs2(alpha) + sig), re(alpha));
+					tk = (from_re<T>(beta) - alpha) / beta;
+					scal = one<T>() / (alpha - beta);
+				}
+#pragma unroll
+				for (int t = 0; t < RPL; t++) {
+					const int r = j0 + lane + 32 * t;
+					if (r > j) x[t] *= scal;
+					else if (r == j) x[t] = from_re<T>(beta);
+					if (r < N) colc[r] = x[t];
+				}
+				if (lane == 0) {
+					tau[j] = tk;
+					dsh[j] = beta;
+					vv[j] = 1.0 + sig * abs2(scal);
+				}
+			}
+			bar_panel();
+			if (c != k && c < nb) {
+				const T *vk = A + (size_t)ld * j;
+				T vr[RPL];
+				T d = zero<T>();
+#pragma unroll
+				for (int t = 0; t < RPL; t++) {
+					const int r = j0 + lane + 32 * t;
+					vr[t] = (r > j && r < N) ? vk[r] : ((r == j) ? one<T>() : zero<T>());
+					d += conjv(vr[t]) * x[t];
+				}
+				d = warp_sum(d);
+				if (c > k) {
+					const T f = conjv(tau[j]) * d;
+					double s2 = 0.0;
+#pragma unroll
+					for (int t = 0; t < RPL; t++) {
+						x[t] -= vr[t] * f;
+						if (j0 + lane + 32 * t > j + 1) s2 += abs2(x[t]);
+					}
+					if (c == k + 1) sig = warp_sum(s2);
+				} else if (lane == 0) {
+					ybuf[c] = conjv(d);
+				}
+			}
+			bar_panel();
+			// T[0:k, k] = -tau_k T[0:k, 0:k] y, T[k, k] = tau_k
+			if (c == k) {
+				if (lane < k) {
+					T sm = zero<T>();
+#pragma unroll
+					for (int m = 0; m < NBK; m++)
+						if (m >= lane && m < k) sm += Tp[lane + NBK * m] * ybuf[m];
+					Tp[lane + NBK * k] = -tk * sm;
+				}
+				if (lane == k) Tp[k + NBK * k] = tk;
+			}
+		}
+		if (c < nb) {
+#pragma unroll
+			for (int t = 0; t < RPL; t++) {
+				const int r = j0 + lane + 32 * t;
+				if (r < N) colc[r] = x[t];
+			}
+		}
+	};
+
+	if (w < NBK) panel(0);
+	__syncthreads();
+	for (int p = 0; p < np; p++) {
+		const int j0 = p * NBK, nb = min(NBK, N - j0), j1 = j0 + nb;
+		const T *Vp = A + (size_t)ld * j0;
+		const T *Tp = Ts + (size_t)p * NBK * NBK;
+		if (w < NBK) {
+			if (j1 < N) {
+				// the next panel's columns first, then that panel
+				if constexpr (is_cplx<T>::value) {
+					if (j1 + w < N)
+						qrb_apply<T, NBK, RPL, true>(A + (size_t)ld * (j1 + w), Vp, ld, Tp, N, j0, nb, lane);
+				} else {
+					if (w == 0) qrb_apply8<NBK, true>(A, ld, j1, min(j1 + NBK, N), Vp, Tp, N, j0, nb, lane);
+				}
+				bar_panel();
+				panel(p + 1);
+			}
+		} else {
+			qrb_apply_cols<T, NBK, RPL, true>(A, ld, j1 + NBK, Vp, Tp, N, j0, nb, w - NBK, NW - NBK, lane);
+		}
+		__syncthreads();
+	}
+
+	// D^-1 R in position order, diag(R) (0 -> 1) and the order
+	for (int j = w; j < N; j += NW)
+		for (int r = lane; r < N; r += 32) {
+			const double dr = dsh[r] == 0.0 ? 1.0 : dsh[r];
+			a.Rs[(size_t)item * a.r_stride + r + (size_t)N * j] =
+				(r <= j) ? A[r + (size_t)ld * j] / dr : zero<T>();
+		}
+	for (int r = tid; r < N; r += blockDim.x) {
+		a.dout[(size_t)item * a.dout_stride + r] = dsh[r] == 0.0 ? 1.0 : dsh[r];
+		if (a.pvt) a.pvt[(size_t)item * a.p_stride + r] = pvt[r];
+	}
+	__syncthreads();
+
+	// Q = H_0 ... H_{N-1}, accumulated backwards by blocks in place of A:
+	// block p acts on rows and columns >= j0 of the partial product, whose
+	// panel columns are still e_c there and whose rows j0..j1-1 are zero
+	for (int p = np - 1; p >= 0; p--) {
+		const int j0 = p * NBK, nb = min(NBK, N - j0), j1 = j0 + nb, mr = N - j0;
+		for (int q = tid; q < mr * nb; q += blockDim.x) {
+			const int r = j0 + q % mr, k = q / mr;
+			Vb[r + (size_t)ld * k] = A[r + (size_t)ld * (j0 + k)];
+		}
+		__syncthreads();
+		for (int q = tid; q < mr * nb; q += blockDim.x) {
+			const int r = j0 + q % mr, k = q / mr;
+			A[r + (size_t)ld * (j0 + k)] = (r == j0 + k) ? one<T>() : zero<T>();
+		}
+		for (int q = tid; q < nb * (N - j1); q += blockDim.x) {
+			const int r = j0 + q % nb, c = j1 + q / nb;
+			A[r + (size_t)ld * c] = zero<T>();
+		}
+		__syncthreads();
+		qrb_apply_cols<T, NBK, RPL, false>(A, ld, j0, Vb, Ts + (size_t)p * NBK * NBK, N, j0, nb, w, NW,
+		                                   lane);
+		__syncthreads();
+	}
+	T *Q = a.Q + (size_t)item * a.q_stride;
+	for (int q = tid; q < N * N; q += blockDim.x) Q[q] = A[(q % N) + (size_t)ld * (q / N)];
+	if (tid == 0 && a.qdet) {
+		T ph = one<T>();
+		for (int j = 0; j < N; j++) ph = ph * phase_of(one<T>() - tau[j] * vv[j]);
+		a.qdet[item] = ph;
+	}
+}
+
 template <typename T>
 struct RecArgs {
 	int N, batch;
