@@ -177,11 +177,45 @@ static int launch_qrb_rpl(const QrArgs<T> &a, cudaStream_t st)
 	return 0;
 }
 
-// the blocked pre-sorted QR wherever its N x N matrix fits in shared memory
+template <typename T, int RPL>
+static int launch_qrp_rpl(const QrArgs<T> &a, cudaStream_t st)
+{
+	constexpr int NW = 16, NBK = 8;
+	const size_t sm = qrp_smem_bytes<T, NBK>(a.N);
+	static size_t attr = 0;
+	if (sm > attr) {
+		if (cudaFuncSetAttribute(k_qrp<T, NW, NBK, RPL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		                         (int)sm) != cudaSuccess)
+			return DQMC_E_ARG;
+		attr = sm;
+	}
+	k_qrp<T, NW, NBK, RPL><<<a.batch, NW * 32, sm, st>>>(a);
+	return 0;
+}
+
+// the shared-memory QRs wherever the N x N matrix fits (226 KB leaves room
+// for the kernels' static shared memory)
 template <typename T>
 static bool use_qrb(const QrArgs<T> &a)
 {
-	return a.mode == QR_PRESORT && qrb_smem_bytes<T, 8>(a.N) <= 227 * 1024;
+	return a.mode == QR_PRESORT && qrb_smem_bytes<T, 8>(a.N) <= 226 * 1024;
+}
+
+template <typename T>
+static bool use_qrp(const QrArgs<T> &a)
+{
+	return a.mode == QR_PIVOT && qrp_smem_bytes<T, 8>(a.N) <= 226 * 1024;
+}
+
+template <typename T>
+static int launch_qrp(const QrArgs<T> &a, cudaStream_t st)
+{
+	if (a.N <= 32) return launch_qrp_rpl<T, 1>(a, st);
+	if (a.N <= 64) return launch_qrp_rpl<T, 2>(a, st);
+	if (a.N <= 96) return launch_qrp_rpl<T, 3>(a, st);
+	if (a.N <= 128) return launch_qrp_rpl<T, 4>(a, st);
+	if (a.N <= 160) return launch_qrp_rpl<T, 5>(a, st);
+	return DQMC_E_ARG;
 }
 
 template <typename T>
@@ -200,6 +234,7 @@ int launch_qr(const QrArgs<T> &a, cudaStream_t st)
 {
 	if (a.N < 1 || a.N > max_dense_n<T>()) return DQMC_E_ARG;
 	if (use_qrb(a)) return launch_qrb(a, st);
+	if (use_qrp(a)) return launch_qrp(a, st);
 #define X(NMAX, R, C, W) if (a.N <= NMAX) return launch_qr_cfg<T, R, C, W>(a, st);
 	DQ_SHAPES(X)
 #undef X

@@ -575,6 +575,80 @@ __device__ inline void qrb_apply_cols(T *A, int ld, int cfirst, const T *Vp, con
 	}
 }
 
+// T of the block of reflectors j0 .. j0+nb-1 stored below the diagonal of
+// A (larft, forward columnwise): one warp
+template <typename T, int NBK>
+__device__ inline void qrb_block_t(const T *A, int ld, const T *tau, T *Tp, int N, int j0, int nb,
+		int lane)
+{
+	for (int k = 0; k < nb; k++) {
+		const int jk = j0 + k;
+		T y[NBK];
+#pragma unroll
+		for (int m = 0; m < NBK; m++) y[m] = zero<T>();
+		for (int r = jk + lane; r < N; r += 32) {
+			const T vk = (r == jk) ? one<T>() : A[r + (size_t)ld * jk];
+#pragma unroll
+			for (int m = 0; m < NBK; m++)
+				if (m < k) y[m] += conjv(A[r + (size_t)ld * (j0 + m)]) * vk;
+		}
+#pragma unroll
+		for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+			for (int m = 0; m < NBK; m++) y[m] += shfl_xor(y[m], o);
+		const T tk = tau[jk];
+		if (lane < k) {
+			T sm = zero<T>();
+#pragma unroll
+			for (int m = 0; m < NBK; m++)
+				if (m >= lane && m < k) sm += Tp[lane + NBK * m] * y[m];
+			Tp[lane + NBK * k] = -tk * sm;
+		}
+		if (lane == k) Tp[k + NBK * k] = tk;
+		__syncwarp();
+	}
+}
+
+// Q = H_0 ... H_{N-1} from the reflectors below the diagonal of A and the
+// block factors Ts, accumulated backwards by blocks in place of A (block p
+// acts on rows and columns >= j0 of the partial product, whose panel
+// columns are still e_c there and whose rows j0..j1-1 are zero), then Q to
+// global memory and the phase of det Q.  All warps of the CTA.
+template <typename T, int NW, int NBK, int RPL>
+__device__ inline void qrb_form_q(const QrArgs<T> &a, int item, T *A, int ld, T *Vb, const T *Ts,
+		const T *tau, const double *vv, int N)
+{
+	const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+	const int np = (N + NBK - 1) / NBK;
+	for (int p = np - 1; p >= 0; p--) {
+		const int j0 = p * NBK, nb = min(NBK, N - j0), j1 = j0 + nb, mr = N - j0;
+		for (int q = tid; q < mr * nb; q += blockDim.x) {
+			const int r = j0 + q % mr, k = q / mr;
+			Vb[r + (size_t)ld * k] = A[r + (size_t)ld * (j0 + k)];
+		}
+		__syncthreads();
+		for (int q = tid; q < mr * nb; q += blockDim.x) {
+			const int r = j0 + q % mr, k = q / mr;
+			A[r + (size_t)ld * (j0 + k)] = (r == j0 + k) ? one<T>() : zero<T>();
+		}
+		for (int q = tid; q < nb * (N - j1); q += blockDim.x) {
+			const int r = j0 + q % nb, c = j1 + q / nb;
+			A[r + (size_t)ld * c] = zero<T>();
+		}
+		__syncthreads();
+		qrb_apply_cols<T, NBK, RPL, false>(A, ld, j0, Vb, Ts + (size_t)p * NBK * NBK, N, j0, nb, w, NW,
+		                                   lane);
+		__syncthreads();
+	}
+	T *Q = a.Q + (size_t)item * a.q_stride;
+	for (int q = tid; q < N * N; q += blockDim.x) Q[q] = A[(q % N) + (size_t)ld * (q / N)];
+	if (tid == 0 && a.qdet) {
+		T ph = one<T>();
+		for (int j = 0; j < N; j++) ph = ph * phase_of(one<T>() - tau[j] * vv[j]);
+		a.qdet[item] = ph;
+	}
+}
+
 template <typename T, int NW, int NBK, int RPL>
 __global__ void __launch_bounds__(NW * 32) k_qrb(QrArgs<T> a)
 {
@@ -771,36 +845,199 @@ __global__ void __launch_bounds__(NW * 32) k_qrb(QrArgs<T> a)
 	}
 	__syncthreads();
 
-	// Q = H_0 ... H_{N-1}, accumulated backwards by blocks in place of A:
-	// block p acts on rows and columns >= j0 of the partial product, whose
-	// panel columns are still e_c there and whose rows j0..j1-1 are zero
-	for (int p = np - 1; p >= 0; p--) {
-		const int j0 = p * NBK, nb = min(NBK, N - j0), j1 = j0 + nb, mr = N - j0;
-		for (int q = tid; q < mr * nb; q += blockDim.x) {
-			const int r = j0 + q % mr, k = q / mr;
-			Vb[r + (size_t)ld * k] = A[r + (size_t)ld * (j0 + k)];
+	qrb_form_q<T, NW, NBK, RPL>(a, item, A, ld, Vb, Ts, tau, vv, N);
+}
+
+// ----------------------------------------------- column-pivoted QR
+//
+// The QR_PIVOT factorisation of k_qr (geqp3 as greens.c:97-101 calls it:
+// column pivoting by the largest partial column norm, norms downdated as
+// LAPACK dlaqp2 does and recomputed when cancellation makes the downdate
+// unreliable), with the matrix in shared memory and columns swapped in
+// place so that column j holds pivot position j.  Step j: warp 0 picks
+// the pivot (first largest norm in position order, as idamax), swaps and
+// forms the reflector; all warps then update the remaining columns and
+// their norms.  Q is formed from blocks of NBK reflectors as in k_qrb.
+// Outputs are those of k_qr in QR_PIVOT mode (T = D^-1 R P^T).
+
+template <typename T, int NBK>
+size_t qrp_smem_bytes(int N)
+{
+	return qrb_smem_bytes<T, NBK>(N) + sizeof(double) * (size_t)N + 16;
+}
+
+template <typename T, int NW, int NBK, int RPL>
+__global__ void __launch_bounds__(NW * 32) k_qrp(QrArgs<T> a)
+{
+	const int item = blockIdx.x;
+	if (item >= a.batch) return;
+	const int N = a.N, ld = qrb_ld(N);
+	const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+	const int np = (N + NBK - 1) / NBK;
+	extern __shared__ __align__(16) unsigned char smraw[];
+	T *A = (T *)smraw;
+	T *Vb = A + (size_t)ld * N;
+	T *tau = Vb + (size_t)ld * NBK;
+	T *Ts = tau + N;
+	double *dsh = (double *)(Ts + (size_t)np * NBK * NBK);
+	double *vv = dsh + N;
+	double *vn1 = vv + N;                       // partial column norms
+	int *pvt = (int *)(vn1 + N);                // original column at each position
+	const size_t o2 = ((size_t)((unsigned char *)(pvt + N) - smraw) + 15) & ~(size_t)15;
+	double *vn2 = (double *)(smraw + o2);       // norms at the last recompute
+	if (N > 32 * RPL) {
+		if (tid == 0 && a.err) atomicOr(a.err, DQ_ERR_SIZE);
+		return;
+	}
+	const T *X = a.X + (size_t)item * a.x_stride;
+	for (int c = w; c < N; c += NW) {
+		double s = 0.0;
+		for (int r = lane; r < N; r += 32) {
+			const T v = X[r + (size_t)N * c];
+			A[r + (size_t)ld * c] = v;
+			s += abs2(v);
+		}
+		s = warp_sum(s);
+		if (lane == 0) {
+			vn1[c] = sqrt(s);
+			vn2[c] = vn1[c];
+			pvt[c] = c;
+		}
+	}
+	__syncthreads();
+	const double tol3z = sqrt(2.220446049250313e-16);
+	bool nan_seen = false;
+	for (int j = 0; j < N; j++) {
+		if (w == 0) {
+			// first largest partial norm among positions j..N-1; a NaN norm
+			// ranks below every number but stays a candidate
+			double best = -1.0;
+			int bi = N;
+			for (int c = j + lane; c < N; c += 32) {
+				double v = vn1[c];
+				if (!(v >= 0.0)) {
+					v = -0.5;
+					nan_seen = true;
+				}
+				if (v > best) { best = v; bi = c; }
+			}
+#pragma unroll
+			for (int o = 16; o > 0; o >>= 1) {
+				const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+				const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+				if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+			}
+			const int pj = bi;
+			if (pj != j) {
+				for (int r = lane; r < N; r += 32) {
+					const T t0 = A[r + (size_t)ld * j];
+					A[r + (size_t)ld * j] = A[r + (size_t)ld * pj];
+					A[r + (size_t)ld * pj] = t0;
+				}
+				if (lane == 0) {
+					const double t1 = vn1[j]; vn1[j] = vn1[pj]; vn1[pj] = t1;
+					const double t2 = vn2[j]; vn2[j] = vn2[pj]; vn2[pj] = t2;
+					const int t3 = pvt[j]; pvt[j] = pvt[pj]; pvt[pj] = t3;
+				}
+			}
+			__syncwarp();
+			T *vj = A + (size_t)ld * j;
+			double sig = 0.0;
+			for (int r = j + 1 + lane; r < N; r += 32) sig += abs2(vj[r]);
+			sig = warp_sum(sig);
+			const T alpha = vj[j];
+			T tj, scal;
+			double beta;
+			if (sig == 0.0 && im(alpha) == 0.0) {
+				tj = zero<T>();
+				beta = re(alpha);
+				scal = zero<T>();
+			} else {
+				beta = -copysign(sqrt(abs2(alpha) + sig), re(alpha));
+				tj = (from_re<T>(beta) - alpha) / beta;
+				scal = one<T>() / (alpha - beta);
+			}
+			__syncwarp();
+			for (int r = j + 1 + lane; r < N; r += 32) vj[r] *= scal;
+			if (lane == 0) {
+				vj[j] = from_re<T>(beta);
+				tau[j] = tj;
+				dsh[j] = beta;
+				vv[j] = 1.0 + sig * abs2(scal);
+			}
 		}
 		__syncthreads();
-		for (int q = tid; q < mr * nb; q += blockDim.x) {
-			const int r = j0 + q % mr, k = q / mr;
-			A[r + (size_t)ld * (j0 + k)] = (r == j0 + k) ? one<T>() : zero<T>();
+		// H_j^H = I - conj(tau) v v^H on every remaining column, then the
+		// norm downdate from the updated row j
+		const T *vj = A + (size_t)ld * j;
+		T vr[RPL];
+#pragma unroll
+		for (int t = 0; t < RPL; t++) {
+			const int r = j + lane + 32 * t;
+			vr[t] = (r < N) ? ((r == j) ? one<T>() : vj[r]) : zero<T>();
 		}
-		for (int q = tid; q < nb * (N - j1); q += blockDim.x) {
-			const int r = j0 + q % nb, c = j1 + q / nb;
-			A[r + (size_t)ld * c] = zero<T>();
+		const T ct = conjv(tau[j]);
+		for (int c = j + 1 + w; c < N; c += NW) {
+			T *col = A + (size_t)ld * c;
+			T x[RPL];
+			T d = zero<T>();
+#pragma unroll
+			for (int t = 0; t < RPL; t++) {
+				const int r = j + lane + 32 * t;
+				x[t] = (r < N) ? col[r] : zero<T>();
+				d += conjv(vr[t]) * x[t];
+			}
+			d = warp_sum(d);
+			const T f = ct * d;
+#pragma unroll
+			for (int t = 0; t < RPL; t++) {
+				const int r = j + lane + 32 * t;
+				x[t] -= vr[t] * f;
+				if (r < N) col[r] = x[t];
+			}
+			const double n1 = vn1[c], n2 = vn2[c];
+			if (n1 != 0.0) {
+				const T aj = shfl(x[0], 0);
+				double tt = absv(aj) / n1;
+				tt = fmax(0.0, 1.0 - tt * tt);
+				const double t2 = tt * (n1 / n2) * (n1 / n2);
+				if (t2 <= tol3z) {
+					double s2 = 0.0;
+#pragma unroll
+					for (int t = 0; t < RPL; t++) {
+						const int r = j + lane + 32 * t;
+						if (r > j && r < N) s2 += abs2(x[t]);
+					}
+					s2 = warp_sum(s2);
+					if (lane == 0) {
+						vn1[c] = sqrt(s2);
+						vn2[c] = vn1[c];
+					}
+				} else if (lane == 0) {
+					vn1[c] = n1 * sqrt(tt);
+				}
+			}
 		}
-		__syncthreads();
-		qrb_apply_cols<T, NBK, RPL, false>(A, ld, j0, Vb, Ts + (size_t)p * NBK * NBK, N, j0, nb, w, NW,
-		                                   lane);
 		__syncthreads();
 	}
-	T *Q = a.Q + (size_t)item * a.q_stride;
-	for (int q = tid; q < N * N; q += blockDim.x) Q[q] = A[(q % N) + (size_t)ld * (q / N)];
-	if (tid == 0 && a.qdet) {
-		T ph = one<T>();
-		for (int j = 0; j < N; j++) ph = ph * phase_of(one<T>() - tau[j] * vv[j]);
-		a.qdet[item] = ph;
+	if (nan_seen && lane == 0 && a.err) atomicOr(a.err, DQ_ERR_NAN);
+	// T = D^-1 R P^T: position j is original column pvt[j]
+	for (int j = w; j < N; j += NW) {
+		const int c = pvt[j];
+		for (int r = lane; r < N; r += 32) {
+			const double dr = dsh[r] == 0.0 ? 1.0 : dsh[r];
+			a.Tout[(size_t)item * a.t_stride + r + (size_t)N * c] =
+				(r <= j) ? A[r + (size_t)ld * j] / dr : zero<T>();
+		}
 	}
+	for (int r = tid; r < N; r += blockDim.x) {
+		a.dout[(size_t)item * a.dout_stride + r] = dsh[r] == 0.0 ? 1.0 : dsh[r];
+		if (a.pvt) a.pvt[(size_t)item * a.p_stride + r] = pvt[r];
+	}
+	for (int p = w; p < np; p += NW)
+		qrb_block_t<T, NBK>(A, ld, tau, Ts + (size_t)p * NBK * NBK, N, p * NBK, min(NBK, N - p * NBK), lane);
+	__syncthreads();
+	qrb_form_q<T, NW, NBK, RPL>(a, item, A, ld, Vb, Ts, tau, vv, N);
 }
 
 template <typename T>
