@@ -39,6 +39,19 @@ WORKLOAD = ("256 chains x 12x12 square Hubbard (N=144), U=4, mu=-1, beta=6, dtau
             "(L=120), n_matmul=10, n_delay=16, eqlt every 8 slices, FP64")
 
 
+# launch classes of the engine's per-launch profile whose algorithmic FLOPs
+# are counted (8/3 N^3 per item for the QRs with explicit Q and for the
+# recombine's LU solve, 2 M N K per GEMM), with the kernel behind each
+ROOFLINE_KERNELS = {
+    "gemm": "k_gemm (batched FP64 DMMA: wraps, cluster products, half wraps, UDT products)",
+    "qr_presort": "k_qrb (pre-sorted blocked Householder QR with explicit Q, calc_eq_g)",
+    "qr_pivot": "k_qrp (column-pivoted Householder QR with explicit Q, calc_eq_g)",
+    "recombine": "k_recb (LU solve G = (D_b^-1 Q^H + D_s T)^-1 D_b^-1 Q^H)",
+}
+# DRAM bytes (read + write) per chain-spin item of one launch, from ncu
+# captures of these kernels at 64 items on the same 12x12 model
+TRAFFIC_PER_ITEM = {}
+
 T0 = time.time()
 
 
@@ -292,12 +305,14 @@ def main():
     prof = eng.profile_sweep(True, False)
     log("profile sweep done")
     peak = fp64_peak()
-    gm_ms, gm_n, gm_fl, gm_by = prof["gemm"]
-    eq_ms = prof["calc_eq_g"][0]
-    up_ms = prof["update"][0]
-    me_ms = prof["meas"][0]
-    tot_ms = gm_ms + eq_ms + up_ms + me_ms
-    achieved = gm_fl / (gm_ms / 1e3) / 1e12 if gm_ms > 0 else 0.0
+    sweep_ms = {k: v[0] for k, v in prof.items()}
+    sweep_ms["sum"] = sum(v[0] for v in prof.values())
+    # the dominant kernel among the launch classes with counted FLOPs
+    dom = max(ROOFLINE_KERNELS, key=lambda k: prof[k][0])
+    d_ms, d_n, d_fl, d_by = prof[dom]
+    achieved = d_fl / (d_ms / 1e3) / 1e12 if d_ms > 0 else 0.0
+    items = 2 * nch
+    traffic = TRAFFIC_PER_ITEM.get(dom)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -321,18 +336,19 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "chains_per_gpu": nch,
                        "l2": "inputs larger than L2 (about 2.6 MB of matrices per chain-spin)",
-                       "sweep_profile_ms": {"gemm": gm_ms, "calc_eq_g": eq_ms, "update": up_ms,
-                                            "meas": me_ms, "sum": tot_ms}},
+                       "sweep_profile_ms": sweep_ms},
             "gpu_launches": launches,
             "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
-            "roofline": {"bound": "tensor", "kernel": "k_gemm (batched FP64 DMMA: wrap, "
-                                                      "cluster products, half wrap)",
+            "roofline": {"bound": "tensor", "kernel": ROOFLINE_KERNELS[dom],
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak if peak else None, "traffic": None,
+                         "frac": achieved / peak if peak else None,
+                         "traffic": traffic * items if traffic else None,
+                         "traffic_unit": "bytes per launch (DRAM read + write)",
                          "peak_source": "cuBLAS DGEMM 8192^3 measured in this run "
                                         "(MEASURED_PEAKS.json carries no FP64 figure)",
-                         "launches": int(gm_n)},
+                         "launches_per_sweep": int(d_n),
+                         "ms_per_launch": d_ms / d_n if d_n else None},
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
         }

@@ -241,10 +241,34 @@ int launch_qr(const QrArgs<T> &a, cudaStream_t st)
 	return DQMC_E_ARG;
 }
 
+template <typename T, int RPL>
+static int launch_recb_rpl(const RecArgs<T> &a, cudaStream_t st)
+{
+	constexpr int NW = 16, CB = 3;
+	const size_t sm = recb_smem_bytes<T>(a.N);
+	static size_t attr = 0;
+	if (sm > attr) {
+		if (cudaFuncSetAttribute(k_recb<T, NW, RPL, CB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		                         (int)sm) != cudaSuccess)
+			return DQMC_E_ARG;
+		attr = sm;
+	}
+	k_recb<T, NW, RPL, CB><<<a.batch, NW * 32, sm, st>>>(a);
+	return 0;
+}
+
 template <typename T>
 int launch_rec(const RecArgs<T> &a, cudaStream_t st)
 {
 	if (a.N < 1 || a.N > max_dense_n<T>()) return DQMC_E_ARG;
+	// M in shared memory wherever it fits
+	if (recb_smem_bytes<T>(a.N) <= 226 * 1024) {
+		if (a.N <= 32) return launch_recb_rpl<T, 1>(a, st);
+		if (a.N <= 64) return launch_recb_rpl<T, 2>(a, st);
+		if (a.N <= 96) return launch_recb_rpl<T, 3>(a, st);
+		if (a.N <= 128) return launch_recb_rpl<T, 4>(a, st);
+		if (a.N <= 160) return launch_recb_rpl<T, 5>(a, st);
+	}
 #define X(NMAX, R, C, W) if (a.N <= NMAX) return launch_rec_cfg<T, R, C, W>(a, st);
 	DQ_SHAPES(X)
 #undef X
@@ -325,10 +349,46 @@ struct EqWork {
 	unsigned *err;
 };
 
+// per-launch timing of an eager sweep: begin() before a launch, end() after
+// it with the launch class and its algorithmic FLOPs and operand bytes
+struct ProfHook {
+	virtual void begin() = 0;
+	virtual void end(int cls, double flops, double bytes) = 0;
+};
+
+// launch classes of the per-launch profile (dqmc_engine_profile_sweep)
+enum : int {
+	PC_GEMM = 0, PC_UPDATE = 1, PC_QR_PIVOT = 2, PC_UNEQ = 3, PC_MEAS = 4, PC_QR_PRESORT = 5,
+	PC_RECOMBINE = 6, PC_COUNT = 7
+};
+
 template <typename T>
-static int eq_gemm(const GemmArgs<T> &g, cudaStream_t st, int *count)
+static double gemm_flops(const GemmArgs<T> &g)
 {
+	double fl = 2.0 * g.M * g.N * g.K * g.batch * (is_cplx<T>::value ? 4.0 : 1.0);
+	return (g.mode & GM_A_UPPER) ? 0.5 * fl : fl;
+}
+
+template <typename T>
+static double gemm_bytes(const GemmArgs<T> &g)
+{
+	return (double)sizeof(T) * ((double)g.M * g.K + (double)g.K * g.N + (double)g.M * g.N) * g.batch;
+}
+
+// QR with explicit Q (geqrf 4/3 N^3 + orgqr 4/3 N^3) and the recombine's
+// LU with N right-hand sides (2/3 N^3 + 2 N^3): both 8/3 N^3 per item
+template <typename T>
+static double dense_flops(int N, int batch)
+{
+	return 8.0 / 3.0 * (double)N * N * N * batch * (is_cplx<T>::value ? 4.0 : 1.0);
+}
+
+template <typename T>
+static int eq_gemm(const GemmArgs<T> &g, cudaStream_t st, int *count, ProfHook *ph = nullptr)
+{
+	if (ph) ph->begin();
 	const int rc = launch_gemm<T>(g, st);
+	if (ph) ph->end(PC_GEMM, gemm_flops(g), gemm_bytes(g));
 	if (count) (*count)++;
 	return rc;
 }
@@ -336,7 +396,8 @@ static int eq_gemm(const GemmArgs<T> &g, cudaStream_t st, int *count)
 // G = (I + C_{l0-1} ... C_{l0})^-1 over the F clusters (cyclic), grouped two
 // clusters at a time as calc_eq_g(l0, N, F, 2, C, ...) does (greens.c:69-208)
 template <typename T>
-static int run_calc_eq_g(const EqWork<T> &w, int l0, cudaStream_t st, int *count)
+static int run_calc_eq_g(const EqWork<T> &w, int l0, cudaStream_t st, int *count,
+		ProfHook *ph = nullptr)
 {
 	const int N = w.N, F = w.F, NB = w.NB;
 	const size_t NN = (size_t)N * N;
@@ -352,20 +413,23 @@ static int run_calc_eq_g(const EqWork<T> &w, int l0, cudaStream_t st, int *count
 	q.pvt = w.pvt; q.p_stride = N;
 	const int first = (F == 1) ? 1 : ((F - 1) % 2 == 1 ? 2 : 1);
 	if (first == 2) {
-		eq_gemm(gargs<T>(N, N, N, NB, clu(l0 + 1), aCl, N, clu(l0), aCl, N, w.X, aI, N), st, count);
+		eq_gemm(gargs<T>(N, N, N, NB, clu(l0 + 1), aCl, N, clu(l0), aCl, N, w.X, aI, N), st, count, ph);
 		q.X = w.X; q.x_stride = NN;
 	} else {
 		q.X = clu(l0); q.x_stride = w.cl_stride;
 	}
 	q.mode = QR_PIVOT;
 	q.Tout = w.Tm; q.t_stride = NN;
+	const double qfl = dense_flops<T>(N, NB), qby = 3.0 * sizeof(T) * NN * NB;
+	if (ph) ph->begin();
 	if (launch_qr<T>(q, st)) return DQMC_E_ARG;
+	if (ph) ph->end(PC_QR_PIVOT, qfl, qby);
 	if (count) (*count)++;
 	T *Tc = w.Tm, *Tn = w.Tm2;
 	while (m != l0) {
 		const int next = (m + 2) % F;
-		eq_gemm(gargs<T>(N, N, N, NB, clu(m + 1), aCl, N, clu(m), aCl, N, w.W, aI, N), st, count);
-		eq_gemm(gargs<T>(N, N, N, NB, w.W, aI, N, w.Qm, aI, N, w.X, aI, N), st, count);
+		eq_gemm(gargs<T>(N, N, N, NB, clu(m + 1), aCl, N, clu(m), aCl, N, w.W, aI, N), st, count, ph);
+		eq_gemm(gargs<T>(N, N, N, NB, w.W, aI, N, w.Qm, aI, N, w.X, aI, N), st, count, ph);
 		m = next;
 		QrArgs<T> r = q;
 		r.mode = QR_PRESORT;
@@ -373,13 +437,15 @@ static int run_calc_eq_g(const EqWork<T> &w, int l0, cudaStream_t st, int *count
 		r.dcol = w.dR; r.d_stride = N;
 		r.Tout = nullptr;
 		r.Rs = w.Rs; r.r_stride = NN;
+		if (ph) ph->begin();
 		if (launch_qr<T>(r, st)) return DQMC_E_ARG;
+		if (ph) ph->end(PC_QR_PRESORT, qfl, qby);
 		if (count) (*count)++;
 		GemmArgs<T> g = gargs<T>(N, N, N, NB, w.Rs, aI, N, Tc, aI, N, Tn, aI, N, one<T>(),
 		                         zero<T>(), GM_A_UPPER | GM_B_GATHER);
 		g.gidx = w.pvt;
 		g.aG = Addr{(long long)N, 0, 1};
-		eq_gemm(g, st, count);
+		eq_gemm(g, st, count, ph);
 		T *t = Tc; Tc = Tn; Tn = t;
 	}
 	RecArgs<T> ra;
@@ -392,7 +458,9 @@ static int run_calc_eq_g(const EqWork<T> &w, int l0, cudaStream_t st, int *count
 	ra.G = w.G; ra.g_stride = w.g_stride;
 	ra.phase = w.phi;
 	ra.err = w.err;
+	if (ph) ph->begin();
 	if (launch_rec<T>(ra, st)) return DQMC_E_ARG;
+	if (ph) ph->end(PC_RECOMBINE, dense_flops<T>(N, NB), qby);
 	if (count) (*count)++;
 	return 0;
 }
@@ -480,7 +548,7 @@ struct GroupBase {
 };
 
 template <typename T>
-struct Group : GroupBase {
+struct Group : GroupBase, ProfHook {
 	dqmc_params p;
 	int C;        // chains
 	int NB;       // items = 2 C
@@ -675,6 +743,8 @@ struct Group : GroupBase {
 		cudaEventRecord(e, st);
 		cur_e0 = (int)pev.size() - 1;
 	}
+	void begin() override { prof_begin(0); }
+	void end(int cls, double flops, double bytes) override { prof_end(cls, flops, bytes); }
 	void prof_end(int cls, double flops, double bytes)
 	{
 		if (!profiling) return;
@@ -710,9 +780,7 @@ struct Group : GroupBase {
 	// G = (I + C_{l0-1} ... C_{l0})^-1 (cyclic), then the chain phases
 	int calc_eq_g(int l0)
 	{
-		prof_begin(2);
-		int rc = run_calc_eq_g<T>(eq_work(), l0, st, &launch_count);
-		prof_end(2, 0.0, 0.0);
+		int rc = run_calc_eq_g<T>(eq_work(), l0, st, &launch_count, profiling ? this : nullptr);
 		watchdog("calc_eq_g");
 		if (rc) return rc;
 		k_combine_phase<T><<<(C + 127) / 128, 128, 0, st>>>(C, phi.p, phase.p);
@@ -741,7 +809,7 @@ struct Group : GroupBase {
 		const int np = (N + 31) / 32 * 32;
 		prof_begin(1);
 		k_update<T><<<C, 2 * np + 32, update_smem_bytes<T>(N, kd, ldp), st>>>(a);
-		prof_end(1, 0.0, 0.0);
+		prof_end(PC_UPDATE, 0.0, 0.0);
 		launch_count++;
 		watchdog("k_update");
 		if (L == 1) draws(0);
@@ -792,7 +860,7 @@ struct Group : GroupBase {
 		m.acc = acc_eq.p; m.acc_stride = eq_size; m.n_sample = n_eq.p;
 		prof_begin(4);
 		k_meas_eqlt<T><<<C, 256, 2 * N * sizeof(T) + 64, st>>>(m);
-		prof_end(4, 0.0, 0.0);
+		prof_end(PC_MEAS, 0.0, 0.0);
 		launch_count++;
 		watchdog("k_meas_eqlt");
 	}
@@ -812,7 +880,9 @@ struct Group : GroupBase {
 		const size_t sm = hqr_smem_bytes<T, NBK, NW>(h.M);
 		auto go = [&](auto kern) -> int {
 			CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+			prof_begin(0);
 			kern<<<h.batch, NW * 32, sm, st>>>(h);
+			prof_end(PC_UNEQ, 0.0, 0.0);
 			launch_count++;
 			return 0;
 		};
@@ -831,10 +901,11 @@ struct Group : GroupBase {
 		const int E = ue.E, NE = ue.NE;
 		const long long NE2 = (long long)NE * NE, q4 = 4LL * (long long)NN;
 		const long long qstride = (long long)std::max(E - 1, 1) * q4;
-		prof_begin(3);
+		prof_begin(0);
 		k_build_bib<T><<<grid_for((long long)L * NB * NN), 256, 0, st>>>(N, L, NB, expK.p, iexpK.p,
 		                                                               dv.p, dvi.p, ue.Bs.p, ue.iBs.p);
 		launch_count++;
+		prof_end(PC_UNEQ, 0.0, 0.0);
 		// calc_o (greens.c:247-264): I on the diagonal, -C_{2e+1} C_{2e} at
 		// (e+1, e), the remaining clusters' product at (0, E-1)
 		CK(cudaMemsetAsync(ue.O.p, 0, sizeof(T) * NB * NE2, st));
@@ -848,12 +919,16 @@ struct Group : GroupBase {
 			              Cl.p + (size_t)(F - 2) * NN, per_item((long long)F * NN), N, corner,
 			              per_item(NE2), NE));
 		else {
+			prof_begin(0);
 			k_copy2d<T><<<grid_for((long long)NB * NN), 256, 0, st>>>(N, N, NB, Cl.p + (size_t)(F - 1) * NN,
 			        (long long)F * NN, N, corner, NE2, NE, one<T>());
 			launch_count++;
+			prof_end(PC_UNEQ, 0.0, 0.0);
 		}
+		prof_begin(0);
 		k_add_diag<T><<<grid_for((long long)NE * NB), 256, 0, st>>>(NE, NB, ue.O.p, NE2);
 		launch_count++;
+		prof_end(PC_UNEQ, 0.0, 0.0);
 		// bsofi (greens.c:266-337): QR of the 2N x N panels, Q^H carried to
 		// the block columns l+1 and E-1 in the same kernel
 		for (int l = 0; l + 2 < E; l++) {
@@ -884,8 +959,10 @@ struct Group : GroupBase {
 			TriArgs<T> t{N, NE, E, NB, ue.O.p, ue.Gr.p, err.p};
 			const size_t sm = trtri_smem_bytes<T>(N);
 			CK(cudaFuncSetAttribute(k_trtri<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+			prof_begin(0);
 			k_trtri<T><<<NB * E, 256, sm, st>>>(t);
 			launch_count++;
+			prof_end(PC_UNEQ, 0.0, 0.0);
 		}
 		for (int d = 1; d < E; d++) {
 			const int na = E - d;
@@ -898,16 +975,20 @@ struct Group : GroupBase {
 		// O^-1 = R^-1 Q_{E-2}^H ... Q_0^H, each on its two block columns
 		for (int l = lf; l >= 0; l--) {
 			T *cols = ue.Gr.p + (size_t)l * N * NE;
+			prof_begin(0);
 			k_copy2d<T><<<grid_for((long long)NB * NE * wf), 256, 0, st>>>(NE, wf, NB, cols, NE2, NE,
 			        ue.Rw.p, (long long)NE * wf, NE, one<T>());
 			launch_count++;
+			prof_end(PC_UNEQ, 0.0, 0.0);
 			gemm(gargs<T>(NE, wf, wf, NB, ue.Rw.p, per_item((long long)NE * wf), NE,
 			              ue.Qh.p + (size_t)l * q4, per_item(qstride), wf, cols, per_item(NE2), NE));
 		}
 		// expand_g (greens.c:339-469)
+		prof_begin(0);
 		k_ue_seed<T><<<grid_for((long long)NB * E * NN), 256, 0, st>>>(N, E, NB, ue.plan.nme, ue.Gr.p,
 		                                                              ue.G0t.p, ue.Gtt.p, ue.Gt0.p);
 		launch_count++;
+		prof_end(PC_UNEQ, 0.0, 0.0);
 		const long long sl = (long long)NB * NN;     // one slice of a stack
 		for (const UeOp &o : ue.plan.ops) {
 			T *stk = (o.kind < 2) ? ue.G0t.p : (o.kind < 4) ? ue.Gtt.p : ue.Gt0.p;
@@ -939,14 +1020,15 @@ struct Group : GroupBase {
 			if (o.prefill) {
 				const T *src = (o.prefill == 1) ? ue.iBs.p + o.m * sl
 				             : (o.prefill == 2) ? ue.iBs.p + o.next * sl : nullptr;
+				prof_begin(0);
 				k_copy2d<T><<<grid_for((long long)NB * NN), 256, 0, st>>>(N, N, NB, src, (long long)NN, N, dst,
 				        (long long)NN, N, one<T>());
 				launch_count++;
+				prof_end(PC_UNEQ, 0.0, 0.0);
 			}
 			gemm(gargs<T>(N, N, N, NB, at(opA, 0), ai, N, at(opB, 1), ai, N, dst, ai, N,
 			              from_re<T>(o.alpha), from_re<T>(o.beta)));
 		}
-		prof_end(3, 0.0, 0.0);
 		watchdog("calc_ue_g");
 		return 0;
 	}
@@ -971,7 +1053,7 @@ struct Group : GroupBase {
 		m.bond = p.meas_bond_corr;
 		prof_begin(4);
 		k_meas_uneqlt<T><<<dim3(C, L), 256, 0, st>>>(m);
-		prof_end(4, 0.0, 0.0);
+		prof_end(PC_MEAS, 0.0, 0.0);
 		launch_count++;
 		watchdog("k_meas_uneqlt");
 		return 0;

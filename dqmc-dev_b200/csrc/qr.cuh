@@ -514,16 +514,24 @@ __device__ inline void qrb_apply8(double *A, int ld, int c0, int cend, const dou
 {
 	static_assert(NBK == 8, "one m8n8k4 tile of reflectors");
 	const int lr = lane & 3, lq = lane >> 2;
-	double w0 = 0.0, w1 = 0.0;
 	const int cb = c0 + lq;
 	const bool cbok = cb < cend;
-	for (int r0 = j0; r0 < N; r0 += 4) {
-		const int r = r0 + lr;
-		const bool rok = r < N;
-		const double a = rok ? qrb_v(Vp, ld, r, j0, lq, nb) : 0.0;
-		const double b = (rok && cbok) ? A[r + (size_t)ld * cb] : 0.0;
-		dmma(w0, w1, a, b);
+	// W: four independent accumulator pairs over row quads r0, r0+4, ...
+	double w[4][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+	for (int r0 = j0; r0 < N; r0 += 16) {
+		double av[4], bv[4];
+#pragma unroll
+		for (int u = 0; u < 4; u++) {
+			const int r = r0 + 4 * u + lr;
+			const bool rok = r < N;
+			av[u] = rok ? qrb_v(Vp, ld, r, j0, lq, nb) : 0.0;
+			bv[u] = (rok && cbok) ? A[r + (size_t)ld * cb] : 0.0;
+		}
+#pragma unroll
+		for (int u = 0; u < 4; u++) dmma(w[u][0], w[u][1], av[u], bv[u]);
 	}
+	const double w0 = (w[0][0] + w[1][0]) + (w[2][0] + w[3][0]);
+	const double w1 = (w[0][1] + w[1][1]) + (w[2][1] + w[3][1]);
 	double u0 = 0.0, u1 = 0.0;
 #pragma unroll
 	for (int s = 0; s < 2; s++) {
@@ -542,21 +550,34 @@ __device__ inline void qrb_apply8(double *A, int ld, int c0, int cend, const dou
 		const double v0 = __shfl_sync(0xffffffffu, u0, src), v1 = __shfl_sync(0xffffffffu, u1, src);
 		bw[s] = -((lq & 1) ? v1 : v0);
 	}
+	// C -= V W', three row tiles of 8 at a time
 	const int cc = c0 + 2 * lr;
 	const bool ok0 = cc < cend, ok1 = cc + 1 < cend;
-	for (int r0 = j0; r0 < N; r0 += 8) {
-		const int r = r0 + lq;
-		const bool rok = r < N;
-		double *p0 = A + r + (size_t)ld * cc;
-		double x0 = (rok && ok0) ? p0[0] : 0.0;
-		double x1 = (rok && ok1) ? p0[ld] : 0.0;
+	for (int r0 = j0; r0 < N; r0 += 24) {
+		double x0[3], x1[3], va[3][2];
 #pragma unroll
-		for (int s = 0; s < 2; s++) {
-			const double a = rok ? qrb_v(Vp, ld, r, j0, 4 * s + lr, nb) : 0.0;
-			dmma(x0, x1, a, bw[s]);
+		for (int u = 0; u < 3; u++) {
+			const int r = r0 + 8 * u + lq;
+			const bool rok = r < N;
+			const double *p0 = A + r + (size_t)ld * cc;
+			x0[u] = (rok && ok0) ? p0[0] : 0.0;
+			x1[u] = (rok && ok1) ? p0[ld] : 0.0;
+#pragma unroll
+			for (int s = 0; s < 2; s++) va[u][s] = rok ? qrb_v(Vp, ld, r, j0, 4 * s + lr, nb) : 0.0;
 		}
-		if (rok && ok0) p0[0] = x0;
-		if (rok && ok1) p0[ld] = x1;
+#pragma unroll
+		for (int s = 0; s < 2; s++)
+#pragma unroll
+			for (int u = 0; u < 3; u++) dmma(x0[u], x1[u], va[u][s], bw[s]);
+#pragma unroll
+		for (int u = 0; u < 3; u++) {
+			const int r = r0 + 8 * u + lq;
+			if (r < N) {
+				double *p0 = A + r + (size_t)ld * cc;
+				if (ok0) p0[0] = x0[u];
+				if (ok1) p0[ld] = x1[u];
+			}
+		}
 	}
 }
 
@@ -622,19 +643,15 @@ __device__ inline void qrb_form_q(const QrArgs<T> &a, int item, T *A, int ld, T 
 	const int np = (N + NBK - 1) / NBK;
 	for (int p = np - 1; p >= 0; p--) {
 		const int j0 = p * NBK, nb = min(NBK, N - j0), j1 = j0 + nb, mr = N - j0;
-		for (int q = tid; q < mr * nb; q += blockDim.x) {
-			const int r = j0 + q % mr, k = q / mr;
-			Vb[r + (size_t)ld * k] = A[r + (size_t)ld * (j0 + k)];
-		}
+		(void)mr;
+		if (w < nb)
+			for (int r = j0 + lane; r < N; r += 32) Vb[r + (size_t)ld * w] = A[r + (size_t)ld * (j0 + w)];
 		__syncthreads();
-		for (int q = tid; q < mr * nb; q += blockDim.x) {
-			const int r = j0 + q % mr, k = q / mr;
-			A[r + (size_t)ld * (j0 + k)] = (r == j0 + k) ? one<T>() : zero<T>();
-		}
-		for (int q = tid; q < nb * (N - j1); q += blockDim.x) {
-			const int r = j0 + q % nb, c = j1 + q / nb;
-			A[r + (size_t)ld * c] = zero<T>();
-		}
+		if (w < nb)
+			for (int r = j0 + lane; r < N; r += 32)
+				A[r + (size_t)ld * (j0 + w)] = (r == j0 + w) ? one<T>() : zero<T>();
+		for (int c = j1 + tid / nb; c < N; c += blockDim.x / nb)
+			A[j0 + tid % nb + (size_t)ld * c] = zero<T>();
 		__syncthreads();
 		qrb_apply_cols<T, NBK, RPL, false>(A, ld, j0, Vb, Ts + (size_t)p * NBK * NBK, N, j0, nb, w, NW,
 		                                   lane);
@@ -1309,6 +1326,211 @@ __global__ void __launch_bounds__(NW * 32) k_recombine(RecArgs<T> a)
 			parity ^= (len - 1) & 1;
 		}
 		if (parity) ph = ph * -1.0;
+		a.phase[item] = ph * vs;
+	}
+}
+
+// ----------------------------------------------- recombine in shared memory
+//
+// k_recombine's G = (D_b^-1 Q^H + D_s T)^-1 D_b^-1 Q^H (greens.c:157-178)
+// with M in shared memory: LU with partial pivoting and physical row swaps
+// (getrf: the first largest |M[r, j]| of the column, as idamax); warp 0
+// picks, swaps and scales, all warps update the trailing columns.  Then
+// each warp solves for its right-hand sides, CB at a time held in
+// registers (permutation, unit-lower forward, upper backward), and the
+// phase 1/phase(det G) = phase(det Q) phase(det M) sign(prod v).
+
+template <typename T>
+size_t recb_smem_bytes(int N)
+{
+	return sizeof(T) * (size_t)qrb_ld(N) * N + sizeof(double) * 2 * (size_t)N + sizeof(int) * 2 * (size_t)N
+	       + 64;
+}
+
+template <typename T, int NW, int RPL, int CB>
+__global__ void __launch_bounds__(NW * 32) k_recb(RecArgs<T> a)
+{
+	const int item = blockIdx.x;
+	if (item >= a.batch) return;
+	const int N = a.N, ld = qrb_ld(N);
+	const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+	extern __shared__ __align__(16) unsigned char smraw[];
+	T *M = (T *)smraw;                          // N columns, leading dimension ld
+	double *vsh = (double *)(M + (size_t)ld * N);   // D_b^-1
+	double *dss = vsh + N;                      // D_s
+	int *ipiv = (int *)(dss + N);               // row swapped with row j at step j
+	int *perm = ipiv + N;                       // row r of P Y is row perm[r] of Y
+	if (N > 32 * RPL) {
+		if (tid == 0 && a.err) atomicOr(a.err, DQ_ERR_SIZE);
+		return;
+	}
+	const T *Q = a.Q + (size_t)item * a.q_stride;
+	const T *Tm = a.Tm + (size_t)item * a.t_stride;
+	const double *d = a.d + (size_t)item * a.d_stride;
+	for (int r = tid; r < N; r += blockDim.x) {
+		const double dr = d[r];
+		if (fabs(dr) > 1.0) { vsh[r] = 1.0 / dr; dss[r] = 1.0; }
+		else { vsh[r] = 1.0; dss[r] = dr; }
+	}
+	__syncthreads();
+	for (int c = w; c < N; c += NW)
+		for (int r = lane; r < N; r += 32)
+			M[r + (size_t)ld * c] = conjv(Q[c + (size_t)N * r]) * vsh[r] + Tm[r + (size_t)N * c] * dss[r];
+	__syncthreads();
+
+	bool nan_seen = false, sing = false;
+	for (int j = 0; j < N; j++) {
+		if (w == 0) {
+			double best = -1.0;
+			int br = N;
+			for (int r = j + lane; r < N; r += 32) {
+				double m = absv(M[r + (size_t)ld * j]);
+				if (!(m >= 0.0)) {
+					m = -0.5;
+					nan_seen = true;
+				}
+				if (m > best) { best = m; br = r; }
+			}
+#pragma unroll
+			for (int o = 16; o > 0; o >>= 1) {
+				const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+				const int orr = __shfl_xor_sync(0xffffffffu, br, o);
+				if (ob > best || (ob == best && orr < br)) { best = ob; br = orr; }
+			}
+			if (br != j)
+				for (int c = lane; c < N; c += 32) {
+					const T t0 = M[j + (size_t)ld * c];
+					M[j + (size_t)ld * c] = M[br + (size_t)ld * c];
+					M[br + (size_t)ld * c] = t0;
+				}
+			if (lane == 0) ipiv[j] = br;
+			__syncwarp();
+			T piv = M[j + (size_t)ld * j];
+			if (re(piv) == 0.0 && im(piv) == 0.0) {
+				sing = true;
+				piv = one<T>();
+			}
+			const T ip = one<T>() / piv;
+			for (int r = j + 1 + lane; r < N; r += 32) M[r + (size_t)ld * j] *= ip;
+		}
+		__syncthreads();
+		T l[RPL];
+#pragma unroll
+		for (int t = 0; t < RPL; t++) {
+			const int r = j + 1 + lane + 32 * t;
+			l[t] = (r < N) ? M[r + (size_t)ld * j] : zero<T>();
+		}
+		for (int c = j + 1 + w; c < N; c += NW) {
+			T *col = M + (size_t)ld * c;
+			const T u = col[j];
+#pragma unroll
+			for (int t = 0; t < RPL; t++) {
+				const int r = j + 1 + lane + 32 * t;
+				if (r < N) col[r] -= l[t] * u;
+			}
+		}
+		__syncthreads();
+	}
+	if (tid == 0) {
+		for (int r = 0; r < N; r++) perm[r] = r;
+		for (int j = 0; j < N; j++) {
+			const int q = ipiv[j];
+			const int t0 = perm[j];
+			perm[j] = perm[q];
+			perm[q] = t0;
+		}
+	}
+	if (w == 0 && lane == 0) {
+		if (nan_seen && a.err) atomicOr(a.err, DQ_ERR_NAN);
+		if (sing && a.err) atomicOr(a.err, DQ_ERR_SINGULAR);
+	}
+	__syncthreads();
+
+	// right-hand sides Y = D_b^-1 Q^H, CB columns per pass of a warp
+	T *G = a.G + (size_t)item * a.g_stride;
+	for (int c0 = w * CB; c0 < N; c0 += NW * CB) {
+		T y[CB][RPL];
+#pragma unroll
+		for (int b = 0; b < CB; b++) {
+			const int c = c0 + b;
+#pragma unroll
+			for (int t = 0; t < RPL; t++) {
+				const int r = lane + 32 * t;
+				const int pr = (r < N) ? perm[r] : 0;
+				y[b][t] = (c < N && r < N) ? conjv(Q[c + (size_t)N * pr]) * vsh[pr] : zero<T>();
+			}
+		}
+		// L (unit lower)
+		for (int k = 0; k < N - 1; k++) {
+			const int tk = k >> 5, lk = k & 31;
+			T yk[CB];
+#pragma unroll
+			for (int b = 0; b < CB; b++) {
+				T v = zero<T>();
+#pragma unroll
+				for (int t = 0; t < RPL; t++)
+					if (t == tk) v = y[b][t];
+				yk[b] = shfl(v, lk);
+			}
+#pragma unroll
+			for (int t = 0; t < RPL; t++) {
+				const int r = lane + 32 * t;
+				if (r > k && r < N) {
+					const T lv = M[r + (size_t)ld * k];
+#pragma unroll
+					for (int b = 0; b < CB; b++) y[b][t] -= lv * yk[b];
+				}
+			}
+		}
+		// U
+		for (int k = N - 1; k >= 0; k--) {
+			const int tk = k >> 5, lk = k & 31;
+			T ukk = M[k + (size_t)ld * k];
+			if (re(ukk) == 0.0 && im(ukk) == 0.0) ukk = one<T>();
+			const T iu = one<T>() / ukk;
+			T yk[CB];
+#pragma unroll
+			for (int b = 0; b < CB; b++) {
+				T v = zero<T>();
+#pragma unroll
+				for (int t = 0; t < RPL; t++)
+					if (t == tk) v = y[b][t];
+				yk[b] = shfl(v, lk) * iu;
+			}
+#pragma unroll
+			for (int t = 0; t < RPL; t++) {
+				const int r = lane + 32 * t;
+				if (r < k) {
+					const T uv = M[r + (size_t)ld * k];
+#pragma unroll
+					for (int b = 0; b < CB; b++) y[b][t] -= uv * yk[b];
+				} else if (r == k) {
+#pragma unroll
+					for (int b = 0; b < CB; b++) y[b][t] = yk[b];
+				}
+			}
+		}
+#pragma unroll
+		for (int b = 0; b < CB; b++) {
+			const int c = c0 + b;
+			if (c >= N) continue;
+#pragma unroll
+			for (int t = 0; t < RPL; t++) {
+				const int r = lane + 32 * t;
+				if (r < N) G[r + (size_t)N * c] = y[b][t];
+			}
+		}
+	}
+	if (tid == 0) {
+		T ph = a.qdet ? a.qdet[item] : one<T>();
+		double vs = 1.0;
+		int nswap = 0;
+		for (int j = 0; j < N; j++) {
+			ph = ph * phase_of(M[j + (size_t)ld * j]);
+			vs *= (vsh[j] < 0.0) ? -1.0 : 1.0;
+			nswap += (ipiv[j] != j);
+		}
+		if (nswap & 1) ph = ph * -1.0;
 		a.phase[item] = ph * vs;
 	}
 }

@@ -163,13 +163,16 @@ class Engine:
     def launches_per_sweep(self, meas_eq: bool, meas_ue: bool) -> int:
         return int(self.lib.dqmc_engine_launches_per_sweep(self.h, int(meas_eq), int(meas_ue)))
 
-    def profile_sweep(self, meas_eq: bool, meas_ue: bool = False, n_class: int = 5):
+    PROFILE_CLASSES = ["gemm", "update", "qr_pivot", "uneqlt_g", "meas", "qr_presort",
+                       "recombine"]
+
+    def profile_sweep(self, meas_eq: bool, meas_ue: bool = False, n_class: int = 7):
         """One eagerly launched sweep with per-launch CUDA events; returns
         {class: (ms, launches, flops, bytes)}."""
         out = (C.c_double * (4 * n_class))()
         _lib.check(self.lib.dqmc_engine_profile_sweep(self.h, int(meas_eq), int(meas_ue), out,
                                                       n_class), "dqmc_engine_profile_sweep")
-        names = ["gemm", "update", "calc_eq_g", "uneqlt_g", "meas"]
+        names = self.PROFILE_CLASSES
         return {names[c]: tuple(out[4 * c:4 * c + 4]) for c in range(n_class)}
 
     def stream(self) -> int:

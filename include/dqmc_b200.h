@@ -113,8 +113,9 @@ int dqmc_engine_launches_per_sweep(dqmc_engine *e, int meas_eq, int meas_ue);
 /* Runs one sweep eagerly with CUDA events around every launch (it advances
  * the chains like dqmc_engine_sweeps(e, 1, 1)).  out[4*c + k], c < n_class:
  * k = 0 total ms, 1 launches, 2 algorithmic FLOPs, 3 operand bytes, for the
- * launch classes c = 0 batched GEMM, 1 delayed update, 2 calc_eq_g (its
- * GEMMs included), 3 unequal-time G, 4 measurements. */
+ * launch classes c = 0 batched GEMM (calc_eq_g's included), 1 delayed
+ * update, 2 column-pivoted QR, 3 unequal-time G (its GEMMs under 0),
+ * 4 measurements, 5 pre-sorted QR, 6 recombine (LU solve of G). */
 int dqmc_engine_profile_sweep(dqmc_engine *e, int meas_eq, int meas_ue, double *out,
 		int n_class);
 
