@@ -129,7 +129,9 @@ __global__ void k_update(UpdArgs<T> a)
 {
 	constexpr bool CX = is_cplx<T>::value;
 	constexpr int PL = CX ? 2 : 1;
-	constexpr int FT = 4;          // G tiles in flight per warp during a flush
+	constexpr int FT = 4;          // G tiles in flight per warp (flushes of more than 4 FKS columns)
+	constexpr int FKS = 4;         // k steps of 4 held in registers by the flush
+	constexpr int FRT = 4;         // row tiles per DMMA group in the flush
 	const int c = blockIdx.x;
 	if (c >= a.nchain) return;
 	const int N = a.N, KD = a.n_delay, LDP = a.ldp;
@@ -187,61 +189,130 @@ __global__ void k_update(UpdArgs<T> a)
 	} else {
 		int k = 0;
 		auto flush = [&](int kc) {
-			// G_s += A_s B_s^T for both spins; 8x8 output tiles, FT per warp at once
+			// G_s += A_s B_s^T for both spins.  Each warp takes an 8-column
+			// tile of one spin, holds its B fragments (k < 4 FKS) in registers
+			// and sweeps the row tiles FRT at a time, independent DMMA chains
+			// per row tile; the k order per tile is ascending as before.
 			const int nt = (N + 7) / 8;
-			const int ntt = nt * nt;
 			const int lane = tid & 31, warp = tid >> 5, nwarp = NM >> 5;
 			const int gq = lane >> 2, tq = lane & 3;
-			for (int t0 = warp * FT; t0 < 2 * ntt; t0 += nwarp * FT) {
-				T gv[FT][2];
-				int r_[FT], c_[FT], sp_[FT];
-#pragma unroll
-				for (int f = 0; f < FT; f++) {
-					const int tile = t0 + f;
-					const int sp = tile / ntt, tt = tile - sp * ntt;
-					const int r0 = (tt % nt) * 8, c0 = (tt / nt) * 8;
-					sp_[f] = sp;
-					r_[f] = r0;
-					c_[f] = c0;
-					const T *Gt = a.G + (size_t)(2 * c + (sp & 1)) * NN;
-#pragma unroll
-					for (int h = 0; h < 2; h++) {
-						const int rr = r0 + gq, cc = c0 + 2 * tq + h;
-						gv[f][h] = (tile < 2 * ntt && rr < N && cc < N) ? Gt[rr + (size_t)N * cc] : zero<T>();
-					}
-				}
-#pragma unroll
-				for (int f = 0; f < FT; f++) {
-					const int tile = t0 + f;
-					if (tile >= 2 * ntt) break;
-					const int sp = sp_[f], r0 = r_[f], c0 = c_[f];
+			if (kc <= 4 * FKS) {
+				for (int task = warp; task < 2 * nt; task += nwarp) {
+					const int sp = task >= nt ? 1 : 0;
+					const int c0 = (task - sp * nt) * 8;
+					T *Gt = a.G + (size_t)(2 * c + sp) * NN;
 					const double *Ar = P(sp, 0, 0), *Br = P(sp, 1, 0);
 					const double *Ai = P(sp, 0, PL - 1), *Bi = P(sp, 1, PL - 1);
-					double cr[2] = {0.0, 0.0}, ci[2] = {0.0, 0.0};
-					const int ra = r0 + gq, cb = c0 + gq;
-					for (int k0 = 0; k0 < kc; k0 += 4) {
-						const int kk = k0 + tq;
-						const bool okk = kk < kc;
-						const double ar = (okk && ra < N) ? Ar[ra + LDP * kk] : 0.0;
-						const double br = (okk && cb < N) ? Br[cb + LDP * kk] : 0.0;
-						dmma(cr[0], cr[1], ar, br);
-						if (CX) {
-							const double ai = (okk && ra < N) ? Ai[ra + LDP * kk] : 0.0;
-							const double bi = (okk && cb < N) ? Bi[cb + LDP * kk] : 0.0;
-							dmma(cr[0], cr[1], -ai, bi);
-							dmma(ci[0], ci[1], ar, bi);
-							dmma(ci[0], ci[1], ai, br);
+					const int cb = c0 + gq, cc0 = c0 + 2 * tq;
+					double bre[FKS], bim[FKS];
+#pragma unroll
+					for (int q = 0; q < FKS; q++) {
+						const int kk = 4 * q + tq;
+						const bool ok = kk < kc && cb < N;
+						bre[q] = ok ? Br[cb + LDP * kk] : 0.0;
+						bim[q] = (CX && ok) ? Bi[cb + LDP * kk] : 0.0;
+					}
+					for (int r0 = 0; r0 < N; r0 += 8 * FRT) {
+						T gv[FRT][2];
+						double cr[FRT][2], ci[FRT][2];
+#pragma unroll
+						for (int u = 0; u < FRT; u++) {
+							const int rr = r0 + 8 * u + gq;
+#pragma unroll
+							for (int h = 0; h < 2; h++) {
+								gv[u][h] = (rr < N && cc0 + h < N) ? Gt[rr + (size_t)N * (cc0 + h)] : zero<T>();
+								cr[u][h] = 0.0;
+								ci[u][h] = 0.0;
+							}
+						}
+#pragma unroll
+						for (int q = 0; q < FKS; q++) {
+							if (4 * q < kc) {
+								const int kk = 4 * q + tq;
+#pragma unroll
+								for (int u = 0; u < FRT; u++) {
+									const int ra = r0 + 8 * u + gq;
+									const bool ok = kk < kc && ra < N;
+									const double ar = ok ? Ar[ra + LDP * kk] : 0.0;
+									dmma(cr[u][0], cr[u][1], ar, bre[q]);
+									if (CX) {
+										const double ai = ok ? Ai[ra + LDP * kk] : 0.0;
+										dmma(cr[u][0], cr[u][1], -ai, bim[q]);
+										dmma(ci[u][0], ci[u][1], ar, bim[q]);
+										dmma(ci[u][0], ci[u][1], ai, bre[q]);
+									}
+								}
+							}
+						}
+#pragma unroll
+						for (int u = 0; u < FRT; u++) {
+							const int rr = r0 + 8 * u + gq;
+#pragma unroll
+							for (int h = 0; h < 2; h++) {
+								if (rr < N && cc0 + h < N) {
+									if constexpr (CX) {
+										Gt[rr + (size_t)N * (cc0 + h)] = gv[u][h] + mkz(cr[u][h], ci[u][h]);
+									} else {
+										Gt[rr + (size_t)N * (cc0 + h)] = gv[u][h] + cr[u][h];
+									}
+								}
+							}
 						}
 					}
-					T *Gt = a.G + (size_t)(2 * c + sp) * NN;
-#pragma unroll
-					for (int h = 0; h < 2; h++) {
-						const int rr = r0 + gq, cc = c0 + 2 * tq + h;
-						if (rr < N && cc < N) {
-							if constexpr (CX) {
-								Gt[rr + (size_t)N * cc] = gv[f][h] + mkz(cr[h], ci[h]);
-							} else {
-								Gt[rr + (size_t)N * cc] = gv[f][h] + cr[h];
+				}
+			} else {
+				const int ntt = nt * nt;
+				for (int t0 = warp * FT; t0 < 2 * ntt; t0 += nwarp * FT) {
+					T gv[FT][2];
+					int r_[FT], c_[FT], sp_[FT];
+	#pragma unroll
+					for (int f = 0; f < FT; f++) {
+						const int tile = t0 + f;
+						const int sp = tile / ntt, tt = tile - sp * ntt;
+						const int r0 = (tt % nt) * 8, c0 = (tt / nt) * 8;
+						sp_[f] = sp;
+						r_[f] = r0;
+						c_[f] = c0;
+						const T *Gt = a.G + (size_t)(2 * c + (sp & 1)) * NN;
+	#pragma unroll
+						for (int h = 0; h < 2; h++) {
+							const int rr = r0 + gq, cc = c0 + 2 * tq + h;
+							gv[f][h] = (tile < 2 * ntt && rr < N && cc < N) ? Gt[rr + (size_t)N * cc] : zero<T>();
+						}
+					}
+	#pragma unroll
+					for (int f = 0; f < FT; f++) {
+						const int tile = t0 + f;
+						if (tile >= 2 * ntt) break;
+						const int sp = sp_[f], r0 = r_[f], c0 = c_[f];
+						const double *Ar = P(sp, 0, 0), *Br = P(sp, 1, 0);
+						const double *Ai = P(sp, 0, PL - 1), *Bi = P(sp, 1, PL - 1);
+						double cr[2] = {0.0, 0.0}, ci[2] = {0.0, 0.0};
+						const int ra = r0 + gq, cb = c0 + gq;
+						for (int k0 = 0; k0 < kc; k0 += 4) {
+							const int kk = k0 + tq;
+							const bool okk = kk < kc;
+							const double ar = (okk && ra < N) ? Ar[ra + LDP * kk] : 0.0;
+							const double br = (okk && cb < N) ? Br[cb + LDP * kk] : 0.0;
+							dmma(cr[0], cr[1], ar, br);
+							if (CX) {
+								const double ai = (okk && ra < N) ? Ai[ra + LDP * kk] : 0.0;
+								const double bi = (okk && cb < N) ? Bi[cb + LDP * kk] : 0.0;
+								dmma(cr[0], cr[1], -ai, bi);
+								dmma(ci[0], ci[1], ar, bi);
+								dmma(ci[0], ci[1], ai, br);
+							}
+						}
+						T *Gt = a.G + (size_t)(2 * c + sp) * NN;
+	#pragma unroll
+						for (int h = 0; h < 2; h++) {
+							const int rr = r0 + gq, cc = c0 + 2 * tq + h;
+							if (rr < N && cc < N) {
+								if constexpr (CX) {
+									Gt[rr + (size_t)N * cc] = gv[f][h] + mkz(cr[h], ci[h]);
+								} else {
+									Gt[rr + (size_t)N * cc] = gv[f][h] + cr[h];
+								}
 							}
 						}
 					}
