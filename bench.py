@@ -34,6 +34,7 @@ sys.path.insert(0, os.path.join(ROOT, "dqmc-dev_b200"))
 CFG = dict(Nx=12, Ny=12, U=4.0, mu=-1.0, tp=0.0, dt=0.05, L=120, n_matmul=10, n_delay=16,
            period_eqlt=8)
 CHAINS = 256
+SEED = 1000
 METRIC = "chain-sweeps/s"
 WORKLOAD = ("256 chains x 12x12 square Hubbard (N=144), U=4, mu=-1, beta=6, dtau=0.05 "
             "(L=120), n_matmul=10, n_delay=16, eqlt every 8 slices, FP64")
@@ -60,9 +61,11 @@ def log(msg):
     print(f"[bench {time.time() - T0:7.1f}s] {msg}", file=sys.stderr, flush=True)
 
 
-def sim_dicts(n, seed, n_sweep):
-    from dqmc_b200 import gen
-    rngs = gen.chain_rngs(seed, n)
+def sim_dicts(chains, seed, n_sweep):
+    """Sim data of the given global chains of the job: chain c starts from
+    the master stream of `seed` jumped c times (dqmc_b200.replicas)."""
+    from dqmc_b200 import gen, replicas
+    rngs = replicas.chain_streams(seed, chains)
     d0 = gen.make_sim(init_rng=rngs[0], n_sweep_warm=0, n_sweep_meas=n_sweep, **CFG)
     out = [d0]
     N, L = CFG["Nx"] * CFG["Ny"], CFG["L"]
@@ -87,13 +90,8 @@ def dist_setup(gpus):
 
 
 def max_over_ranks(x, world):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from dqmc_b200 import replicas
+    return replicas.max_over_ranks(x, world, device="cuda")
 
 
 def barrier(world):
@@ -247,7 +245,9 @@ def main():
 
     nch = args.chains
     total = args.warmup + args.steps + 4
-    dicts = sim_dicts(nch, seed=1000 + rank, n_sweep=total)
+    # this rank's block of the job's nch * world chains (weak scaling)
+    from dqmc_b200 import replicas
+    dicts = sim_dicts(replicas.shard(nch * world, rank, world), seed=SEED, n_sweep=total)
     log(f"generated {nch} chains")
     sims = [engine.SimData(d) for d in dicts]
     eng = engine.Engine(sims, device=local)
