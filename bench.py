@@ -51,7 +51,8 @@ ROOFLINE_KERNELS = {
 }
 # DRAM bytes (read + write) per chain-spin item of one launch, from ncu
 # captures of these kernels at 64 items on the same 12x12 model
-TRAFFIC_PER_ITEM = {}
+TRAFFIC_PER_ITEM = {"gemm": 172848, "qr_presort": 168068, "qr_pivot": 166916,
+                    "recombine": 333636}
 
 T0 = time.time()
 
