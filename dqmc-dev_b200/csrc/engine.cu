@@ -109,123 +109,47 @@ static GemmArgs<T> gargs(int M, int N, int K, int batch, const T *A, Addr aA, in
 	return g;
 }
 
-// register shapes for the per-matrix factorisations
-template <typename T, int RPL, int CPW, int NW, int MODE>
-static int launch_qr_mode(const QrArgs<T> &a, cudaStream_t st)
+// largest N the per-matrix factorisations (QR, recombine) support: the
+// shared-memory form while N x N fits there, the global-memory form (working
+// matrix in the caller's per-item workspace, L2-resident) up to 256
+template <typename T> constexpr int max_dense_n() { return 256; }
+
+// rows per lane of a warp column: 32 * RPL >= N
+#define DQ_RPL(X) X(32, 1) X(64, 2) X(96, 3) X(128, 4) X(160, 5) X(192, 6) X(224, 7) X(256, 8)
+
+// 226 KB leaves room for the kernels' static shared memory
+static const size_t SMEM_FIT = 226 * 1024;
+
+template <typename K, typename Args>
+static int launch_dense(K kern, const Args &a, size_t sm, size_t &attr, cudaStream_t st)
 {
-	const size_t sm = qr_smem_bytes<T>(a.N, NW);
-	static size_t attr = 0;
 	if (sm > attr) {
-		if (cudaFuncSetAttribute(k_qr<T, RPL, CPW, NW, MODE>,
-		                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
+		if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
 			return DQMC_E_ARG;
 		attr = sm;
 	}
-	k_qr<T, RPL, CPW, NW, MODE><<<a.batch, NW * 32, sm, st>>>(a);
+	kern<<<a.batch, 512, sm, st>>>(a);
 	return 0;
 }
 
-template <typename T, int RPL, int CPW, int NW>
-static int launch_qr_cfg(const QrArgs<T> &a, cudaStream_t st)
-{
-	return a.mode == QR_PIVOT ? launch_qr_mode<T, RPL, CPW, NW, QR_PIVOT>(a, st)
-	                          : launch_qr_mode<T, RPL, CPW, NW, QR_PRESORT>(a, st);
-}
-
-template <typename T, int RPL, int CPW, int NW>
-static int launch_rec_cfg(const RecArgs<T> &a, cudaStream_t st)
-{
-	const size_t sm = rec_smem_bytes<T>(a.N);
-	static size_t attr = 0;
-	if (sm > attr) {
-		if (cudaFuncSetAttribute(k_recombine<T, RPL, CPW, NW>,
-		                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
-			return DQMC_E_ARG;
-		attr = sm;
-	}
-	k_recombine<T, RPL, CPW, NW><<<a.batch, NW * 32, sm, st>>>(a);
-	return 0;
-}
-
-// largest N the register-resident factorisations support
-template <typename T> constexpr int max_dense_n() { return is_cplx<T>::value ? 112 : 160; }
-
-// (max N, rows per lane, columns per warp, warps); complex stops at 112 so
-// that an N x N complex matrix still fits in shared memory
-#define DQ_SHAPES(X)                    \
-	X(32, 1, 8, 4)                      \
-	X(64, 2, 8, 8)                      \
-	X(96, 3, 8, 12)                     \
-	X(112, 4, 7, 16)                    \
-	X(128, 4, 8, 16)                    \
-	X(144, 5, 9, 16)                    \
-	X(160, 5, 10, 16)
-
-template <typename T, int RPL>
-static int launch_qrb_rpl(const QrArgs<T> &a, cudaStream_t st)
+template <typename T, int RPL, bool GM>
+static int launch_qr_rpl(const QrArgs<T> &a, cudaStream_t st)
 {
 	constexpr int NW = 16, NBK = 8;
-	const size_t sm = qrb_smem_bytes<T, NBK>(a.N);
-	static size_t attr = 0;
-	if (sm > attr) {
-		if (cudaFuncSetAttribute(k_qrb<T, NW, NBK, RPL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-		                         (int)sm) != cudaSuccess)
-			return DQMC_E_ARG;
-		attr = sm;
+	if (a.mode == QR_PRESORT) {
+		static size_t attr = 0;
+		return launch_dense(k_qrb<T, NW, NBK, RPL, GM>, a, qrb_smem_bytes<T, NBK>(a.N, GM), attr, st);
 	}
-	k_qrb<T, NW, NBK, RPL><<<a.batch, NW * 32, sm, st>>>(a);
-	return 0;
-}
-
-template <typename T, int RPL>
-static int launch_qrp_rpl(const QrArgs<T> &a, cudaStream_t st)
-{
-	constexpr int NW = 16, NBK = 8;
-	const size_t sm = qrp_smem_bytes<T, NBK>(a.N);
 	static size_t attr = 0;
-	if (sm > attr) {
-		if (cudaFuncSetAttribute(k_qrp<T, NW, NBK, RPL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-		                         (int)sm) != cudaSuccess)
-			return DQMC_E_ARG;
-		attr = sm;
-	}
-	k_qrp<T, NW, NBK, RPL><<<a.batch, NW * 32, sm, st>>>(a);
-	return 0;
+	return launch_dense(k_qrp<T, NW, NBK, RPL, GM>, a, qrp_smem_bytes<T, NBK>(a.N, GM), attr, st);
 }
 
-// the shared-memory QRs wherever the N x N matrix fits (226 KB leaves room
-// for the kernels' static shared memory)
-template <typename T>
-static bool use_qrb(const QrArgs<T> &a)
+template <typename T, bool GM>
+static int launch_qr_gm(const QrArgs<T> &a, cudaStream_t st)
 {
-	return a.mode == QR_PRESORT && qrb_smem_bytes<T, 8>(a.N) <= 226 * 1024;
-}
-
-template <typename T>
-static bool use_qrp(const QrArgs<T> &a)
-{
-	return a.mode == QR_PIVOT && qrp_smem_bytes<T, 8>(a.N) <= 226 * 1024;
-}
-
-template <typename T>
-static int launch_qrp(const QrArgs<T> &a, cudaStream_t st)
-{
-	if (a.N <= 32) return launch_qrp_rpl<T, 1>(a, st);
-	if (a.N <= 64) return launch_qrp_rpl<T, 2>(a, st);
-	if (a.N <= 96) return launch_qrp_rpl<T, 3>(a, st);
-	if (a.N <= 128) return launch_qrp_rpl<T, 4>(a, st);
-	if (a.N <= 160) return launch_qrp_rpl<T, 5>(a, st);
-	return DQMC_E_ARG;
-}
-
-template <typename T>
-static int launch_qrb(const QrArgs<T> &a, cudaStream_t st)
-{
-	if (a.N <= 32) return launch_qrb_rpl<T, 1>(a, st);
-	if (a.N <= 64) return launch_qrb_rpl<T, 2>(a, st);
-	if (a.N <= 96) return launch_qrb_rpl<T, 3>(a, st);
-	if (a.N <= 128) return launch_qrb_rpl<T, 4>(a, st);
-	if (a.N <= 160) return launch_qrb_rpl<T, 5>(a, st);
+#define X(NMAX, R) if (a.N <= NMAX) return launch_qr_rpl<T, R, GM>(a, st);
+	DQ_RPL(X)
+#undef X
 	return DQMC_E_ARG;
 }
 
@@ -233,46 +157,35 @@ template <typename T>
 int launch_qr(const QrArgs<T> &a, cudaStream_t st)
 {
 	if (a.N < 1 || a.N > max_dense_n<T>()) return DQMC_E_ARG;
-	if (use_qrb(a)) return launch_qrb(a, st);
-	if (use_qrp(a)) return launch_qrp(a, st);
-#define X(NMAX, R, C, W) if (a.N <= NMAX) return launch_qr_cfg<T, R, C, W>(a, st);
-	DQ_SHAPES(X)
-#undef X
-	return DQMC_E_ARG;
+	const size_t sm = a.mode == QR_PRESORT ? qrb_smem_bytes<T, 8>(a.N) : qrp_smem_bytes<T, 8>(a.N);
+	if (sm <= SMEM_FIT) return launch_qr_gm<T, false>(a, st);
+	if (!a.work) return DQMC_E_ARG;
+	return launch_qr_gm<T, true>(a, st);
 }
 
-template <typename T, int RPL>
-static int launch_recb_rpl(const RecArgs<T> &a, cudaStream_t st)
+template <typename T, int RPL, bool GM>
+static int launch_rec_rpl(const RecArgs<T> &a, cudaStream_t st)
 {
-	constexpr int NW = 16, CB = 3;
-	const size_t sm = recb_smem_bytes<T>(a.N);
 	static size_t attr = 0;
-	if (sm > attr) {
-		if (cudaFuncSetAttribute(k_recb<T, NW, RPL, CB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-		                         (int)sm) != cudaSuccess)
-			return DQMC_E_ARG;
-		attr = sm;
-	}
-	k_recb<T, NW, RPL, CB><<<a.batch, NW * 32, sm, st>>>(a);
-	return 0;
+	return launch_dense(k_recb<T, 16, RPL, 3, GM>, a, recb_smem_bytes<T>(a.N, GM), attr, st);
+}
+
+template <typename T, bool GM>
+static int launch_rec_gm(const RecArgs<T> &a, cudaStream_t st)
+{
+#define X(NMAX, R) if (a.N <= NMAX) return launch_rec_rpl<T, R, GM>(a, st);
+	DQ_RPL(X)
+#undef X
+	return DQMC_E_ARG;
 }
 
 template <typename T>
 int launch_rec(const RecArgs<T> &a, cudaStream_t st)
 {
 	if (a.N < 1 || a.N > max_dense_n<T>()) return DQMC_E_ARG;
-	// M in shared memory wherever it fits
-	if (recb_smem_bytes<T>(a.N) <= 226 * 1024) {
-		if (a.N <= 32) return launch_recb_rpl<T, 1>(a, st);
-		if (a.N <= 64) return launch_recb_rpl<T, 2>(a, st);
-		if (a.N <= 96) return launch_recb_rpl<T, 3>(a, st);
-		if (a.N <= 128) return launch_recb_rpl<T, 4>(a, st);
-		if (a.N <= 160) return launch_recb_rpl<T, 5>(a, st);
-	}
-#define X(NMAX, R, C, W) if (a.N <= NMAX) return launch_rec_cfg<T, R, C, W>(a, st);
-	DQ_SHAPES(X)
-#undef X
-	return DQMC_E_ARG;
+	if (recb_smem_bytes<T>(a.N) <= SMEM_FIT) return launch_rec_gm<T, false>(a, st);
+	if (!a.work) return DQMC_E_ARG;
+	return launch_rec_gm<T, true>(a, st);
 }
 
 // ------------------------------------------------------- small helper kernels
@@ -411,6 +324,7 @@ static int run_calc_eq_g(const EqWork<T> &w, int l0, cudaStream_t st, int *count
 	q.dout = w.dR; q.dout_stride = N;
 	q.qdet = w.qdet;
 	q.pvt = w.pvt; q.p_stride = N;
+	q.work = w.W; q.w_stride = NN;     // free while a QR runs
 	const int first = (F == 1) ? 1 : ((F - 1) % 2 == 1 ? 2 : 1);
 	if (first == 2) {
 		eq_gemm(gargs<T>(N, N, N, NB, clu(l0 + 1), aCl, N, clu(l0), aCl, N, w.X, aI, N), st, count, ph);
@@ -457,6 +371,7 @@ static int run_calc_eq_g(const EqWork<T> &w, int l0, cudaStream_t st, int *count
 	ra.qdet = w.qdet;
 	ra.G = w.G; ra.g_stride = w.g_stride;
 	ra.phase = w.phi;
+	ra.work = w.W; ra.w_stride = NN;
 	ra.err = w.err;
 	if (ph) ph->begin();
 	if (launch_rec<T>(ra, st)) return DQMC_E_ARG;

@@ -1,29 +1,19 @@
 // The dense factorisations of the stabilised equal-time Green's function
-// (reference src/greens.c:69-208, calc_eq_g), one CTA per (chain, spin)
-// matrix with the working matrix held in registers:
+// (reference src/greens.c:69-208, calc_eq_g), one CTA of 16 warps per
+// (chain, spin) matrix, the N x N working matrix in shared memory (or, where
+// it does not fit, in a per-item global workspace):
 //
-//   warp w owns columns c = w + NW*q (q < CPW), lane l owns rows l + 32*p
-//   (p < RPL); Householder vectors and scalars live in shared memory.
-//
-// Every elimination step updates all CPW columns of a warp at once: the CPW
-// dot products are accumulated independently and reduced together with
-// interleaved butterfly shuffles, and columns that take no part are masked
-// arithmetically, so the work of a step is straight-line code with CPW-fold
-// instruction-level parallelism.
-//
-// k_qr      Householder QR that picks, at each step, which remaining column
-//           to eliminate next, so no columns are moved:
-//             QR_PIVOT   largest remaining partial column norm, with the norm
-//                        downdating and recomputation rule of LAPACK geqp3
-//                        (greens.c:89);
-//             QR_PRESORT columns in order of decreasing norm, computed once
-//                        after scaling by d (the norm pre-pivoting of
-//                        greens.c:112-135), then unpivoted.
-//           Q is formed explicitly (so that later g*Q is a plain GEMM and
-//           diag(v) Q^H is elementwise), with the phase of det Q.
-// k_recombine  G = (D_b^-1 Q^H + D_s T)^-1 D_b^-1 Q^H (greens.c:157-178) by
-//           LU with partial (implicit) row pivoting and a two-sided solve,
-//           plus the phase of det G (greens.c:194-207).
+// k_qrp   Householder QR with column pivoting by the largest remaining
+//         partial column norm, downdated and recomputed as LAPACK geqp3 does
+//         (greens.c:89, QR_PIVOT);
+// k_qrb   Householder QR of the columns in order of decreasing norm, computed
+//         once after scaling by d (the norm pre-pivoting of greens.c:112-135,
+//         QR_PRESORT), blocked by 8 with DMMA block-reflector updates;
+//         both form Q explicitly (so that a later g*Q is a plain GEMM and
+//         diag(v) Q^H is elementwise), with the phase of det Q;
+// k_recb  G = (D_b^-1 Q^H + D_s T)^-1 D_b^-1 Q^H (greens.c:157-178) by LU
+//         with partial row pivoting and two triangular solves, plus the
+//         phase of det G (greens.c:194-207).
 #pragma once
 
 #include "common.cuh"
@@ -43,408 +33,36 @@ struct QrArgs {
 	int *pvt; long long p_stride;         // pivot order (column chosen at step j)
 	double *dout; long long dout_stride;  // diag(R), 0 -> 1 (real: Householder beta)
 	T *qdet;                              // phase of det Q per item
+	T *work; long long w_stride;          // N x N per item: working matrix of the
+	                                      // shared-memory kernels' global-memory form
 	unsigned *err;
 };
 
-template <typename T>
-size_t qr_smem_bytes(int N, int nw)
-{
-	return sizeof(T) * ((size_t)N * N + N) + sizeof(double) * (4 * (size_t)N + 2 * nw)
-	       + sizeof(int) * (3 * (size_t)N + 2 * nw) + 64;
-}
-
-// value of row r (uniform across the warp) from the lane that holds it
-template <typename T, int RPL>
-__device__ inline T row_of(const T (&col)[RPL], int r, int lane)
-{
-	T v = zero<T>();
-#pragma unroll
-	for (int p = 0; p < RPL; p++)
-		if (lane + 32 * p == r) v = col[p];
-	return shfl(v, r & 31);
-}
-
-// CPW independent warp sums, their butterfly stages interleaved
-template <typename T, int CPW>
-__device__ inline void warp_sums(T (&s)[CPW])
-{
-#pragma unroll
-	for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-		for (int q = 0; q < CPW; q++) s[q] += shfl_xor(s[q], o);
-}
-
-template <typename T, int RPL, int CPW, int NW, int MODE>
-__global__ void __launch_bounds__(NW * 32) k_qr(QrArgs<T> a)
-{
-	const int item = blockIdx.x;
-	if (item >= a.batch) return;
-	const int N = a.N;
-	const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-	extern __shared__ __align__(16) unsigned char smraw[];
-	T *V = (T *)smraw;                          // N*N reflectors, column j = v_j
-	T *tau = V + (size_t)N * N;                 // N
-	double *vn1 = (double *)(tau + N);          // N column norms (partial norms when pivoting)
-	double *vn2 = vn1 + N;                      // N norms at the last recompute
-	double *dsh = vn2 + N;                      // N diag(R)
-	double *vv = dsh + N;                       // N  v^H v
-	double *cval = vv + N;                      // NW candidate norms
-	int *pvt = (int *)(cval + NW);              // N  column chosen at step j
-	int *ccol = pvt + N;                        // NW candidate columns
-	__shared__ int s_col;
-
-	const T *X = a.X + (size_t)item * a.x_stride;
-	T x[CPW][RPL];
-	int posr[CPW];    // step at which each own column is eliminated (N: not yet)
-#pragma unroll
-	for (int q = 0; q < CPW; q++) {
-		const int c = w + NW * q;
-		const double sc = (MODE == QR_PRESORT && c < N) ? a.dcol[(size_t)item * a.d_stride + c] : 1.0;
-#pragma unroll
-		for (int p = 0; p < RPL; p++) {
-			const int r = lane + 32 * p;
-			x[q][p] = (c < N && r < N) ? X[r + (size_t)N * c] * sc : zero<T>();
-		}
-		posr[q] = N;
-	}
-	// column norms (squared)
-	{
-		double s[CPW];
-#pragma unroll
-		for (int q = 0; q < CPW; q++) {
-			s[q] = 0.0;
-#pragma unroll
-			for (int p = 0; p < RPL; p++) s[q] += abs2(x[q][p]);
-		}
-		warp_sums(s);
-#pragma unroll
-		for (int q = 0; q < CPW; q++) {
-			const int c = w + NW * q;
-			const double v = (MODE == QR_PIVOT) ? sqrt(s[q]) : s[q];
-			if (lane == 0 && c < N) {
-				vn1[c] = v;
-				vn2[c] = v;
-			}
-		}
-	}
-	__syncthreads();
-	if (MODE == QR_PRESORT) {
-		// stable descending order of the squared norms (greens.c:123-129)
-		// (a NaN norm ranks last, so the order stays a permutation)
-		for (int c = tid; c < N; c += blockDim.x) {
-			double v = vn1[c];
-			if (!(v >= 0.0)) {
-				v = -1.0;
-				if (a.err) atomicOr(a.err, DQ_ERR_NAN);
-			}
-			int rank = 0;
-			for (int o = 0; o < N; o++) {
-				double u = vn1[o];
-				if (!(u >= 0.0)) u = -1.0;
-				rank += (u > v) || (u == v && o < c);
-			}
-			pvt[rank] = c;
-		}
-		__syncthreads();
-		// reload in pivot-position order: slot q of warp w holds position
-		// q*NW + w, so eliminated columns are whole slots that later steps skip
-#pragma unroll
-		for (int q = 0; q < CPW; q++) {
-			const int jq = q * NW + w;
-			const int c = jq < N ? pvt[jq] : 0;
-			const double sc = jq < N ? a.dcol[(size_t)item * a.d_stride + c] : 0.0;
-#pragma unroll
-			for (int p = 0; p < RPL; p++) {
-				const int r = lane + 32 * p;
-				x[q][p] = (jq < N && r < N) ? X[r + (size_t)N * c] * sc : zero<T>();
-			}
-			posr[q] = jq < N ? jq : N;
-		}
-	}
-
-	const double tol3z = sqrt(2.220446049250313e-16);
-	for (int j = 0; j < N; j++) {
-		int cj;
-		if (MODE == QR_PIVOT) {
-			// warp candidate: largest partial norm among remaining own columns
-			double best = -1.0;
-			int bc = N;
-#pragma unroll
-			for (int q = 0; q < CPW; q++) {
-				const int c = w + NW * q;
-				if (c < N && posr[q] == N) {
-					double v = vn1[c];
-					if (!(v >= 0.0)) v = -0.5;   // NaN: last choice, still a candidate
-					if (v > best || (v == best && c < bc)) {
-						best = v;
-						bc = c;
-					}
-				}
-			}
-			if (lane == 0) { cval[w] = best; ccol[w] = bc; }
-			__syncthreads();
-			if (tid == 0) {
-				double bb = -1.0;
-				int bcol = N;
-				for (int q = 0; q < NW; q++)
-					if (cval[q] > bb || (cval[q] == bb && ccol[q] < bcol)) { bb = cval[q]; bcol = ccol[q]; }
-				if (bcol >= N) {
-					// no finite candidate (NaN norms): take the first unused column
-					if (a.err) atomicOr(a.err, DQ_ERR_NAN);
-					for (int q = 0; q < N; q++) {
-						bool taken = false;
-						for (int jj = 0; jj < j; jj++) taken |= (pvt[jj] == q);
-						if (!taken) { bcol = q; break; }
-					}
-				}
-				s_col = bcol;
-				pvt[j] = bcol;
-			}
-			__syncthreads();
-			cj = s_col;
-			if (cj % NW == w) {
-#pragma unroll
-				for (int q = 0; q < CPW; q++)
-					if (q == cj / NW) posr[q] = j;
-			}
-		} else {
-			cj = j;     // position order: step j eliminates slot j / NW of warp j % NW
-		}
-		const int ow = cj % NW, oq = cj / NW;
-		if (w == ow) {
-			T col[RPL];
-#pragma unroll
-			for (int p = 0; p < RPL; p++) {
-				T v = x[0][p];
-#pragma unroll
-				for (int q = 1; q < CPW; q++)
-					if (q == oq) v = x[q][p];
-				col[p] = v;
-			}
-			// alpha = row j, sigma = sum over rows > j
-			double sig = 0.0;
-#pragma unroll
-			for (int p = 0; p < RPL; p++) {
-				const int r = lane + 32 * p;
-				if (r > j && r < N) sig += abs2(col[p]);
-			}
-			sig = warp_sum(sig);
-			const T alpha = row_of(col, j, lane);
-			const double anorm2 = abs2(alpha);
-			T tj, scal;
-			double beta;
-			if (sig == 0.0 && im(alpha) == 0.0) {
-				tj = zero<T>();
-				beta = re(alpha);
-				scal = zero<T>();
-			} else {
-				beta = -copysign(sqrt(anorm2 + sig), re(alpha));
-				tj = (from_re<T>(beta) - alpha) / beta;
-				scal = one<T>() / (alpha - beta);
-			}
-#pragma unroll
-			for (int p = 0; p < RPL; p++) {
-				const int r = lane + 32 * p;
-				if (r < N) {
-					T v;
-					if (r < j) v = zero<T>();
-					else if (r == j) v = one<T>();
-					else v = col[p] * scal;
-					V[r + (size_t)N * j] = v;
-					if (r == j) col[p] = from_re<T>(beta);
-					else if (r > j) col[p] = zero<T>();
-				}
-			}
-			if (lane == 0) {
-				tau[j] = tj;
-				dsh[j] = beta;
-				vv[j] = 1.0 + sig * abs2(scal);
-			}
-#pragma unroll
-			for (int q = 0; q < CPW; q++)
-				if (q == oq)
-#pragma unroll
-					for (int p = 0; p < RPL; p++) x[q][p] = col[p];
-		}
-		__syncthreads();
-		// apply H_j^H = I - conj(tau) v v^H to every remaining own column;
-		// v is zero above row j, so row blocks p < j/32 take no part, and in
-		// position order (PRESORT) whole slots are already eliminated
-		const T ct = conjv(tau[j]);
-		const int pa = j >> 5;
-		T vr[RPL];
-#pragma unroll
-		for (int p = 0; p < RPL; p++) {
-			const int r = lane + 32 * p;
-			vr[p] = (p >= pa && r < N) ? V[r + (size_t)N * j] : zero<T>();
-		}
-		T s[CPW];
-#pragma unroll
-		for (int q = 0; q < CPW; q++) {
-			s[q] = zero<T>();
-#pragma unroll
-			for (int p = 0; p < RPL; p++) s[q] = fma_(conjv(vr[p]), x[q][p], s[q]);
-		}
-		warp_sums(s);
-#pragma unroll
-		for (int q = 0; q < CPW; q++) {
-			const bool act = (MODE == QR_PRESORT) ? (q * NW + w > j) : (posr[q] > j);
-			const T f = act ? ct * s[q] : zero<T>();
-#pragma unroll
-			for (int p = 0; p < RPL; p++) x[q][p] = x[q][p] - vr[p] * f;
-		}
-		if (MODE == QR_PIVOT) {
-			// partial norm downdate over rows > j (LAPACK dlaqp2); the norms of
-			// a warp's columns are private to it (lane 0 writes them)
-			T xj[CPW];
-#pragma unroll
-			for (int q = 0; q < CPW; q++) {
-				T v = zero<T>();
-#pragma unroll
-				for (int p = 0; p < RPL; p++)
-					if (lane + 32 * p == j) v = x[q][p];
-				xj[q] = v;
-			}
-#pragma unroll
-			for (int q = 0; q < CPW; q++) xj[q] = shfl(xj[q], j & 31);
-			bool need = false;
-			double nv[CPW];
-			bool rec[CPW];
-#pragma unroll
-			for (int q = 0; q < CPW; q++) {
-				const int c = w + NW * q;
-				const double n1 = (c < N) ? vn1[c] : 0.0, n2 = (c < N) ? vn2[c] : 1.0;
-				const bool act = posr[q] == N && c < N && n1 != 0.0;
-				double t = act ? absv(xj[q]) / n1 : 0.0;
-				t = fmax(0.0, 1.0 - t * t);
-				const double t2 = act ? t * (n1 / n2) * (n1 / n2) : 1.0;
-				rec[q] = act && t2 <= tol3z;
-				need |= rec[q];
-				nv[q] = act ? n1 * sqrt(t) : n1;
-			}
-			if (need) {
-				double s2[CPW];
-#pragma unroll
-				for (int q = 0; q < CPW; q++) {
-					s2[q] = 0.0;
-#pragma unroll
-					for (int p = 0; p < RPL; p++)
-						if (lane + 32 * p > j && lane + 32 * p < N) s2[q] += abs2(x[q][p]);
-				}
-				warp_sums(s2);
-#pragma unroll
-				for (int q = 0; q < CPW; q++)
-					if (rec[q]) nv[q] = sqrt(s2[q]);
-			}
-			__syncwarp();
-			if (lane == 0) {
-#pragma unroll
-				for (int q = 0; q < CPW; q++) {
-					const int c = w + NW * q;
-					if (c < N && posr[q] == N) {
-						vn1[c] = nv[q];
-						if (rec[q]) vn2[c] = nv[q];
-					}
-				}
-			}
-			__syncwarp();
-		}
-	}
-	__syncthreads();
-
-	// R outputs: PIVOT slots hold original columns c (R[:, posr]); PRESORT
-	// slots hold positions
-#pragma unroll
-	for (int q = 0; q < CPW; q++) {
-		const int c = w + NW * q;
-		if (c >= N) continue;
-		const int jc = (MODE == QR_PRESORT) ? c : posr[q];
-#pragma unroll
-		for (int p = 0; p < RPL; p++) {
-			const int r = lane + 32 * p;
-			if (r >= N) continue;
-			const double dr = dsh[r] == 0.0 ? 1.0 : dsh[r];
-			const T v = (r <= jc) ? x[q][p] / dr : zero<T>();
-			if (MODE == QR_PIVOT) a.Tout[(size_t)item * a.t_stride + r + (size_t)N * c] = v;
-			else a.Rs[(size_t)item * a.r_stride + r + (size_t)N * jc] = v;
-		}
-	}
-	for (int r = tid; r < N; r += blockDim.x) {
-		a.dout[(size_t)item * a.dout_stride + r] = dsh[r] == 0.0 ? 1.0 : dsh[r];
-		if (a.pvt) a.pvt[(size_t)item * a.p_stride + r] = pvt[r];
-	}
-
-	// explicit Q = H_0 H_1 ... H_{N-1}: columns by position, reflectors backwards
-#pragma unroll
-	for (int q = 0; q < CPW; q++) {
-		const int c = w + NW * q;
-#pragma unroll
-		for (int p = 0; p < RPL; p++) x[q][p] = (lane + 32 * p == c) ? one<T>() : zero<T>();
-	}
-	for (int j = N - 1; j >= 0; j--) {
-		const T tj = tau[j];
-		const int pa = j >> 5;
-		T vr[RPL];
-#pragma unroll
-		for (int p = 0; p < RPL; p++) {
-			const int r = lane + 32 * p;
-			vr[p] = (p >= pa && r < N) ? V[r + (size_t)N * j] : zero<T>();
-		}
-		T s[CPW];
-#pragma unroll
-		for (int q = 0; q < CPW; q++) {
-			s[q] = zero<T>();
-#pragma unroll
-			for (int p = 0; p < RPL; p++) s[q] = fma_(conjv(vr[p]), x[q][p], s[q]);
-		}
-		warp_sums(s);
-#pragma unroll
-		for (int q = 0; q < CPW; q++) {
-			const T f = (w + NW * q >= j) ? tj * s[q] : zero<T>();
-#pragma unroll
-			for (int p = 0; p < RPL; p++) x[q][p] = x[q][p] - vr[p] * f;
-		}
-	}
-	T *Q = a.Q + (size_t)item * a.q_stride;
-#pragma unroll
-	for (int q = 0; q < CPW; q++) {
-		const int c = w + NW * q;
-		if (c >= N) continue;
-#pragma unroll
-		for (int p = 0; p < RPL; p++) {
-			const int r = lane + 32 * p;
-			if (r < N) Q[r + (size_t)N * c] = x[q][p];
-		}
-	}
-	if (tid == 0 && a.qdet) {
-		T ph = one<T>();
-		for (int j = 0; j < N; j++) ph = ph * phase_of(one<T>() - tau[j] * vv[j]);
-		a.qdet[item] = ph;
-	}
-}
-
 // ----------------------------------------------- blocked QR, pre-sorted
 //
-// The QR_PRESORT factorisation of k_qr (greens.c:119-146: columns scaled by
+// The QR_PRESORT factorisation (greens.c:119-146: columns scaled by
 // the previous D, ordered by descending norm, then geqrf and the explicit
 // Q), with the matrix in shared memory and the reflectors taken NBK = 8 at
-// a time.  Warp 0 factors a panel of 8 columns with warp-level syncs only
-// and forms its block-reflector factor T (larft, forward columnwise); the
-// other warps meanwhile apply the previous panel's block reflector
-// I - V T^H V^H to the trailing columns (one-panel look-ahead), 8 columns
-// per warp as FP64 tensor-core (DMMA m8n8k4) tiles in the real case.  Q is
-// then accumulated backwards, block by block, in the same shared memory.
-// Outputs are those of k_qr in QR_PRESORT mode.
+// a time.  Warps 0-7 factor a panel of 8 columns (one column each, named
+// barriers) and form its block-reflector factor T (larft, forward
+// columnwise); warps 8-15 meanwhile apply the previous panel's block
+// reflector I - V T^H V^H to the trailing columns (one-panel look-ahead), 8
+// columns per warp as FP64 tensor-core (DMMA m8n8k4) tiles in the real case.
+// Q is then accumulated backwards, block by block, in the same memory.
+// Outputs: Q, D^-1 R in position order (Rs), diag(R) and the order.
 
 // leading dimension: N rounded so that ld = 4 (mod 16) doubles, which keeps
 // the 8 x 4 DMMA fragment loads of neighbouring columns bank-conflict free
 __host__ __device__ inline int qrb_ld(int N) { return (N + 11) / 16 * 16 + 4; }
 
+// In the global-memory form (GM) the N x N working matrix lives in the
+// caller's per-item workspace with leading dimension N, and shared memory
+// keeps only the small arrays; otherwise it is the first part of shared memory.
 template <typename T, int NBK>
-size_t qrb_smem_bytes(int N)
+size_t qrb_smem_bytes(int N, bool gm = false)
 {
-	const int np = (N + NBK - 1) / NBK, ld = qrb_ld(N);
-	return sizeof(T) * ((size_t)ld * N + (size_t)ld * NBK + N + (size_t)np * NBK * NBK)
+	const int np = (N + NBK - 1) / NBK, ld = gm ? N : qrb_ld(N);
+	return sizeof(T) * ((gm ? 0 : (size_t)ld * N) + (size_t)ld * NBK + N + (size_t)np * NBK * NBK)
 	       + sizeof(double) * 3 * (size_t)N + sizeof(int) * (size_t)N + 64;
 }
 
@@ -666,17 +284,18 @@ __device__ inline void qrb_form_q(const QrArgs<T> &a, int item, T *A, int ld, T 
 	}
 }
 
-template <typename T, int NW, int NBK, int RPL>
+template <typename T, int NW, int NBK, int RPL, bool GM>
 __global__ void __launch_bounds__(NW * 32) k_qrb(QrArgs<T> a)
 {
 	const int item = blockIdx.x;
 	if (item >= a.batch) return;
-	const int N = a.N, ld = qrb_ld(N);
+	const int N = a.N, ld = GM ? N : qrb_ld(N);
 	const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
 	const int np = (N + NBK - 1) / NBK;
 	extern __shared__ __align__(16) unsigned char smraw[];
-	T *A = (T *)smraw;                          // N columns, leading dimension ld, position order
-	T *Vb = A + (size_t)ld * N;                 // copy of one panel's V (ld x NBK)
+	// N columns, leading dimension ld, position order
+	T *A = GM ? a.work + (size_t)item * a.w_stride : (T *)smraw;
+	T *Vb = GM ? (T *)smraw : A + (size_t)ld * N;   // copy of one panel's V (ld x NBK)
 	T *tau = Vb + (size_t)ld * NBK;             // N
 	T *Ts = tau + N;                            // np blocks of NBK x NBK
 	double *dsh = (double *)(Ts + (size_t)np * NBK * NBK);
@@ -867,7 +486,7 @@ __global__ void __launch_bounds__(NW * 32) k_qrb(QrArgs<T> a)
 
 // ----------------------------------------------- column-pivoted QR
 //
-// The QR_PIVOT factorisation of k_qr (geqp3 as greens.c:97-101 calls it:
+// The QR_PIVOT factorisation (geqp3 as greens.c:97-101 calls it:
 // column pivoting by the largest partial column norm, norms downdated as
 // LAPACK dlaqp2 does and recomputed when cancellation makes the downdate
 // unreliable), with the matrix in shared memory and columns swapped in
@@ -875,25 +494,25 @@ __global__ void __launch_bounds__(NW * 32) k_qrb(QrArgs<T> a)
 // the pivot (first largest norm in position order, as idamax), swaps and
 // forms the reflector; all warps then update the remaining columns and
 // their norms.  Q is formed from blocks of NBK reflectors as in k_qrb.
-// Outputs are those of k_qr in QR_PIVOT mode (T = D^-1 R P^T).
+// Outputs: Q, T = D^-1 R P^T, diag(R) and the pivot order.
 
 template <typename T, int NBK>
-size_t qrp_smem_bytes(int N)
+size_t qrp_smem_bytes(int N, bool gm = false)
 {
-	return qrb_smem_bytes<T, NBK>(N) + sizeof(double) * (size_t)N + 16;
+	return qrb_smem_bytes<T, NBK>(N, gm) + sizeof(double) * (size_t)N + 16;
 }
 
-template <typename T, int NW, int NBK, int RPL>
+template <typename T, int NW, int NBK, int RPL, bool GM>
 __global__ void __launch_bounds__(NW * 32) k_qrp(QrArgs<T> a)
 {
 	const int item = blockIdx.x;
 	if (item >= a.batch) return;
-	const int N = a.N, ld = qrb_ld(N);
+	const int N = a.N, ld = GM ? N : qrb_ld(N);
 	const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
 	const int np = (N + NBK - 1) / NBK;
 	extern __shared__ __align__(16) unsigned char smraw[];
-	T *A = (T *)smraw;
-	T *Vb = A + (size_t)ld * N;
+	T *A = GM ? a.work + (size_t)item * a.w_stride : (T *)smraw;
+	T *Vb = GM ? (T *)smraw : A + (size_t)ld * N;
 	T *tau = Vb + (size_t)ld * NBK;
 	T *Ts = tau + N;
 	double *dsh = (double *)(Ts + (size_t)np * NBK * NBK);
@@ -1066,273 +685,13 @@ struct RecArgs {
 	const T *qdet;
 	T *G; long long g_stride;
 	T *phase;                 // per item: 1 / phase(det G)
+	T *work; long long w_stride;   // N x N per item, global-memory form only
 	unsigned *err;
 };
 
-template <typename T>
-size_t rec_smem_bytes(int N)
-{
-	return sizeof(T) * ((size_t)N * N + N) + sizeof(int) * 3 * (size_t)N + sizeof(double) * 2 * N + 64;
-}
-
-template <typename T, int RPL, int CPW, int NW>
-__global__ void __launch_bounds__(NW * 32) k_recombine(RecArgs<T> a)
-{
-	const int item = blockIdx.x;
-	if (item >= a.batch) return;
-	const int N = a.N;
-	const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-	extern __shared__ __align__(16) unsigned char smraw[];
-	T *LU = (T *)smraw;                 // N*N
-	T *lcol = LU + (size_t)N * N;       // N current multipliers
-	double *vsh = (double *)(lcol + N); // N  v = D_b^-1
-	double *dss = vsh + N;              // N  D_s
-	int *prow = (int *)(dss + N);       // N pivot row of step j
-	int *stepof = prow + N;             // N step at which row r became pivot
-	int *rused = stepof + N;            // N
-	__shared__ int s_prow;
-
-	const T *Q = a.Q + (size_t)item * a.q_stride;
-	const T *Tm = a.Tm + (size_t)item * a.t_stride;
-	const double *d = a.d + (size_t)item * a.d_stride;
-	for (int r = tid; r < N; r += blockDim.x) {
-		const double dr = d[r];
-		if (fabs(dr) > 1.0) { vsh[r] = 1.0 / dr; dss[r] = 1.0; }
-		else { vsh[r] = 1.0; dss[r] = dr; }
-		rused[r] = 0;
-		stepof[r] = N;
-	}
-	__syncthreads();
-	// M = diag(v) Q^H + diag(ds) T
-	T x[CPW][RPL];
-#pragma unroll
-	for (int q = 0; q < CPW; q++) {
-		const int c = w + NW * q;
-#pragma unroll
-		for (int p = 0; p < RPL; p++) {
-			const int r = lane + 32 * p;
-			x[q][p] = (c < N && r < N) ? conjv(Q[c + (size_t)N * r]) * vsh[r] + Tm[r + (size_t)N * c] * dss[r]
-			                           : zero<T>();
-		}
-	}
-	// rows of this lane still free to become pivots
-	bool freer[RPL];
-#pragma unroll
-	for (int p = 0; p < RPL; p++) freer[p] = lane + 32 * p < N;
-	// LU, implicit partial pivoting: rows stay put, prow[j] is the pivot row
-	for (int j = 0; j < N; j++) {
-		const int ow = j % NW, oq = j / NW;
-		if (w == ow) {
-			T col[RPL];
-#pragma unroll
-			for (int p = 0; p < RPL; p++) {
-				T v = x[0][p];
-#pragma unroll
-				for (int q = 1; q < CPW; q++)
-					if (q == oq) v = x[q][p];
-				col[p] = v;
-			}
-			double best = -1.0;
-			int br = N;
-#pragma unroll
-			for (int p = 0; p < RPL; p++) {
-				const int r = lane + 32 * p;
-				if (freer[p]) {
-					const double m = absv(col[p]);
-					if (m > best || (m == best && r < br)) { best = m; br = r; }
-				}
-			}
-			for (int o = 16; o > 0; o >>= 1) {
-				const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-				const int orr = __shfl_xor_sync(0xffffffffu, br, o);
-				if (ob > best || (ob == best && orr < br)) { best = ob; br = orr; }
-			}
-			if (br >= N) {
-				// no comparable candidate (NaN column): first free row
-				if (lane == 0 && a.err) atomicOr(a.err, DQ_ERR_NAN);
-				int fr = N;
-#pragma unroll
-				for (int p = 0; p < RPL; p++)
-					if (freer[p] && lane + 32 * p < fr) fr = lane + 32 * p;
-				for (int o = 16; o > 0; o >>= 1) fr = min(fr, __shfl_xor_sync(0xffffffffu, fr, o));
-				br = fr < N ? fr : 0;
-			}
-			T piv = row_of(col, br, lane);
-			if (re(piv) == 0.0 && im(piv) == 0.0) {
-				if (lane == 0 && a.err) atomicOr(a.err, DQ_ERR_SINGULAR);
-				piv = one<T>();
-			}
-			const T ipiv = one<T>() / piv;
-#pragma unroll
-			for (int p = 0; p < RPL; p++) {
-				const int r = lane + 32 * p;
-				if (r < N) {
-					const bool el = freer[p] && r != br;
-					const T l = el ? col[p] * ipiv : zero<T>();
-					lcol[r] = l;
-					if (el) LU[r + (size_t)N * j] = l;
-				}
-			}
-			if (lane == 0) {
-				s_prow = br;
-				prow[j] = br;
-				stepof[br] = j;
-			}
-		}
-		__syncthreads();
-		const int pr = s_prow;
-#pragma unroll
-		for (int p = 0; p < RPL; p++)
-			if (lane + 32 * p == pr) freer[p] = false;
-		T lr[RPL];
-#pragma unroll
-		for (int p = 0; p < RPL; p++) {
-			const int r = lane + 32 * p;
-			lr[p] = (r < N) ? lcol[r] : zero<T>();
-		}
-		T xp[CPW];
-#pragma unroll
-		for (int q = 0; q < CPW; q++) {
-			T v = zero<T>();
-#pragma unroll
-			for (int p = 0; p < RPL; p++)
-				if (lane + 32 * p == pr) v = x[q][p];
-			xp[q] = v;
-		}
-#pragma unroll
-		for (int q = 0; q < CPW; q++) xp[q] = shfl(xp[q], pr & 31);
-#pragma unroll
-		for (int q = 0; q < CPW; q++) {
-			const T f = (w + NW * q > j) ? xp[q] : zero<T>();
-#pragma unroll
-			for (int p = 0; p < RPL; p++) x[q][p] = x[q][p] - lr[p] * f;
-		}
-		__syncthreads();
-	}
-	// U entries: row r holds U[stepof[r]][c] for c >= stepof[r]
-#pragma unroll
-	for (int q = 0; q < CPW; q++) {
-		const int c = w + NW * q;
-		if (c >= N) continue;
-#pragma unroll
-		for (int p = 0; p < RPL; p++) {
-			const int r = lane + 32 * p;
-			if (r < N && stepof[r] <= c) LU[r + (size_t)N * c] = x[q][p];
-		}
-	}
-	__syncthreads();
-
-	// right-hand sides Y = diag(v) Q^H, solve M G = Y
-	int sr[RPL];
-#pragma unroll
-	for (int p = 0; p < RPL; p++) {
-		const int r = lane + 32 * p;
-		sr[p] = r < N ? stepof[r] : -1;
-	}
-#pragma unroll
-	for (int q = 0; q < CPW; q++) {
-		const int c = w + NW * q;
-#pragma unroll
-		for (int p = 0; p < RPL; p++) {
-			const int r = lane + 32 * p;
-			x[q][p] = (c < N && r < N) ? conjv(Q[c + (size_t)N * r]) * vsh[r] : zero<T>();
-		}
-	}
-	// forward: eliminate below the pivots in step order
-	for (int j = 0; j < N; j++) {
-		const int pr = prow[j];
-		T m[RPL];
-#pragma unroll
-		for (int p = 0; p < RPL; p++) {
-			const int r = lane + 32 * p;
-			m[p] = (r < N && sr[p] > j) ? LU[r + (size_t)N * j] : zero<T>();
-		}
-		T yp[CPW];
-#pragma unroll
-		for (int q = 0; q < CPW; q++) {
-			T v = zero<T>();
-#pragma unroll
-			for (int p = 0; p < RPL; p++)
-				if (lane + 32 * p == pr) v = x[q][p];
-			yp[q] = v;
-		}
-#pragma unroll
-		for (int q = 0; q < CPW; q++) yp[q] = shfl(yp[q], pr & 31);
-#pragma unroll
-		for (int q = 0; q < CPW; q++)
-#pragma unroll
-			for (int p = 0; p < RPL; p++) x[q][p] = x[q][p] - m[p] * yp[q];
-	}
-	// backward: x_j = y[prow j] / U_jj, then remove it from earlier pivot rows
-	for (int j = N - 1; j >= 0; j--) {
-		const int pr = prow[j];
-		const T ujj = LU[pr + (size_t)N * j];
-		const T iu = (re(ujj) == 0.0 && im(ujj) == 0.0) ? one<T>() : one<T>() / ujj;
-		T u[RPL];
-#pragma unroll
-		for (int p = 0; p < RPL; p++) {
-			const int r = lane + 32 * p;
-			u[p] = (r < N && sr[p] < j) ? LU[r + (size_t)N * j] : zero<T>();
-		}
-		T yp[CPW];
-#pragma unroll
-		for (int q = 0; q < CPW; q++) {
-			T v = zero<T>();
-#pragma unroll
-			for (int p = 0; p < RPL; p++)
-				if (lane + 32 * p == pr) v = x[q][p];
-			yp[q] = v;
-		}
-#pragma unroll
-		for (int q = 0; q < CPW; q++) yp[q] = shfl(yp[q], pr & 31) * iu;
-#pragma unroll
-		for (int q = 0; q < CPW; q++)
-#pragma unroll
-			for (int p = 0; p < RPL; p++) {
-				if (lane + 32 * p == pr) x[q][p] = yp[q];
-				else x[q][p] = x[q][p] - u[p] * yp[q];
-			}
-	}
-	T *G = a.G + (size_t)item * a.g_stride;
-#pragma unroll
-	for (int q = 0; q < CPW; q++) {
-		const int c = w + NW * q;
-		if (c >= N) continue;
-#pragma unroll
-		for (int p = 0; p < RPL; p++) {
-			const int r = lane + 32 * p;
-			if (r < N) G[sr[p] + (size_t)N * c] = x[q][p];
-		}
-	}
-	if (tid == 0) {
-		// 1/phase(det G) = phase(det M) conj(phase(prod v)) phase(det Q)
-		T ph = a.qdet ? a.qdet[item] : one<T>();
-		double vs = 1.0;
-		for (int j = 0; j < N; j++) {
-			ph = ph * phase_of(LU[prow[j] + (size_t)N * j]);
-			vs *= (vsh[j] < 0.0) ? -1.0 : 1.0;
-		}
-		// sign of the permutation j -> prow[j]
-		int parity = 0;
-		for (int j = 0; j < N; j++) rused[j] = 0;
-		for (int j = 0; j < N; j++) {
-			if (rused[j]) continue;
-			int len = 0, q = j;
-			while (q >= 0 && q < N && !rused[q] && len <= N) { rused[q] = 1; q = prow[q]; len++; }
-			if (q < 0 || q >= N) {
-				if (a.err) atomicOr(a.err, DQ_ERR_NAN);
-				break;
-			}
-			parity ^= (len - 1) & 1;
-		}
-		if (parity) ph = ph * -1.0;
-		a.phase[item] = ph * vs;
-	}
-}
-
 // ----------------------------------------------- recombine in shared memory
 //
-// k_recombine's G = (D_b^-1 Q^H + D_s T)^-1 D_b^-1 Q^H (greens.c:157-178)
+// G = (D_b^-1 Q^H + D_s T)^-1 D_b^-1 Q^H (greens.c:157-178)
 // with M in shared memory: LU with partial pivoting and physical row swaps
 // (getrf: the first largest |M[r, j]| of the column, as idamax); warp 0
 // picks, swaps and scales, all warps update the trailing columns.  Then
@@ -1341,22 +700,23 @@ __global__ void __launch_bounds__(NW * 32) k_recombine(RecArgs<T> a)
 // phase 1/phase(det G) = phase(det Q) phase(det M) sign(prod v).
 
 template <typename T>
-size_t recb_smem_bytes(int N)
+size_t recb_smem_bytes(int N, bool gm = false)
 {
-	return sizeof(T) * (size_t)qrb_ld(N) * N + sizeof(double) * 2 * (size_t)N + sizeof(int) * 2 * (size_t)N
-	       + 64;
+	return (gm ? 0 : sizeof(T) * (size_t)qrb_ld(N) * N) + sizeof(double) * 2 * (size_t)N
+	       + sizeof(int) * 2 * (size_t)N + 64;
 }
 
-template <typename T, int NW, int RPL, int CB>
+template <typename T, int NW, int RPL, int CB, bool GM>
 __global__ void __launch_bounds__(NW * 32) k_recb(RecArgs<T> a)
 {
 	const int item = blockIdx.x;
 	if (item >= a.batch) return;
-	const int N = a.N, ld = qrb_ld(N);
+	const int N = a.N, ld = GM ? N : qrb_ld(N);
 	const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
 	extern __shared__ __align__(16) unsigned char smraw[];
-	T *M = (T *)smraw;                          // N columns, leading dimension ld
-	double *vsh = (double *)(M + (size_t)ld * N);   // D_b^-1
+	// N columns, leading dimension ld
+	T *M = GM ? a.work + (size_t)item * a.w_stride : (T *)smraw;
+	double *vsh = GM ? (double *)smraw : (double *)(M + (size_t)ld * N);   // D_b^-1
 	double *dss = vsh + N;                      // D_s
 	int *ipiv = (int *)(dss + N);               // row swapped with row j at step j
 	int *perm = ipiv + N;                       // row r of P Y is row perm[r] of Y

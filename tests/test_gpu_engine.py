@@ -316,12 +316,15 @@ def _gen_case(tmp_path, Nx, Ny, **kw):
     return path
 
 
-@pytest.mark.parametrize("Nx,Ny", [(10, 10), (12, 12), (16, 10)])
-def test_calc_eq_g_seam_large(eng, Nx, Ny, tmp_path):
+# 10x10 .. 12x12 real run the shared-memory kernels; 16x10, 14x14 and 16x16
+# real and 12x12 complex the global-memory form of the same kernels
+@pytest.mark.parametrize("Nx,Ny,nflux", [(10, 10, 0), (12, 12, 0), (16, 10, 0), (14, 14, 0),
+                                         (16, 16, 0), (12, 12, 1)])
+def test_calc_eq_g_seam_large(eng, Nx, Ny, nflux, tmp_path):
     import torch
     from dqmc_b200 import lib
     path = _gen_case(tmp_path, Nx, Ny, U=4.0, mu=-1.0, dt=0.05, L=40, n_matmul=5, n_delay=16,
-                     period_eqlt=8)
+                     period_eqlt=8, nflux=nflux)
     o = Sim(path)
     N, F, nmul = o.N, o.p["F"], o.p["n_matmul"]
     for spin in (0, 1):
@@ -344,12 +347,12 @@ def test_calc_eq_g_seam_large(eng, Nx, Ny, tmp_path):
             assert abs(dph.cpu().numpy()[0] - ph_o[0]) < 1e-12
 
 
-@pytest.mark.parametrize("Nx,Ny", [(12, 12)])
-def test_engine_large_matches_oracle(eng, Nx, Ny, tmp_path):
-    """2 sweeps of a 12x12 chain (L = 20): HS fields and RNG bit-exact, G and
+@pytest.mark.parametrize("Nx,Ny,nflux", [(12, 12, 0), (16, 16, 0), (10, 10, 1)])
+def test_engine_large_matches_oracle(eng, Nx, Ny, nflux, tmp_path):
+    """2 sweeps of a large chain (L = 20): HS fields and RNG bit-exact, G and
     the equal-time measurements within tolerance of the oracle."""
     path = _gen_case(tmp_path, Nx, Ny, U=4.0, mu=-1.0, dt=0.05, L=20, n_matmul=5, n_delay=16,
-                     period_eqlt=5, n_sweep_warm=0, n_sweep_meas=2)
+                     period_eqlt=5, n_sweep_warm=0, n_sweep_meas=2, nflux=nflux)
     o = Sim(path)
     gu_o, gd_o, ph_o = o.run(stop_sweep=2)
     s, e = _run(eng, path, 2)
