@@ -444,6 +444,29 @@ static void invert_map(const int *map, int n_entries, int n_class, std::vector<i
 	for (int e = 0; e < n_entries; e++) idx[fill[map[e]]++] = e;
 }
 
+// The dynamic shared-memory limit of a kernel is one setting per function,
+// shared by every engine of the process: only ever raise it, so that a group
+// created later with smaller needs cannot shrink it below what an earlier
+// group's launches (and captured graphs) rely on.
+template <typename K>
+static cudaError_t raise_smem(K kern, size_t bytes)
+{
+	static std::mutex mu;
+	static std::map<const void *, size_t> cur;
+	std::lock_guard<std::mutex> lk(mu);
+	size_t &c = cur[(const void *)kern];
+	if (bytes <= c) return cudaSuccess;
+	const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+	if (e == cudaSuccess) c = bytes;
+	return e;
+}
+
+template <typename T>
+static cudaError_t update_attr(size_t bytes)
+{
+	return raise_smem(k_update<T>, bytes);
+}
+
 struct GroupBase {
 	virtual ~GroupBase() {}
 	virtual int set_chain(int c, const double *el, const double *del, const uint64_t *rng,
@@ -594,8 +617,7 @@ struct Group : GroupBase, ProfHook {
 		kd = p.n_delay < 1 ? 1 : p.n_delay;
 		ldp = (N + 15) / 16 * 16 + 4;
 		while (kd > 1 && update_smem_bytes<T>(N, kd, ldp) > 200 * 1024) kd /= 2;
-		cudaFuncSetAttribute(k_update<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-		                     (int)update_smem_bytes<T>(N, kd, ldp));
+		CK(update_attr<T>(update_smem_bytes<T>(N, kd, ldp)));
 		CK(cudaDeviceSynchronize());
 		return 0;
 	}
@@ -794,7 +816,7 @@ struct Group : GroupBase, ProfHook {
 		constexpr int NBK = 8, NW = 16;
 		const size_t sm = hqr_smem_bytes<T, NBK, NW>(h.M);
 		auto go = [&](auto kern) -> int {
-			CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+			CK(raise_smem(kern, sm));
 			prof_begin(0);
 			kern<<<h.batch, NW * 32, sm, st>>>(h);
 			prof_end(PC_UNEQ, 0.0, 0.0);
@@ -873,7 +895,7 @@ struct Group : GroupBase, ProfHook {
 		{
 			TriArgs<T> t{N, NE, E, NB, ue.O.p, ue.Gr.p, err.p};
 			const size_t sm = trtri_smem_bytes<T>(N);
-			CK(cudaFuncSetAttribute(k_trtri<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+			CK(raise_smem(k_trtri<T>, sm));
 			prof_begin(0);
 			k_trtri<T><<<NB * E, 256, sm, st>>>(t);
 			launch_count++;
@@ -1346,8 +1368,7 @@ static int seam_update(int batch, int N, int n_delay, const double *del, uint64_
 	int kd = n_delay;
 	const int ldp = (N + 15) / 16 * 16 + 4;
 	while (kd > 1 && update_smem_bytes<T>(N, kd, ldp) > 200 * 1024) kd /= 2;
-	CK(cudaFuncSetAttribute(k_update<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-	                        (int)update_smem_bytes<T>(N, kd, ldp)));
+	CK(update_attr<T>(update_smem_bytes<T>(N, kd, ldp)));
 	Scratch<T> sc;
 	uint64_t *ck = sc.template get<uint64_t>((size_t)batch * 17);
 	int *ord = sc.template get<int>((size_t)batch * 2 * N);

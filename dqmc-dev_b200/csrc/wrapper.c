@@ -584,33 +584,83 @@ int dqmc_wrapper_batch(int n_files, const char *const *sim_files, const char *lo
 		ng++;
 	}
 	fprintf(log, "%d files in %d parameter groups\n", n_files, ng);
+	/* one engine (and CUDA stream) per group; each round queues one sweep
+	 * of every unfinished group on its own stream, so that groups of
+	 * different lattices, L or n_delay run concurrently, then waits for all */
+	struct grp {
+		dqmc_engine *e;
+		struct sim **m;
+		int *idx;
+		int n, rc, done, queued;
+	};
+	struct grp *gs = calloc(ng > 0 ? ng : 1, sizeof(struct grp));
 	for (int gi = 0; gi < ng; gi++) {
+		struct grp *g = &gs[gi];
+		for (int i = 0; i < n_files; i++) g->n += group[i] == gi;
+		g->m = calloc(g->n, sizeof(struct sim *));
+		g->idx = calloc(g->n, sizeof(int));
 		int n = 0;
-		for (int i = 0; i < n_files; i++) n += group[i] == gi;
-		struct sim **members = calloc(n, sizeof(struct sim *));
-		int *idx = calloc(n, sizeof(int));
-		n = 0;
 		for (int i = 0; i < n_files; i++)
-			if (group[i] == gi) { idx[n] = i; members[n++] = &sims[i]; }
-		dqmc_engine *e = NULL;
-		int64_t t0 = time_wall();
-		int rc = engine_from(members, n, &e);
+			if (group[i] == gi) { g->idx[n] = i; g->m[n++] = &sims[i]; }
+		const int64_t t0 = time_wall();
+		g->rc = engine_from(g->m, g->n, &g->e);
 		pr.t[PR_INIT] += time_wall() - t0;
 		pr.n[PR_INIT]++;
-		if (!rc) rc = run_group(e, members, n, &stp, &pr);
+	}
+	for (;;) {
+		int active = 0;
+		const int64_t t0 = time_wall();
+		for (int gi = 0; gi < ng; gi++) {
+			struct grp *g = &gs[gi];
+			g->queued = 0;
+			if (g->done || g->rc) continue;
+			const dqmc_params *p = &g->m[0]->p;
+			const int sweep = g->m[0]->sweep;
+			if (sweep >= p->n_sweep) { g->done = 1; continue; }
+			if (check_stop(&stp, sweep, p->n_sweep_warm, p->n_sweep)) { g->rc = 5; continue; }
+			const int ce = g->m[0]->checkpoint_every;
+			if (ce > 0 && sweep % ce == 0) {
+				const int64_t tc = time_wall();
+				int rc = engine_pull(g->e, g->m, g->n);
+				for (int c = 0; rc == 0 && c < g->n; c++) rc = sim_save(g->m[c]);
+				pr.t[PR_CHECKPOINT] += time_wall() - tc;
+				pr.n[PR_CHECKPOINT]++;
+				if (rc) { g->rc = 6; continue; }
+			}
+			g->rc = dqmc_engine_sweeps(g->e, 1, 0);
+			if (g->rc) continue;
+			g->queued = 1;
+			active = 1;
+		}
+		if (!active) break;
+		for (int gi = 0; gi < ng; gi++) {
+			struct grp *g = &gs[gi];
+			if (!g->queued) continue;
+			g->rc = dqmc_engine_sync(g->e);
+			if (g->rc) continue;
+			for (int c = 0; c < g->n; c++) g->m[c]->sweep++;
+		}
+		pr.t[PR_SWEEPS] += time_wall() - t0;
+		pr.n[PR_SWEEPS]++;
+	}
+	for (int gi = 0; gi < ng; gi++) {
+		struct grp *g = &gs[gi];
+		int rc = g->rc;
+		if (!rc && g->e) rc = engine_pull(g->e, g->m, g->n);
 		int st = 0;
 		if (rc == 5) st = WRAP_INCOMPLETE;
 		else if (rc) st = WRAP_FAIL;
 		if (st == 0 && !bench)
-			for (int k = 0; k < n; k++)
-				if (sim_save(members[k]) < 0) status[idx[k]] = WRAP_FAIL;
-		for (int k = 0; k < n; k++)
-			if (!status[idx[k]]) status[idx[k]] = st;
-		fprintf(log, "group %d: %d chains, status %d\n", gi, n, st);
-		dqmc_engine_destroy(e);
-		free(members);
-		free(idx);
+			for (int k = 0; k < g->n; k++)
+				if (sim_save(g->m[k]) < 0) status[g->idx[k]] = WRAP_FAIL;
+		for (int k = 0; k < g->n; k++)
+			if (!status[g->idx[k]]) status[g->idx[k]] = st;
+		fprintf(log, "group %d: %d chains, status %d\n", gi, g->n, st);
+		if (g->e) dqmc_engine_destroy(g->e);
+		free(g->m);
+		free(g->idx);
 	}
+	free(gs);
 	for (int i = 0; i < n_files; i++) {
 		if (status[i] == WRAP_FAIL) worst = WRAP_FAIL;
 		else if (status[i] == WRAP_INCOMPLETE && worst == 0) worst = WRAP_INCOMPLETE;

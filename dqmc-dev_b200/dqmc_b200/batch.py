@@ -1,0 +1,126 @@
+"""Ragged batches: chains of different lattices, U and beta on one GPU.
+
+The engine advances a group of chains that share every parameter it keeps
+per group: the lattice and its measurement maps, L and n_matmul, the
+hopping matrices, the measurement periods and the sweep counters.  U may
+differ inside a group, because exp_lambda and del are per chain.  A ragged
+batch therefore splits its chains into such groups.  Each group gets its own
+engine and CUDA stream, and each sweep queues every group's captured sweep
+graph before waiting for any of them.  Groups of different size and length
+so run concurrently, as the C drop-in's dqmc_wrapper_batch runs them.
+
+The delay rank (n_delay: rank-k updates collected before they are flushed
+into G) trades per-accept work against flush traffic, and the best value
+depends on N.  With `autotune`, each lattice size gets the candidate whose
+timed sweep of a copy of its first group is shortest.  Changing n_delay
+changes results only by rounding; without `autotune` every group keeps its
+files' value.
+"""
+from __future__ import annotations
+
+import hashlib
+import time
+from collections import OrderedDict
+
+import numpy as np
+
+from .engine import INT_PARAMS, Engine, SimData
+
+# parameters a group shares (everything except U's exp_lambda and del)
+_SHARED_ARRAYS = ("map_i", "map_ij", "bonds", "map_bb", "peierlsu", "peierlsd")
+
+
+def group_key(s: SimData) -> str:
+    """Digest of the parameters the chains of one group must share."""
+    h = hashlib.sha1()
+    h.update(repr([(k, s.p[k]) for k in INT_PARAMS if k not in ("n_delay",)]).encode())
+    h.update(repr((s.cplx, s.sweep)).encode())
+    for name in _SHARED_ARRAYS:
+        a = getattr(s, name, None)
+        if a is not None:
+            h.update(np.ascontiguousarray(a).tobytes())
+    for name in sorted(s.mats):
+        h.update(np.ascontiguousarray(s.mats[name]).tobytes())
+    return h.hexdigest()
+
+
+def time_sweep(sims: list[SimData], n_delay: int | None, device: int = 0) -> float:
+    """Seconds of one sweep of copies of `sims` at delay rank n_delay (after
+    one untimed sweep that also captures the sweep graph)."""
+    copies = [s.clone() for s in sims]
+    e = Engine(copies, device=device, n_delay=n_delay)
+    try:
+        e.init()
+        e.sweeps(1, sync=True)
+        t0 = time.perf_counter()
+        e.sweeps(1, sync=True)
+        return time.perf_counter() - t0
+    finally:
+        e.close()
+
+
+def autotune_delay(sims: list[SimData], candidates=(4, 8, 16, 32), device: int = 0,
+                   max_chains: int = 8) -> int:
+    """The candidate delay rank with the shortest timed sweep of (up to
+    max_chains of) these chains; candidates a chain cannot use are skipped."""
+    probe = sims[:max_chains]
+    best, best_t = None, None
+    for kd in candidates:
+        if kd > probe[0].N:
+            continue
+        t = time_sweep(probe, kd, device)
+        if best_t is None or t < best_t:
+            best, best_t = kd, t
+    return best
+
+
+class RaggedBatch:
+    """Chains of any parameters advanced together; see the module docstring."""
+
+    def __init__(self, sims: list[SimData], device: int = 0, autotune: bool = False,
+                 candidates=(4, 8, 16, 32)):
+        if not sims:
+            raise ValueError("no chains")
+        self.sims = sims
+        groups: OrderedDict[str, list[int]] = OrderedDict()
+        for i, s in enumerate(sims):
+            groups.setdefault(group_key(s), []).append(i)
+        self.groups = list(groups.values())
+        self.delay = {}
+        if autotune:
+            # one tuning per lattice size, on the first group of that size
+            for idx in self.groups:
+                n = sims[idx[0]].N
+                if n not in self.delay:
+                    self.delay[n] = autotune_delay([sims[i] for i in idx], candidates, device)
+        self.engines = [Engine([sims[i] for i in idx], device=device,
+                               n_delay=self.delay.get(sims[idx[0]].N))
+                        for idx in self.groups]
+
+    def init(self):
+        for e in self.engines:
+            e.init()
+
+    def sweeps(self, n: int = 1):
+        """n sweeps of every chain: sweep by sweep, all groups queued before
+        any is waited for."""
+        for _ in range(n):
+            for e in self.engines:
+                e.sweeps(1, sync=False)
+            for e in self.engines:
+                e.sync()
+
+    def errors(self) -> int:
+        out = 0
+        for e in self.engines:
+            out |= e.errors()
+        return out
+
+    def pull(self):
+        for e in self.engines:
+            e.pull()
+
+    def close(self):
+        for e in self.engines:
+            e.close()
+        self.engines = []

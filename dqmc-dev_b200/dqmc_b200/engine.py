@@ -68,6 +68,11 @@ class SimData:
             self.ue_acc = np.concatenate(parts).astype(nt)
         self._sizes = (ni, nij, nbb)
 
+    def clone(self) -> "SimData":
+        """An independent copy (state and accumulators included)."""
+        import copy
+        return copy.deepcopy(self)
+
     @classmethod
     def read(cls, path: str) -> "SimData":
         d = simfile.read(path)
@@ -129,13 +134,18 @@ class SimData:
 class Engine:
     """A group of chains with one parameter set, advanced on one GPU."""
 
-    def __init__(self, sims: list[SimData], device: int = 0):
+    def __init__(self, sims: list[SimData], device: int = 0, n_delay: int | None = None):
+        """n_delay overrides the sim files' delay rank (the flush period of
+        the delayed update); results then differ from the file's setting
+        only by rounding."""
         if not sims:
             raise ValueError("no chains")
         self.lib = _lib.load()
         self.sims = sims
         s0 = sims[0]
         self._p, self._keep = s0.params()
+        if n_delay is not None:
+            self._p.n_delay = int(n_delay)
         h = C.c_void_p()
         _lib.check(self.lib.dqmc_engine_create(C.byref(self._p), len(sims), device, C.byref(h)),
                    "dqmc_engine_create")

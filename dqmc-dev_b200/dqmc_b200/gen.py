@@ -330,3 +330,24 @@ def create_batch(Nfiles=1, prefix="sim", seed=0, **kw):
         simfile.write(path, sim)
         paths.append(path)
     return paths
+
+
+def make_ragged(n: int, seed: int, sides=(6, 8, 10, 14, 16), U=(2.0, 8.0), beta=(2.0, 8.0),
+                dt: float = 0.05, n_matmul: int = 10, **kw) -> list:
+    """Sim data of n chains with uneven lattices, U and beta: side uniform in
+    `sides`, U and beta uniform in their ranges, L = beta / dt rounded to a
+    multiple of n_matmul (the generator requires L % n_matmul == 0).  The
+    per-chain draws come from numpy's PCG64 of `seed`; chain c's Markov
+    chain starts from the master stream of `seed` jumped c times."""
+    draw = np.random.Generator(np.random.PCG64(seed))
+    rngs = chain_rngs(seed, n)
+    period_eqlt = kw.pop("period_eqlt", n_matmul)
+    out = []
+    for c in range(n):
+        side = int(draw.choice(np.asarray(sides)))
+        u = float(draw.uniform(*U))
+        b = float(draw.uniform(*beta))
+        L = max(n_matmul, int(round(b / dt / n_matmul)) * n_matmul)
+        out.append(make_sim(Nx=side, Ny=side, U=u, dt=dt, L=L, n_matmul=n_matmul,
+                            init_rng=rngs[c], period_eqlt=period_eqlt, **kw))
+    return out
