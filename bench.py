@@ -223,6 +223,116 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(line))
 
 
+def plain_chain_rate(sim, device, warm=2, timed=3):
+    """chain-sweeps/s of the plain single-chain GPU path: one chain of the
+    same model alone in an engine (graph-replayed sweeps, CUDA events)."""
+    import torch
+    from dqmc_b200 import engine
+    c = sim.clone()
+    c.p["n_sweep"] = c.sweep + warm + timed + 2     # room for the sweeps below
+    e = engine.Engine([c], device=device)
+    try:
+        e.init()
+        e.sweeps(warm, sync=True)
+        st = torch.cuda.ExternalStream(e.stream())
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(st)
+        e.sweeps(timed, sync=False)
+        b.record(st)
+        torch.cuda.synchronize()
+        return timed / (a.elapsed_time(b) / 1e3)
+    finally:
+        e.close()
+
+
+# further workloads of the benchmark configurations, one JSON line each:
+# builder(n_sweep) -> list of sim dicts, description
+def _ragged64(n_sweep):
+    from dqmc_b200 import gen
+    return gen.make_ragged(64, SEED, n_sweep_warm=0, n_sweep_meas=n_sweep, period_eqlt=10), (
+        "64 ragged chains: square lattice side uniform in {6,8,10,14,16}, U uniform in [2,8], "
+        "beta uniform in [2,8], dtau=0.05, L rounded to a multiple of n_matmul=10, n_delay "
+        "autotuned per lattice size, eqlt every 10 slices, FP64")
+
+
+def _complex64(n_sweep):
+    from dqmc_b200 import gen, replicas
+    rngs = replicas.chain_streams(SEED, range(64))
+    base = gen.make_sim(Nx=10, Ny=10, U=4.0, mu=0.0, dt=0.1, L=50, n_matmul=5, n_delay=16,
+                        nflux=1, period_eqlt=5, period_uneqlt=1, meas_bond_corr=1,
+                        n_sweep_warm=0, n_sweep_meas=n_sweep, init_rng=rngs[0])
+    return _restream(base, rngs, 100, 50), (
+        "64 chains x 10x10 square Hubbard with one flux quantum (Peierls phases, complex128), "
+        "U=4, mu=0, beta=5, dtau=0.1 (L=50), n_matmul=5, eqlt every 5 slices, unequal-time "
+        "(with current-current bond correlators) every sweep")
+
+
+def _uneq8x8(n_sweep):
+    from dqmc_b200 import gen, replicas
+    rngs = replicas.chain_streams(SEED, range(1))
+    return [gen.make_sim(Nx=8, Ny=8, tp=-0.25, U=6.0, mu=-0.5, dt=0.1, L=80, n_matmul=8,
+                         n_delay=16, period_eqlt=8, period_uneqlt=4, n_sweep_warm=0,
+                         n_sweep_meas=n_sweep, init_rng=rngs[0])], (
+        "1 chain x 8x8 square Hubbard, t'=-0.25, U=6, mu=-0.5, beta=8, dtau=0.1 (L=80), "
+        "n_matmul=8, n_delay=16, eqlt every 8 slices, unequal-time every 4 sweeps, FP64")
+
+
+def _restream(base, rngs, N, L):
+    from dqmc_b200 import gen
+    out = [base]
+    for r in rngs[1:]:
+        hs, rng = gen.initial_hs(r, L, N)
+        d = dict(base)
+        d["state/init_rng"], d["state/rng"], d["state/hs"] = r, rng, hs
+        out.append(d)
+    return out
+
+
+EXTRA = {"ragged64": _ragged64, "complex64": _complex64, "uneq8x8": _uneq8x8}
+
+
+def run_extra(args, rank, world, local):
+    """One of the further benchmark workloads as a ragged batch (one engine
+    and stream per parameter group): K sweeps of every chain, timed on the
+    host around synchronised sweeps because several streams take part."""
+    import torch
+    torch.cuda.set_device(local)
+    from dqmc_b200 import batch, engine
+    dicts, desc = EXTRA[args.workload](args.warmup + args.steps + 2)
+    sims = [engine.SimData(d) for d in dicts]
+    log(f"generated {len(sims)} chains")
+    rb = batch.RaggedBatch(sims, device=local, autotune=args.workload == "ragged64")
+    rb.init()
+    rb.sweeps(args.warmup)
+    barrier(world)
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        t0 = time.perf_counter()
+        rb.sweeps(args.steps)
+        torch.cuda.synchronize()
+        t = time.perf_counter() - t0
+    barrier(world)
+    assert rb.errors() == 0, "device error word set"
+    t_max = max_over_ranks(t, world)
+    launches = sum(max(e.launches_per_sweep(True, False), e.launches_per_sweep(True, True))
+                   for e in rb.engines) * args.steps
+    rb.close()
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": len(sims) * args.steps * world / t_max, "unit": METRIC,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "c128" if sims[0].cplx else "f64", "data": "synthetic",
+            "config": {"workload": desc, "chains_per_gpu": len(sims), "groups": len(rb.groups),
+                       "delay_rank": {str(k): v for k, v in rb.delay.items()},
+                       "timing": "host clock around device-synchronised sweeps (several streams)"},
+            "gpu_launches": launches, "e2e": None, "roofline": None,
+            "clocks": clk.summary(), "cpu_baseline": None,
+        }))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -231,8 +341,16 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--chains", type=int, default=CHAINS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="batch256", choices=["batch256"] + sorted(EXTRA),
+                    help="batch256: the headline (default); the others print their own line")
     args = ap.parse_args()
     rank, world, local = dist_setup(args.gpus)
+    if args.impl == "ours" and args.workload != "batch256":
+        run_extra(args, rank, world, local)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
         if world > 1:
@@ -315,6 +433,9 @@ def main():
     items = 2 * nch
     traffic = TRAFFIC_PER_ITEM.get(dom)
 
+    plain = plain_chain_rate(sims[0], local)
+    log("plain single-chain sweeps done")
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -337,7 +458,10 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "chains_per_gpu": nch,
                        "l2": "inputs larger than L2 (about 2.6 MB of matrices per chain-spin)",
-                       "sweep_profile_ms": sweep_ms},
+                       "sweep_profile_ms": sweep_ms,
+                       "plain_1chain_gpu": {"value": plain, "unit": METRIC,
+                                            "batched_over_plain": value / world / plain
+                                            if plain else None}},
             "gpu_launches": launches,
             "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
