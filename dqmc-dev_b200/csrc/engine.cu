@@ -259,6 +259,7 @@ struct EqWork {
 	T *qdet;                           // NB
 	T *G; long long g_stride;          // output
 	T *phi;                            // NB output phases
+	double *logdet;                    // NB, optional: log |det(I + C...C)|
 	unsigned *err;
 };
 
@@ -372,6 +373,7 @@ static int run_calc_eq_g(const EqWork<T> &w, int l0, cudaStream_t st, int *count
 	ra.G = w.G; ra.g_stride = w.g_stride;
 	ra.phase = w.phi;
 	ra.work = w.W; ra.w_stride = NN;
+	ra.logdet = w.logdet;
 	ra.err = w.err;
 	if (ph) ph->begin();
 	if (launch_rec<T>(ra, st)) return DQMC_E_ARG;
@@ -444,6 +446,25 @@ static void invert_map(const int *map, int n_entries, int n_class, std::vector<i
 	for (int e = 0; e < n_entries; e++) idx[fill[map[e]]++] = e;
 }
 
+// S_b += diag(d_l) (I - G_b) diag(1/d_l): the slice-l term of the log-det
+// gradient sums, d_l = exp(V_l) of item b
+template <typename T>
+__global__ void k_grad_acc(int N, int NB, int L, int l, const T *G, const double *dv,
+		const double *dvi, T *S)
+{
+	const long long NN = (long long)N * N;
+	for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < NN * NB;
+	     q += (long long)gridDim.x * blockDim.x) {
+		const int b = (int)(q / NN);
+		const long long e = q % NN;
+		const int i = (int)(e % N), j = (int)(e / N);
+		const size_t o = ((size_t)b * L + l) * N;
+		const T g = G[q];
+		const T x = (i == j) ? one<T>() - g : -g;
+		S[q] = S[q] + x * (dv[o + i] * dvi[o + j]);
+	}
+}
+
 // The dynamic shared-memory limit of a kernel is one setting per function,
 // shared by every engine of the process: only ever raise it, so that a group
 // created later with smaller needs cannot shrink it below what an earlier
@@ -483,6 +504,7 @@ struct GroupBase {
 	virtual cudaStream_t stream() = 0;
 	virtual int launches(int meq, int mue) = 0;
 	virtual int profile(int meq, int mue, double *out, int ncls) = 0;
+	virtual int logdet_grad(double *logdet, void *S) = 0;
 };
 
 template <typename T>
@@ -532,7 +554,8 @@ struct Group : GroupBase, ProfHook {
 	bool need_draws = true;
 	bool need_init = true;     // G must be recomputed from the fields before sweeping
 	DevBuf<T> phase, G, Cl, Qm, Tm, Tm2, Rs, X, W, Gh, acc_eq, acc_ue, phi, qdet;
-	DevBuf<double> dR;
+	DevBuf<T> Sg;                  // gradient sums, allocated by the first logdet_grad
+	DevBuf<double> dR, ldet;       // UDT scales; log |det(I + B...B)| per item
 	DevBuf<int> pvt;
 	DevBuf<unsigned> err;
 	UneqState<T> ue;
@@ -541,12 +564,12 @@ struct Group : GroupBase, ProfHook {
 	{
 		for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
 		DevBuf<T> *tb[] = {&expK, &iexpK, &ehK, &iehK, &peu, &ped, &phase, &G, &Cl, &Qm, &Tm,
-		                   &Tm2, &Rs, &X, &W, &Gh, &acc_eq, &acc_ue, &phi, &qdet};
+		                   &Tm2, &Rs, &X, &W, &Gh, &acc_eq, &acc_ue, &phi, &qdet, &Sg};
 		for (auto *b : tb) b->release();
 		DevBuf<int> *ib[] = {&i_off, &i_idx, &ij_off, &ij_idx, &bb_off, &bb_idx, &bonds, &hs,
 		                     &nacc, &n_eq, &n_ue, &pvt};
 		for (auto *b : ib) b->release();
-		el.release(); del.release(); dv.release(); dvi.release(); dR.release();
+		el.release(); del.release(); dv.release(); dvi.release(); dR.release(); ldet.release();
 		rng.release(); rng_ckpt.release(); order.release(); ubuf.release(); err.release();
 		ue.release();
 		if (st) cudaStreamDestroy(st);
@@ -579,6 +602,7 @@ struct Group : GroupBase, ProfHook {
 		rc |= Qm.alloc(NB * NN); rc |= Tm.alloc(NB * NN); rc |= Tm2.alloc(NB * NN);
 		rc |= Rs.alloc(NB * NN); rc |= X.alloc(NB * NN); rc |= W.alloc(NB * NN);
 		rc |= Gh.alloc(NB * NN); rc |= dR.alloc((size_t)NB * N); rc |= pvt.alloc((size_t)NB * N);
+		rc |= ldet.alloc(NB);
 		rc |= err.alloc(1);
 		eq_size = eq_acc_size(p.num_i, p.num_ij);
 		ue_size = p.period_uneqlt > 0 ? ue_acc_size(p.num_ij, p.num_bb, L, p.meas_bond_corr) : 0;
@@ -705,12 +729,14 @@ struct Group : GroupBase, ProfHook {
 	EqWork<T> eq_work()
 	{
 		EqWork<T> w;
+		memset(&w, 0, sizeof(w));
 		w.N = N; w.F = F; w.NB = NB;
 		w.Cl = Cl.p; w.cl_stride = (long long)F * N * N;
 		w.Qm = Qm.p; w.Tm = Tm.p; w.Tm2 = Tm2.p; w.Rs = Rs.p; w.X = X.p; w.W = W.p;
 		w.dR = dR.p; w.pvt = pvt.p; w.qdet = qdet.p;
 		w.G = G.p; w.g_stride = (long long)N * N;
 		w.phi = phi.p; w.err = err.p;
+		w.logdet = ldet.p;
 		return w;
 	}
 
@@ -1123,6 +1149,38 @@ struct Group : GroupBase, ProfHook {
 		return 0;
 	}
 
+	// log |det(I + B_{L-1} ... B_0)| of every item and the sums
+	// S = sum_l diag(d_l) (I - G_l) diag(1/d_l) over the slices of one
+	// update-free sweep, G_l the equal-time G before slice l: the gradient
+	// d log |det| / d theta = sum_l tr[S_l D_theta] with D_theta =
+	// exp(dt K) d exp(-dt K) / d theta.  Fields, RNG and sweep count stay.
+	int logdet_grad(double *ld_out, void *S_out) override
+	{
+		const size_t NN = (size_t)N * N;
+		if (need_init) {
+			const int rc = init();
+			if (rc) return rc;
+		}
+		if (!Sg.p && Sg.alloc(NB * NN)) return DQMC_E_NOMEM;
+		CK(cudaMemsetAsync(Sg.p, 0, sizeof(T) * NB * NN, st));
+		for (int l = 0; l < L; l++) {
+			k_grad_acc<T><<<grid_for((long long)NB * NN), 256, 0, st>>>(N, NB, L, l, G.p, dv.p, dvi.p, Sg.p);
+			if ((l + 1) % nmul == 0) {
+				const int rc = calc_eq_g((l / nmul + 1) % F);
+				if (rc) return rc;
+			} else {
+				wrap(l);
+			}
+		}
+		CK(cudaStreamSynchronize(st));
+		CK(cudaGetLastError());
+		std::vector<double> ld(NB);
+		CK(cudaMemcpy(ld.data(), ldet.p, sizeof(double) * NB, cudaMemcpyDeviceToHost));
+		for (int c = 0; c < C; c++) if (ld_out) ld_out[c] = ld[2 * c] + ld[2 * c + 1];
+		if (S_out) CK(cudaMemcpy(S_out, Sg.p, sizeof(T) * NB * NN, cudaMemcpyDeviceToHost));
+		return sync();
+	}
+
 	int sync() override
 	{
 		CK(cudaStreamSynchronize(st));
@@ -1304,6 +1362,11 @@ int dqmc_engine_launches_per_sweep(dqmc_engine *e, int meas_eq, int meas_ue)
 	return e ? e->g->launches(meas_eq, meas_ue) : DQMC_E_ARG;
 }
 
+int dqmc_engine_logdet_grad(dqmc_engine *e, double *logdet, void *S)
+{
+	return e ? e->g->logdet_grad(logdet, S) : DQMC_E_ARG;
+}
+
 int dqmc_engine_profile_sweep(dqmc_engine *e, int meas_eq, int meas_ue, double *out, int n_class)
 {
 	return (e && out && n_class > 0) ? e->g->profile(meas_eq, meas_ue, out, n_class) : DQMC_E_ARG;
@@ -1337,6 +1400,7 @@ static int seam_calc_eq_g(int batch, int N, int F, int l, const void *C, void *G
 	const size_t NN = (size_t)N * N;
 	Scratch<T> sc;
 	EqWork<T> w;
+	memset(&w, 0, sizeof(w));
 	w.N = N; w.F = F; w.NB = batch;
 	w.Cl = (const T *)C; w.cl_stride = (long long)F * NN;
 	w.Qm = sc.template get<T>(batch * NN); w.Tm = sc.template get<T>(batch * NN);
@@ -1525,6 +1589,7 @@ static int noalloc_calc_eq_g(int batch, int N, int F, int l, const void *C, void
 	const size_t NN = (size_t)N * N;
 	auto take = [&](size_t bytes) { unsigned char *q = p; p += al256(bytes); return (void *)q; };
 	EqWork<T> w;
+	memset(&w, 0, sizeof(w));
 	w.N = N; w.F = F; w.NB = batch;
 	w.Cl = (const T *)C; w.cl_stride = (long long)F * NN;
 	w.Qm = (T *)take(sizeof(T) * batch * NN); w.Tm = (T *)take(sizeof(T) * batch * NN);

@@ -685,6 +685,7 @@ struct RecArgs {
 	const T *qdet;
 	T *G; long long g_stride;
 	T *phase;                 // per item: 1 / phase(det G)
+	double *logdet;           // per item, optional: log |det(I + B...B)| = -log |det G|
 	T *work; long long w_stride;   // N x N per item, global-memory form only
 	unsigned *err;
 };
@@ -892,6 +893,12 @@ __global__ void __launch_bounds__(NW * 32) k_recb(RecArgs<T> a)
 		}
 		if (nswap & 1) ph = ph * -1.0;
 		a.phase[item] = ph * vs;
+		if (a.logdet) {
+			// G = M^-1 diag(v) Q^H: log |det G| = sum log |v_j| - sum log |U_jj|
+			double l = 0.0;
+			for (int j = 0; j < N; j++) l += log(absv(M[j + (size_t)ld * j])) - log(fabs(vsh[j]));
+			a.logdet[item] = l;
+		}
 	}
 }
 

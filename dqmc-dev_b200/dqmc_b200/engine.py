@@ -185,6 +185,16 @@ class Engine:
         names = self.PROFILE_CLASSES
         return {names[c]: tuple(out[4 * c:4 * c + 4]) for c in range(n_class)}
 
+    def logdet_grad(self):
+        """(logdet per chain, S per chain and spin as N x N arrays): see
+        dqmc_engine_logdet_grad; fields, RNG and sweep counts stay."""
+        n, N = len(self.sims), self.sims[0].N
+        ld = np.zeros(n)
+        S = np.zeros(n * 2 * N * N, dtype=self.sims[0].nt)
+        _lib.check(self.lib.dqmc_engine_logdet_grad(self.h, ld.ctypes.data, S.ctypes.data),
+                   "dqmc_engine_logdet_grad")
+        return ld, S.reshape(n, 2, N, N).transpose(0, 1, 3, 2)
+
     def stream(self) -> int:
         return int(self.lib.dqmc_engine_stream(self.h) or 0)
 

@@ -1,0 +1,159 @@
+"""Gradients of log |det M_up det M_dn| at fixed Hubbard-Stratonovich fields.
+
+For B_l = exp(-dt K) exp(V_l) and M = I + B_{L-1} ... B_0 (one spin),
+
+    d log det M / d theta = sum_l tr[(I - G_l) B_l^-1 dB_l/d theta]
+                          = tr[S D_theta],
+    S = sum_l exp(V_l) (I - G_l) exp(-V_l),
+    D_theta = exp(dt K) d exp(-dt K) / d theta,
+
+with G_l the equal-time Green's function before slice l.  The engine
+accumulates S over one update-free sweep of the stabilised chain
+(dqmc_engine_logdet_grad).  D_theta for every parameter comes from one
+eigen-decomposition K = V diag(k) V^T: in that basis the Frechet derivative
+of exp(-dt K) along E is (V^T E V) * Phi with Phi_ij the divided difference
+of exp at -dt k_i, -dt k_j (computed with expm1).  The contraction over all
+parameters is then a single einsum.
+
+Parameters of the square-lattice model (periodic, as gen.hopping_square):
+theta = [t, t', mu, h_0 ... h_{2N-1}], the nearest-neighbour hopping on bond
+b being t + h_b.  Bonds are numbered as hopping_square adds them: site
+ix + Nx iy, first the x bond to (ix+1, iy), then the y bond to (ix, iy+1).
+So d/dt is the sum of the per-bond derivatives.
+
+LogDet wraps this in a torch.autograd.Function: the forward runs the sweep
+and keeps the per-configuration gradients for the backward.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import gen
+from .engine import Engine, SimData
+
+
+def square_bonds(Nx: int, Ny: int):
+    """(nearest-neighbour bonds, next-nearest pairs) as (i, j) site pairs."""
+    nn, nnn = [], []
+    for iy in range(Ny):
+        for ix in range(Nx):
+            iy1, ix1 = (iy + 1) % Ny, (ix + 1) % Nx
+            i = ix + Nx * iy
+            nn.append((i, ix1 + Nx * iy))
+            nn.append((i, ix + Nx * iy1))
+            nnn.append((i, ix1 + Nx * iy1))
+            nnn.append((ix1 + Nx * iy, ix + Nx * iy1))
+    return nn, nnn
+
+
+class SquareModel:
+    """Fixed fields of `n_cfg` configurations of the square-lattice Hubbard
+    model; evaluate(theta) gives log |det M_up M_dn| and its gradient."""
+
+    def __init__(self, Nx: int, Ny: int, U: float, dt: float, L: int, fields: np.ndarray,
+                 n_matmul: int = 8, device: int = 0):
+        self.Nx, self.Ny, self.N = Nx, Ny, Nx * Ny
+        self.U, self.dt, self.L, self.n_matmul = U, dt, L, n_matmul
+        self.fields = np.ascontiguousarray(np.asarray(fields, dtype=np.int32).reshape(-1, L, self.N))
+        self.n_cfg = self.fields.shape[0]
+        self.device = device
+        self.nn, self.nnn = square_bonds(Nx, Ny)
+        self.n_params = 3 + len(self.nn)
+        N = self.N
+        # dK / d theta_k
+        dK = np.zeros((self.n_params, N, N))
+        for b, (i, j) in enumerate(self.nn):
+            for k in (0, 3 + b):
+                dK[k, i, j] -= 1.0
+                dK[k, j, i] -= 1.0
+        for i, j in self.nnn:
+            dK[1, i, j] -= 1.0
+            dK[1, j, i] -= 1.0
+        dK[2] -= np.eye(N)
+        self.dK = dK
+
+    def K(self, theta: np.ndarray) -> np.ndarray:
+        t, tp, mu, h = theta[0], theta[1], theta[2], theta[3:]
+        N = self.N
+        K = np.zeros((N, N))
+        for b, (i, j) in enumerate(self.nn):
+            K[i, j] -= t + h[b]
+            K[j, i] -= t + h[b]
+        for i, j in self.nnn:
+            K[i, j] -= tp
+            K[j, i] -= tp
+        K -= mu * np.eye(N)
+        return K
+
+    def _sims(self, K: np.ndarray) -> list[SimData]:
+        from scipy.linalg import expm
+        dt = self.dt
+        d0 = gen.make_sim(Nx=self.Nx, Ny=self.Ny, U=self.U, dt=dt, L=self.L,
+                          n_matmul=self.n_matmul, period_eqlt=self.n_matmul, n_sweep_warm=0,
+                          n_sweep_meas=1)
+        mats = {"exp_Ku": expm(-dt * K), "inv_exp_Ku": expm(dt * K),
+                "exp_halfKu": expm(-dt / 2 * K), "inv_exp_halfKu": expm(dt / 2 * K)}
+        for k in list(mats):
+            mats[k.replace("u", "d") if k.endswith("u") else k] = mats[k]
+        for k, v in mats.items():
+            d0["params/" + k] = v
+        d0["params/Ku"], d0["params/Kd"] = K, K.copy()
+        out = []
+        for c in range(self.n_cfg):
+            d = dict(d0)
+            d["state/hs"] = self.fields[c]
+            out.append(SimData(d))
+        return out
+
+    def d_theta(self, K: np.ndarray):
+        """(V, weights) with D_theta = V [(V^T dK_theta V) * weights] V^T:
+        weights_ij = -dt exp(dt k_i) Phi_ij (Phi: divided differences of
+        exp at a = -dt k)."""
+        k, V = np.linalg.eigh(K)
+        a = -self.dt * k
+        da = a[:, None] - a[None, :]
+        with np.errstate(divide="ignore", invalid="ignore"):
+            ratio = np.where(np.abs(da) > 1e-300, np.expm1(da) / da, 1.0)
+        phi = np.exp(a)[None, :] * ratio                  # (e^{a_i} - e^{a_j}) / (a_i - a_j)
+        w = -self.dt * np.exp(-a)[:, None] * phi          # exp(dt k_i) = exp(-a_i)
+        return V, w
+
+    def evaluate(self, theta) -> tuple[np.ndarray, np.ndarray]:
+        """log |det M_up det M_dn| per configuration and its gradient
+        (n_cfg x n_params) at the parameters theta."""
+        theta = np.asarray(theta, dtype=np.float64)
+        K = self.K(theta)
+        sims = self._sims(K)
+        e = Engine(sims, device=self.device)
+        try:
+            ld, S = e.logdet_grad()
+        finally:
+            e.close()
+        V, w = self.d_theta(K)
+        E = np.einsum("ai,kab,bj->kij", V, self.dK, V, optimize=True)    # V^T dK V
+        Sp = np.einsum("ai,csab,bj->cij", V, S, V, optimize=True)        # V^T (S_up + S_dn) V
+        # tr[S D] = sum_ij (V^T S V)_ji w_ij E_ij
+        grad = np.einsum("cji,ij,kij->ck", Sp, w, E, optimize=True)
+        return ld, grad
+
+
+try:
+    import torch
+
+    class LogDet(torch.autograd.Function):
+        """y_c = log |det M_up det M_dn| of configuration c as a function of
+        theta (a float64 tensor); the backward contracts the incoming
+        gradient with the per-configuration gradients of the forward."""
+
+        @staticmethod
+        def forward(ctx, theta, model: SquareModel):
+            ld, grad = model.evaluate(theta.detach().cpu().numpy())
+            ctx.save_for_backward(torch.from_numpy(grad).to(theta.device))
+            return torch.from_numpy(ld).to(theta.device)
+
+        @staticmethod
+        def backward(ctx, g):
+            (grad,) = ctx.saved_tensors
+            return (g[:, None].to(grad.dtype) * grad).sum(0), None
+except ImportError:  # pragma: no cover - torch is part of the environment
+    LogDet = None

@@ -119,6 +119,17 @@ int dqmc_engine_launches_per_sweep(dqmc_engine *e, int meas_eq, int meas_ue);
 int dqmc_engine_profile_sweep(dqmc_engine *e, int meas_eq, int meas_ue, double *out,
 		int n_class);
 
+/* Fixed-field log-determinant and its gradient sums (no counterpart in the
+ * reference, whose sweep only samples).  For every chain: logdet[chain] =
+ * log |det(I + B_{L-1} ... B_0)| summed over both spins, and
+ * S[chain][spin] (N x N, column-major num) = sum_l exp(V_l) (I - G_l)
+ * exp(-V_l) over one sweep without updates, G_l the equal-time Green's
+ * function before slice l.  Then for any parameter theta of the hopping
+ * matrix K_spin, d logdet / d theta = sum_spin tr[S_spin D_theta,spin] with
+ * D_theta = exp(dt K) d exp(-dt K) / d theta.  The chains' fields, RNG
+ * states and sweep counts do not change. */
+int dqmc_engine_logdet_grad(dqmc_engine *e, double *logdet, void *S);
+
 /* ---------------------------------------------------------------------------
  * Kernel-level seams on device pointers, batched over `batch` independent
  * problems laid out back to back.  Each mirrors one reference function.

@@ -1,0 +1,114 @@
+"""Gradients of log |det M_up det M_dn| at fixed fields (dqmc_b200.grad):
+the GPU log-determinant against numpy's slogdet of the explicit space-time
+fermion matrix O (N L x N L: I on the diagonal, -B_l below it, +B_{L-1} in
+the corner, greens.c:247-264 with one slice per block), the gradient against
+the explicit tr[O^-1 dO] and against central differences (h = 1e-5), and
+the torch.autograd.Function's backward."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+LD_RTOL = 1e-10
+GRAD_RTOL = 1e-8      # against the explicit fermion-matrix gradient
+FD_RTOL = 1e-6        # against central differences
+
+
+@pytest.fixture(scope="module")
+def grad():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from dqmc_b200 import grad as G, lib
+    lib.load()
+    return G
+
+
+def _fields(n_cfg, L, N, seed):
+    rng = np.random.default_rng(seed)
+    return rng.integers(0, 2, size=(n_cfg, L, N)).astype(np.int32)
+
+
+def _explicit(model, theta, fields):
+    """log |det O_up O_dn| and its gradient from the explicit fermion matrices"""
+    from scipy.linalg import expm, expm_frechet
+    from dqmc_b200 import gen
+    N, L, dt = model.N, model.L, model.dt
+    K = model.K(theta)
+    eK = expm(-dt * K)
+    dE = [expm_frechet(-dt * K, -dt * model.dK[k])[1] for k in range(model.n_params)]
+    lam = np.exp(0.5 * model.U * dt) + np.sqrt(np.expm1(model.U * dt))
+    el = np.array([1.0 / lam, lam])
+    ld, g = 0.0, np.zeros(model.n_params)
+    for spin in (0, 1):
+        h = fields if spin == 0 else 1 - fields
+        d = el[h]                                   # (L, N)
+        O = np.eye(N * L)
+        for l in range(L):
+            B = eK * d[l][None, :]
+            r, c = ((l + 1) % L) * N, l * N
+            O[r:r + N, c:c + N] += B if l == L - 1 else -B
+        sign, v = np.linalg.slogdet(O)
+        ld += v
+        Oi = np.linalg.inv(O)
+        for k in range(model.n_params):
+            tr = 0.0
+            for l in range(L):
+                dB = dE[k] * d[l][None, :]
+                r, c = ((l + 1) % L) * N, l * N
+                blk = Oi[c:c + N, r:r + N]
+                tr += np.sum(blk.T * (dB if l == L - 1 else -dB))
+            g[k] += tr
+    return ld, g
+
+
+@pytest.mark.parametrize("Nx,L,nmul", [(4, 8, 4), (4, 12, 3)])
+def test_logdet_and_gradient_match_fermion_matrix(grad, Nx, L, nmul):
+    fields = _fields(3, L, Nx * Nx, 5)
+    m = grad.SquareModel(Nx, Nx, U=4.0, dt=0.1, L=L, fields=fields, n_matmul=nmul)
+    rng = np.random.default_rng(1)
+    theta = np.concatenate([[1.0, -0.2, -0.3], 0.05 * rng.standard_normal(2 * Nx * Nx)])
+    ld, g = m.evaluate(theta)
+    for c in range(3):
+        ld_x, g_x = _explicit(m, theta, fields[c])
+        assert abs(ld[c] - ld_x) < LD_RTOL * max(1.0, abs(ld_x))
+        np.testing.assert_allclose(g[c], g_x, rtol=GRAD_RTOL, atol=GRAD_RTOL * np.abs(g_x).max())
+
+
+def test_gradient_matches_central_differences(grad):
+    fields = _fields(2, 8, 16, 7)
+    m = grad.SquareModel(4, 4, U=4.0, dt=0.1, L=8, fields=fields, n_matmul=4)
+    theta = np.concatenate([[1.0, -0.2, -0.3], np.zeros(32)])
+    _, g = m.evaluate(theta)
+    h = 1e-5
+    for k in (0, 1, 2, 3, 17):
+        tp, tm = theta.copy(), theta.copy()
+        tp[k] += h
+        tm[k] -= h
+        fd = (m.evaluate(tp)[0] - m.evaluate(tm)[0]) / (2 * h)
+        np.testing.assert_allclose(g[:, k], fd, rtol=FD_RTOL, atol=FD_RTOL * np.abs(g).max())
+
+
+def test_autograd_function(grad):
+    import torch
+    fields = _fields(4, 8, 16, 9)
+    m = grad.SquareModel(4, 4, U=4.0, dt=0.1, L=8, fields=fields, n_matmul=4)
+    theta = torch.tensor(np.concatenate([[1.0, -0.2, -0.3], np.zeros(32)]), dtype=torch.float64,
+                         requires_grad=True)
+    w = torch.arange(1, 5, dtype=torch.float64)
+    y = grad.LogDet.apply(theta, m)
+    (w * y).sum().backward()
+    _, g = m.evaluate(theta.detach().numpy())
+    np.testing.assert_allclose(theta.grad.numpy(), (w.numpy()[:, None] * g).sum(0), rtol=1e-12)
+
+
+def test_full_size_configuration(grad):
+    """8x8, L = 40 (N L = 2560), t' = -0.2, U = 4, mu = -0.3: one configuration
+    against the explicit fermion-matrix gradient."""
+    fields = _fields(1, 40, 64, 11)
+    m = grad.SquareModel(8, 8, U=4.0, dt=0.1, L=40, fields=fields, n_matmul=8)
+    theta = np.concatenate([[1.0, -0.2, -0.3], np.zeros(128)])
+    ld, g = m.evaluate(theta)
+    ld_x, g_x = _explicit(m, theta, fields[0])
+    assert abs(ld[0] - ld_x) < LD_RTOL * max(1.0, abs(ld_x))
+    np.testing.assert_allclose(g[0], g_x, rtol=GRAD_RTOL, atol=GRAD_RTOL * np.abs(g_x).max())
