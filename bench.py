@@ -289,7 +289,53 @@ def _restream(base, rngs, N, L):
     return out
 
 
-EXTRA = {"ragged64": _ragged64, "complex64": _complex64, "uneq8x8": _uneq8x8}
+EXTRA = {"ragged64": _ragged64, "complex64": _complex64, "uneq8x8": _uneq8x8, "grad128": None}
+
+
+def run_grad(args, rank, world, local):
+    """Gradient evaluations at fixed fields: 128 field configurations
+    (uniform +-1 from the seed) of the 8x8 model, t=1, t'=-0.2, U=4,
+    mu=-0.3, beta=4, dtau=0.1 (L=40).  A step evaluates, for every
+    configuration, log |det M_up M_dn|, <n> and <docc> and their gradients
+    with respect to t, t', mu and the 128 bond hoppings (131 parameters)."""
+    import torch
+    torch.cuda.set_device(local)
+    from dqmc_b200 import grad, replicas
+    n_cfg = 128
+    blk = replicas.shard(n_cfg * world, rank, world)
+    draw = np.random.Generator(np.random.PCG64(SEED + blk.start))
+    fields = draw.integers(0, 2, size=(len(blk), 40, 64)).astype(np.int32)
+    m = grad.SquareModel(8, 8, U=4.0, dt=0.1, L=40, fields=fields, n_matmul=8, device=local)
+    theta = np.concatenate([[1.0, -0.2, -0.3], np.zeros(128)])
+    for _ in range(args.warmup):
+        m.evaluate(theta)
+        m.evaluate_obs(theta)
+    barrier(world)
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            m.evaluate(theta)
+            m.evaluate_obs(theta)
+        torch.cuda.synchronize()
+        t = time.perf_counter() - t0
+    barrier(world)
+    t_max = max_over_ranks(t, world)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "grad evals/s", "value": n_cfg * args.steps * world / t_max,
+            "unit": "grad evals/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "128 fixed HS field configurations, 8x8 square, t=1, t'=-0.2, "
+                                   "U=4, mu=-0.3, beta=4, dtau=0.1 (L=40); one grad eval = "
+                                   "log|det M_up M_dn|, <n>, <docc> and their gradients in t, t', "
+                                   "mu and 128 bond hoppings for one configuration",
+                       "timing": "host clock around the complete evaluations (device sweeps, "
+                                 "space-time Green's functions, host contractions)"},
+            "gpu_launches": None, "e2e": None, "roofline": None,
+            "clocks": clk.summary(), "cpu_baseline": None,
+        }))
 
 
 def run_extra(args, rank, world, local):
@@ -346,7 +392,7 @@ def main():
     args = ap.parse_args()
     rank, world, local = dist_setup(args.gpus)
     if args.impl == "ours" and args.workload != "batch256":
-        run_extra(args, rank, world, local)
+        (run_grad if args.workload == "grad128" else run_extra)(args, rank, world, local)
         if world > 1:
             import torch.distributed as dist
             dist.destroy_process_group()

@@ -465,6 +465,67 @@ __global__ void k_grad_acc(int N, int NB, int L, int l, const T *G, const double
 	}
 }
 
+// O of every item with one slice per block (greens.c:247-264 for
+// n_matmul = 1): identity, -B_e at block (e+1, e), +B_{L-1} at (0, L-1),
+// B_e = exp_K diag(d_e); leading dimension NL, item stride NL^2; O must
+// hold the identity on entry (the corner adds to it when L = 1)
+template <typename T>
+__global__ void k_build_o(int N, int L, int NB, const T *expK, const double *dv, T *O)
+{
+	const long long NN = (long long)N * N, NL = (long long)N * L, tot = NN * L * NB;
+	for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot;
+	     q += (long long)gridDim.x * blockDim.x) {
+		const long long el = q % NN;
+		const int e = (int)((q / NN) % L), b = (int)(q / (NN * L));
+		const int i = (int)(el % N), j = (int)(el / N);
+		const double sg = (e == L - 1) ? 1.0 : -1.0;
+		const T v = expK[(size_t)(b & 1) * NN + el] * (sg * dv[((size_t)b * L + e) * N + j]);
+		T *p = O + (size_t)b * NL * NL + ((e + 1) % L) * (long long)N + i + NL * ((long long)e * N + j);
+		*p = *p + v;
+	}
+}
+
+// diagonal of every item's N L x N L matrix
+template <typename T>
+__global__ void k_diag_of(long long n, int NB, const T *A, T *out)
+{
+	for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n * NB;
+	     q += (long long)gridDim.x * blockDim.x) {
+		const long long r = q % n, b = q / n;
+		out[q] = A[b * n * n + r * (n + 1)];
+	}
+}
+
+// out_b = diag(w_b) A_b for n x n matrices
+template <typename T>
+__global__ void k_rowscale(long long n, int NB, const T *A, const double *w, T *out)
+{
+	for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n * n * NB;
+	     q += (long long)gridDim.x * blockDim.x) {
+		const long long b = q / (n * n), r = (q % (n * n)) % n;
+		out[q] = A[q] * w[b * n + r];
+	}
+}
+
+// Yh_b = sum_m s_m diag(d_m) Y_{b,m}, s_m = +1 (m < L-1), -1 (m = L-1)
+template <typename T>
+__global__ void k_yhat(int N, int L, int NB, const T *Y, const double *dv, T *Yh)
+{
+	const long long NN = (long long)N * N;
+	for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < NN * NB;
+	     q += (long long)gridDim.x * blockDim.x) {
+		const int b = (int)(q / NN);
+		const long long el = q % NN;
+		const int i = (int)(el % N);
+		T s = zero<T>();
+		for (int m = 0; m < L; m++) {
+			const double f = dv[((size_t)b * L + m) * N + i] * (m == L - 1 ? -1.0 : 1.0);
+			s = s + Y[((size_t)b * L + m) * NN + el] * f;
+		}
+		Yh[q] = s;
+	}
+}
+
 // The dynamic shared-memory limit of a kernel is one setting per function,
 // shared by every engine of the process: only ever raise it, so that a group
 // created later with smaller needs cannot shrink it below what an earlier
@@ -505,6 +566,7 @@ struct GroupBase {
 	virtual int launches(int meq, int mue) = 0;
 	virtual int profile(int meq, int mue, double *out, int ncls) = 0;
 	virtual int logdet_grad(double *logdet, void *S) = 0;
+	virtual int obs_grad(double *obs, void *Z) = 0;
 };
 
 template <typename T>
@@ -650,6 +712,9 @@ struct Group : GroupBase, ProfHook {
 	              int sw) override
 	{
 		if (c < 0 || c >= C) return DQMC_E_ARG;
+		// the copies below run on the legacy default stream: queued sweeps
+		// that still read these buffers must finish first
+		CK(cudaStreamSynchronize(st));
 		CK(cudaMemcpy(el.p + (size_t)c * 2 * N, e, sizeof(double) * 2 * N, cudaMemcpyHostToDevice));
 		CK(cudaMemcpy(del.p + (size_t)c * 2 * N, d, sizeof(double) * 2 * N, cudaMemcpyHostToDevice));
 		CK(cudaMemcpy(rng.p + (size_t)c * 17, r, sizeof(uint64_t) * 17, cudaMemcpyHostToDevice));
@@ -662,6 +727,7 @@ struct Group : GroupBase, ProfHook {
 
 	int set_acc(int c, int eqn, const void *eq, int uen, const void *uea) override
 	{
+		CK(cudaStreamSynchronize(st));
 		if (c < 0 || c >= C) return DQMC_E_ARG;
 		CK(cudaMemcpy(n_eq.p + c, &eqn, sizeof(int), cudaMemcpyHostToDevice));
 		if (eq) CK(cudaMemcpy(acc_eq.p + (size_t)c * eq_size, eq, sizeof(T) * eq_size, cudaMemcpyHostToDevice));
@@ -856,6 +922,73 @@ struct Group : GroupBase, ProfHook {
 		return DQMC_E_ARG;
 	}
 
+	// bsofi (greens.c:266-337) of NB block-cyclic matrices of E x E blocks
+	// of N x N: O (leading dimension NE = N E, item stride NE^2) is
+	// overwritten by R and O^-1 goes to Gr.  Work: Qh NB x max(E-1,1) x 4N^2,
+	// Tw NB x E x N^2, Rw NB x NE x 2N.
+	int bsofi(int E, T *O, T *Gr, T *Qh, T *Tw, T *Rw)
+	{
+		const size_t NN = (size_t)N * N;
+		const int NE = N * E;
+		const long long NE2 = (long long)NE * NE, q4 = 4LL * (long long)NN;
+		const long long qstride = (long long)std::max(E - 1, 1) * q4;
+		// bsofi (greens.c:266-337): QR of the 2N x N panels, Q^H carried to
+		// the block columns l+1 and E-1 in the same kernel
+		for (int l = 0; l + 2 < E; l++) {
+			HqrArgs<T> h;
+			memset(&h, 0, sizeof(h));
+			h.M = 2 * N; h.n = N; h.batch = NB;
+			h.A = O + (size_t)l * N * (1 + NE); h.aA = per_item(NE2); h.lda = NE;
+			h.nx1 = N;
+			h.nx2 = N; h.X = O + (size_t)l * N + (size_t)(E - 1) * N * NE; h.aX = per_item(NE2);
+			h.Qh = Qh + (size_t)l * q4; h.aQ = per_item(qstride);
+			h.err = err.p;
+			if (launch_hqr(h)) return DQMC_E_ARG;
+		}
+		const int lf = std::max(E - 2, 0), wf = (E >= 2) ? 2 * N : N;
+		{
+			HqrArgs<T> h;
+			memset(&h, 0, sizeof(h));
+			h.M = wf; h.n = wf; h.batch = NB;
+			h.A = O + (size_t)lf * N * (1 + NE); h.aA = per_item(NE2); h.lda = NE;
+			h.Qh = Qh + (size_t)lf * q4; h.aQ = per_item(qstride);
+			h.err = err.p;
+			if (launch_hqr(h)) return DQMC_E_ARG;
+		}
+		// R^-1: diagonal blocks, then the blocks d above the diagonal,
+		// X(i, i+d) = -X(i, i) R(i, i+1..i+d) X(i+1..i+d, i+d)
+		CK(cudaMemsetAsync(Gr, 0, sizeof(T) * NB * NE2, st));
+		{
+			TriArgs<T> t{N, NE, E, NB, O, Gr, err.p};
+			const size_t sm = trtri_smem_bytes<T>(N);
+			CK(raise_smem(k_trtri<T>, sm));
+			prof_begin(0);
+			k_trtri<T><<<NB * E, 256, sm, st>>>(t);
+			launch_count++;
+			prof_end(PC_UNEQ, 0.0, 0.0);
+		}
+		for (int d = 1; d < E; d++) {
+			const int na = E - d;
+			const Addr dg{NE2, (long long)N * (1 + NE), na};
+			gemm(gargs<T>(N, N, d * N, NB * na, O + (size_t)N * NE, dg, NE,
+			              Gr + N + (size_t)d * N * NE, dg, NE, Tw, per_item((long long)NN), N));
+			gemm(gargs<T>(N, N, N, NB * na, Gr, dg, NE, Tw, per_item((long long)NN), N,
+			              Gr + (size_t)d * N * NE, dg, NE, from_re<T>(-1.0), zero<T>()));
+		}
+		// O^-1 = R^-1 Q_{E-2}^H ... Q_0^H, each on its two block columns
+		for (int l = lf; l >= 0; l--) {
+			T *cols = Gr + (size_t)l * N * NE;
+			prof_begin(0);
+			k_copy2d<T><<<grid_for((long long)NB * NE * wf), 256, 0, st>>>(NE, wf, NB, cols, NE2, NE,
+			        Rw, (long long)NE * wf, NE, one<T>());
+			launch_count++;
+			prof_end(PC_UNEQ, 0.0, 0.0);
+			gemm(gargs<T>(NE, wf, wf, NB, Rw, per_item((long long)NE * wf), NE,
+			              Qh + (size_t)l * q4, per_item(qstride), wf, cols, per_item(NE2), NE));
+		}
+		return 0;
+	}
+
 	// G(0,t), G(t,t), G(t,0) of every slice from this sweep's clusters
 	// (calc_ue_g, greens.c:471-494, with N_MUL = 2 as dqmc.c:399 calls it)
 	int calc_ue_g()
@@ -892,59 +1025,9 @@ struct Group : GroupBase, ProfHook {
 		k_add_diag<T><<<grid_for((long long)NE * NB), 256, 0, st>>>(NE, NB, ue.O.p, NE2);
 		launch_count++;
 		prof_end(PC_UNEQ, 0.0, 0.0);
-		// bsofi (greens.c:266-337): QR of the 2N x N panels, Q^H carried to
-		// the block columns l+1 and E-1 in the same kernel
-		for (int l = 0; l + 2 < E; l++) {
-			HqrArgs<T> h;
-			memset(&h, 0, sizeof(h));
-			h.M = 2 * N; h.n = N; h.batch = NB;
-			h.A = ue.O.p + (size_t)l * N * (1 + NE); h.aA = per_item(NE2); h.lda = NE;
-			h.nx1 = N;
-			h.nx2 = N; h.X = ue.O.p + (size_t)l * N + (size_t)(E - 1) * N * NE; h.aX = per_item(NE2);
-			h.Qh = ue.Qh.p + (size_t)l * q4; h.aQ = per_item(qstride);
-			h.err = err.p;
-			if (launch_hqr(h)) return DQMC_E_ARG;
-		}
-		const int lf = std::max(E - 2, 0), wf = (E >= 2) ? 2 * N : N;
 		{
-			HqrArgs<T> h;
-			memset(&h, 0, sizeof(h));
-			h.M = wf; h.n = wf; h.batch = NB;
-			h.A = ue.O.p + (size_t)lf * N * (1 + NE); h.aA = per_item(NE2); h.lda = NE;
-			h.Qh = ue.Qh.p + (size_t)lf * q4; h.aQ = per_item(qstride);
-			h.err = err.p;
-			if (launch_hqr(h)) return DQMC_E_ARG;
-		}
-		// R^-1: diagonal blocks, then the blocks d above the diagonal,
-		// X(i, i+d) = -X(i, i) R(i, i+1..i+d) X(i+1..i+d, i+d)
-		CK(cudaMemsetAsync(ue.Gr.p, 0, sizeof(T) * NB * NE2, st));
-		{
-			TriArgs<T> t{N, NE, E, NB, ue.O.p, ue.Gr.p, err.p};
-			const size_t sm = trtri_smem_bytes<T>(N);
-			CK(raise_smem(k_trtri<T>, sm));
-			prof_begin(0);
-			k_trtri<T><<<NB * E, 256, sm, st>>>(t);
-			launch_count++;
-			prof_end(PC_UNEQ, 0.0, 0.0);
-		}
-		for (int d = 1; d < E; d++) {
-			const int na = E - d;
-			const Addr dg{NE2, (long long)N * (1 + NE), na};
-			gemm(gargs<T>(N, N, d * N, NB * na, ue.O.p + (size_t)N * NE, dg, NE,
-			              ue.Gr.p + N + (size_t)d * N * NE, dg, NE, ue.Tw.p, per_item((long long)NN), N));
-			gemm(gargs<T>(N, N, N, NB * na, ue.Gr.p, dg, NE, ue.Tw.p, per_item((long long)NN), N,
-			              ue.Gr.p + (size_t)d * N * NE, dg, NE, from_re<T>(-1.0), zero<T>()));
-		}
-		// O^-1 = R^-1 Q_{E-2}^H ... Q_0^H, each on its two block columns
-		for (int l = lf; l >= 0; l--) {
-			T *cols = ue.Gr.p + (size_t)l * N * NE;
-			prof_begin(0);
-			k_copy2d<T><<<grid_for((long long)NB * NE * wf), 256, 0, st>>>(NE, wf, NB, cols, NE2, NE,
-			        ue.Rw.p, (long long)NE * wf, NE, one<T>());
-			launch_count++;
-			prof_end(PC_UNEQ, 0.0, 0.0);
-			gemm(gargs<T>(NE, wf, wf, NB, ue.Rw.p, per_item((long long)NE * wf), NE,
-			              ue.Qh.p + (size_t)l * q4, per_item(qstride), wf, cols, per_item(NE2), NE));
+			const int rc = bsofi(E, ue.O.p, ue.Gr.p, ue.Qh.p, ue.Tw.p, ue.Rw.p);
+			if (rc) return rc;
 		}
 		// expand_g (greens.c:339-469)
 		prof_begin(0);
@@ -1161,7 +1244,10 @@ struct Group : GroupBase, ProfHook {
 			const int rc = init();
 			if (rc) return rc;
 		}
-		if (!Sg.p && Sg.alloc(NB * NN)) return DQMC_E_NOMEM;
+		if (!Sg.p) {
+			if (Sg.alloc(NB * NN)) return DQMC_E_NOMEM;
+			CK(cudaDeviceSynchronize());   // its zeroing ran on the default stream
+		}
 		CK(cudaMemsetAsync(Sg.p, 0, sizeof(T) * NB * NN, st));
 		for (int l = 0; l < L; l++) {
 			k_grad_acc<T><<<grid_for((long long)NB * NN), 256, 0, st>>>(N, NB, L, l, G.p, dv.p, dvi.p, Sg.p);
@@ -1178,6 +1264,88 @@ struct Group : GroupBase, ProfHook {
 		CK(cudaMemcpy(ld.data(), ldet.p, sizeof(double) * NB, cudaMemcpyDeviceToHost));
 		for (int c = 0; c < C; c++) if (ld_out) ld_out[c] = ld[2 * c] + ld[2 * c + 1];
 		if (S_out) CK(cudaMemcpy(S_out, Sg.p, sizeof(T) * NB * NN, cudaMemcpyDeviceToHost));
+		return sync();
+	}
+
+	// Density and double occupancy of the fixed fields, averaged over the L
+	// slices, and for each the matrices Z (per spin) with d obs / d theta =
+	// sum_spin tr[Z D_theta]: Z = sum_m s_m exp(V_m) Y_m exp(-dt K),
+	// Y_m = sum_l Gst(m, l) W_l Gst(l, m+1), Gst = O^-1 the space-time Green's
+	// function (bsofi with one slice per block) and W_l the observable's
+	// weights at slice l.  obs[chain][2], Z[chain][obs][spin][N*N].
+	int obs_grad(double *obs_out, void *Z_out) override
+	{
+		const size_t NN = (size_t)N * N, NL = (size_t)N * L, NL2 = NL * NL;
+		if (need_init) {
+			const int rc = init();
+			if (rc) return rc;
+		}
+		DevBuf<T> O, Gr, Qh, Tw, Rw, Yh, Zb, dg;
+		DevBuf<double> wb;
+		int rc = 0;
+		rc |= O.alloc(NB * NL2); rc |= Gr.alloc(NB * NL2);
+		rc |= Qh.alloc((size_t)NB * std::max(L - 1, 1) * 4 * NN); rc |= Tw.alloc((size_t)NB * L * NN);
+		rc |= Rw.alloc((size_t)NB * NL * 2 * N); rc |= Yh.alloc(NB * NN); rc |= Zb.alloc(NB * NN);
+		rc |= dg.alloc(NB * NL); rc |= wb.alloc(NB * NL);
+		auto release = [&]() {
+			DevBuf<T> *b[] = {&O, &Gr, &Qh, &Tw, &Rw, &Yh, &Zb, &dg};
+			for (auto *x : b) x->release();
+			wb.release();
+		};
+		if (rc) { release(); return DQMC_E_NOMEM; }
+		// the buffers are zeroed on the legacy default stream, which the
+		// engine's non-blocking stream does not wait for
+		CK(cudaDeviceSynchronize());
+		CK(cudaMemsetAsync(O.p, 0, sizeof(T) * NB * NL2, st));
+		k_add_diag<T><<<grid_for((long long)NL * NB), 256, 0, st>>>((int)NL, NB, O.p, (long long)NL2);
+		k_build_o<T><<<grid_for((long long)NN * L * NB), 256, 0, st>>>(N, L, NB, expK.p, dv.p, O.p);
+		rc = bsofi(L, O.p, Gr.p, Qh.p, Tw.p, Rw.p);
+		if (rc) { release(); return rc; }
+		k_diag_of<T><<<grid_for((long long)NL * NB), 256, 0, st>>>((long long)NL, NB, Gr.p, dg.p);
+		std::vector<T> hd(NB * NL);
+		CK(cudaMemcpyAsync(hd.data(), dg.p, sizeof(T) * NB * NL, cudaMemcpyDeviceToHost, st));
+		CK(cudaStreamSynchronize(st));
+		const double inv = 1.0 / (double)NL;
+		for (int c = 0; c < C; c++) {
+			double n = 0.0, d2 = 0.0;
+			for (size_t r = 0; r < NL; r++) {
+				const double nu = 1.0 - re(hd[(2 * c) * NL + r]), nd = 1.0 - re(hd[(2 * c + 1) * NL + r]);
+				n += nu + nd;
+				d2 += nu * nd;
+			}
+			if (obs_out) { obs_out[2 * c] = n * inv; obs_out[2 * c + 1] = d2 * inv; }
+		}
+		std::vector<double> w(NB * NL);
+		for (int o = 0; o < 2; o++) {
+			for (int b = 0; b < NB; b++)
+				for (size_t r = 0; r < NL; r++)
+					w[b * NL + r] = o == 0 ? -inv : -inv * (1.0 - re(hd[(b ^ 1) * NL + r]));
+			// stream-ordered after the previous observable's use of wb
+			CK(cudaMemcpyAsync(wb.p, w.data(), sizeof(double) * NB * NL, cudaMemcpyHostToDevice, st));
+			k_rowscale<T><<<grid_for((long long)NL2 * NB), 256, 0, st>>>((long long)NL, NB, Gr.p, wb.p, O.p);
+			// Y_m = Gst(m-row) (W Gst)((m+1)-column): m < L-1 at once, then m = L-1
+			if (L > 1)
+				gemm(gargs<T>(N, N, (int)NL, NB * (L - 1), Gr.p, Addr{(long long)NL2, (long long)N, L - 1},
+				              (int)NL, O.p + N * NL, Addr{(long long)NL2, (long long)(N * NL), L - 1}, (int)NL,
+				              Tw.p, Addr{(long long)(L * NN), (long long)NN, L - 1}, N));
+			gemm(gargs<T>(N, N, (int)NL, NB, Gr.p + (size_t)(L - 1) * N, per_item((long long)NL2), (int)NL,
+			              O.p, per_item((long long)NL2), (int)NL, Tw.p + (size_t)(L - 1) * NN,
+			              per_item((long long)(L * NN)), N));
+			k_yhat<T><<<grid_for((long long)NN * NB), 256, 0, st>>>(N, L, NB, Tw.p, dv.p, Yh.p);
+			gemm(gargs<T>(N, N, N, NB, Yh.p, per_item((long long)NN), N, expK.p, per_spin((long long)NN), N,
+			              Zb.p, per_item((long long)NN), N));
+			std::vector<T> hz(NB * NN);
+			CK(cudaMemcpyAsync(hz.data(), Zb.p, sizeof(T) * NB * NN, cudaMemcpyDeviceToHost, st));
+			CK(cudaStreamSynchronize(st));
+			if (Z_out)
+				for (int c = 0; c < C; c++)
+					for (int sp = 0; sp < 2; sp++)
+						memcpy((T *)Z_out + ((size_t)(c * 2 + o) * 2 + sp) * NN, hz.data() + (2 * c + sp) * NN,
+						       sizeof(T) * NN);
+		}
+		CK(cudaStreamSynchronize(st));
+		CK(cudaGetLastError());
+		release();
 		return sync();
 	}
 
@@ -1365,6 +1533,11 @@ int dqmc_engine_launches_per_sweep(dqmc_engine *e, int meas_eq, int meas_ue)
 int dqmc_engine_logdet_grad(dqmc_engine *e, double *logdet, void *S)
 {
 	return e ? e->g->logdet_grad(logdet, S) : DQMC_E_ARG;
+}
+
+int dqmc_engine_obs_grad(dqmc_engine *e, double *obs, void *Z)
+{
+	return e ? e->g->obs_grad(obs, Z) : DQMC_E_ARG;
 }
 
 int dqmc_engine_profile_sweep(dqmc_engine *e, int meas_eq, int meas_ue, double *out, int n_class)

@@ -195,6 +195,16 @@ class Engine:
                    "dqmc_engine_logdet_grad")
         return ld, S.reshape(n, 2, N, N).transpose(0, 1, 3, 2)
 
+    def obs_grad(self):
+        """(obs per chain [n, docc], Z per chain, observable and spin as N x N
+        arrays): see dqmc_engine_obs_grad."""
+        n, N = len(self.sims), self.sims[0].N
+        obs = np.zeros(2 * n)
+        Z = np.zeros(n * 4 * N * N, dtype=self.sims[0].nt)
+        _lib.check(self.lib.dqmc_engine_obs_grad(self.h, obs.ctypes.data, Z.ctypes.data),
+                   "dqmc_engine_obs_grad")
+        return obs.reshape(n, 2), Z.reshape(n, 2, 2, N, N).transpose(0, 1, 2, 4, 3)
+
     def stream(self) -> int:
         return int(self.lib.dqmc_engine_stream(self.h) or 0)
 

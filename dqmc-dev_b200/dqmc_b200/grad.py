@@ -21,8 +21,14 @@ b being t + h_b.  Bonds are numbered as hopping_square adds them: site
 ix + Nx iy, first the x bond to (ix+1, iy), then the y bond to (ix, iy+1).
 So d/dt is the sum of the per-bond derivatives.
 
-LogDet wraps this in a torch.autograd.Function: the forward runs the sweep
-and keeps the per-configuration gradients for the backward.
+The same contraction gives the derivatives of the fixed-field density and
+double occupancy (evaluate_obs): with Gst = O^-1 the space-time Green's
+function, d <X> = sum_l tr[W_l dGst(l, l)] and dGst = -Gst dO Gst collapse to
+tr[Z D_theta] with Z = sum_m s_m exp(V_m) Y_m exp(-dt K) and
+Y_m = sum_l Gst(m, l) W_l Gst(l, m+1) (W_l the observable's weights).
+
+LogDet wraps the log-determinant in a torch.autograd.Function: the forward
+runs the sweep and keeps the per-configuration gradients for the backward.
 """
 from __future__ import annotations
 
@@ -135,6 +141,24 @@ class SquareModel:
         # tr[S D] = sum_ij (V^T S V)_ji w_ij E_ij
         grad = np.einsum("cji,ij,kij->ck", Sp, w, E, optimize=True)
         return ld, grad
+
+
+    def evaluate_obs(self, theta) -> tuple[np.ndarray, np.ndarray]:
+        """(obs, grad): obs[c] = (<n>, <docc>) of configuration c averaged
+        over the slices, grad[c, o, k] = d obs[c, o] / d theta_k, from the
+        space-time Green's function (dqmc_engine_obs_grad)."""
+        theta = np.asarray(theta, dtype=np.float64)
+        K = self.K(theta)
+        sims = self._sims(K)
+        e = Engine(sims, device=self.device)
+        try:
+            obs, Z = e.obs_grad()
+        finally:
+            e.close()
+        V, w = self.d_theta(K)
+        E = np.einsum("ai,kab,bj->kij", V, self.dK, V, optimize=True)
+        Zp = np.einsum("ai,cosab,bj->coij", V, Z, V, optimize=True)
+        return obs, np.einsum("coji,ij,kij->cok", Zp, w, E, optimize=True)
 
 
 try:

@@ -130,6 +130,19 @@ int dqmc_engine_profile_sweep(dqmc_engine *e, int meas_eq, int meas_ue, double *
  * states and sweep counts do not change. */
 int dqmc_engine_logdet_grad(dqmc_engine *e, double *logdet, void *S);
 
+/* Fixed-field density and double occupancy (no counterpart in the
+ * reference), each averaged over the L slices of the chain's own fields:
+ * obs[chain][0] = <n> = sum_spin sum_l sum_i (1 - G_l,ii) / (N L),
+ * obs[chain][1] = <docc> = sum_l sum_i (1 - Gup_l,ii)(1 - Gdn_l,ii) / (N L),
+ * and Z[chain][obs][spin] (N x N, column-major num) with
+ * d obs / d theta = sum_spin tr[Z_spin D_theta], D_theta as for
+ * dqmc_engine_logdet_grad.  Z comes from the space-time Green's function
+ * O^-1 (bsofi with one slice per block): Z = sum_m s_m exp(V_m) Y_m
+ * exp(-dt K), Y_m = sum_l O^-1(m, l) W_l O^-1(l, m+1), s_m = -1 for the
+ * corner block m = L-1 and +1 otherwise.  Needs 2 (N L)^2 nums of device
+ * memory per chain and spin for the duration of the call. */
+int dqmc_engine_obs_grad(dqmc_engine *e, double *obs, void *Z);
+
 /* ---------------------------------------------------------------------------
  * Kernel-level seams on device pointers, batched over `batch` independent
  * problems laid out back to back.  Each mirrors one reference function.

@@ -112,3 +112,67 @@ def test_full_size_configuration(grad):
     ld_x, g_x = _explicit(m, theta, fields[0])
     assert abs(ld[0] - ld_x) < LD_RTOL * max(1.0, abs(ld_x))
     np.testing.assert_allclose(g[0], g_x, rtol=GRAD_RTOL, atol=GRAD_RTOL * np.abs(g_x).max())
+
+
+def _explicit_obs(model, theta, fields):
+    """<n>, <docc> and their gradients from the explicit space-time Green's
+    functions Gst = O^-1 of both spins: dGst = -Gst dO Gst"""
+    from scipy.linalg import expm, expm_frechet
+    N, L, dt = model.N, model.L, model.dt
+    K = model.K(theta)
+    eK = expm(-dt * K)
+    dE = [expm_frechet(-dt * K, -dt * model.dK[k])[1] for k in range(model.n_params)]
+    lam = np.exp(0.5 * model.U * dt) + np.sqrt(np.expm1(model.U * dt))
+    el = np.array([1.0 / lam, lam])
+    G, dG = [], []
+    for spin in (0, 1):
+        d = el[fields if spin == 0 else 1 - fields]
+        O = np.eye(N * L)
+        for l in range(L):
+            r, c = ((l + 1) % L) * N, l * N
+            O[r:r + N, c:c + N] += (1 if l == L - 1 else -1) * (eK * d[l][None, :])
+        Gi = np.linalg.inv(O)
+        G.append(np.diag(Gi).copy())
+        dd = []
+        for k in range(model.n_params):
+            dO = np.zeros_like(O)
+            for l in range(L):
+                r, c = ((l + 1) % L) * N, l * N
+                dO[r:r + N, c:c + N] = (1 if l == L - 1 else -1) * (dE[k] * d[l][None, :])
+            dd.append(-np.einsum("ij,jk,ki->i", Gi, dO, Gi))
+        dG.append(np.array(dd))
+    NL = N * L
+    n = ((1 - G[0]) + (1 - G[1])).sum() / NL
+    docc = ((1 - G[0]) * (1 - G[1])).sum() / NL
+    gn = -(dG[0] + dG[1]).sum(1) / NL
+    gd = (-(dG[0] * (1 - G[1])[None, :]) - ((1 - G[0])[None, :] * dG[1])).sum(1) / NL
+    return np.array([n, docc]), np.array([gn, gd])
+
+
+@pytest.mark.parametrize("Nx,L,nmul", [(4, 8, 4), (4, 6, 3)])
+def test_observable_gradients_match_fermion_matrix(grad, Nx, L, nmul):
+    fields = _fields(2, L, Nx * Nx, 21)
+    m = grad.SquareModel(Nx, Nx, U=4.0, dt=0.1, L=L, fields=fields, n_matmul=nmul)
+    rng = np.random.default_rng(3)
+    theta = np.concatenate([[1.0, -0.2, -0.3], 0.05 * rng.standard_normal(2 * Nx * Nx)])
+    obs, g = m.evaluate_obs(theta)
+    for c in range(2):
+        ox, gx = _explicit_obs(m, theta, fields[c])
+        np.testing.assert_allclose(obs[c], ox, rtol=1e-10)
+        for o in range(2):
+            np.testing.assert_allclose(g[c, o], gx[o], rtol=GRAD_RTOL,
+                                       atol=GRAD_RTOL * np.abs(gx[o]).max())
+
+
+def test_observable_gradients_match_central_differences(grad):
+    fields = _fields(1, 8, 16, 23)
+    m = grad.SquareModel(4, 4, U=4.0, dt=0.1, L=8, fields=fields, n_matmul=4)
+    theta = np.concatenate([[1.0, -0.2, -0.3], np.zeros(32)])
+    _, g = m.evaluate_obs(theta)
+    h = 1e-5
+    for k in (0, 1, 2, 9):
+        tp, tm = theta.copy(), theta.copy()
+        tp[k] += h
+        tm[k] -= h
+        fd = (m.evaluate_obs(tp)[0] - m.evaluate_obs(tm)[0]) / (2 * h)
+        np.testing.assert_allclose(g[:, :, k], fd, rtol=FD_RTOL, atol=FD_RTOL * np.abs(g).max())
