@@ -321,6 +321,22 @@ def run_grad(args, rank, world, local):
         t = time.perf_counter() - t0
     barrier(world)
     t_max = max_over_ranks(t, world)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # the explicit fermion-matrix method on the host: one configuration
+        # (two 2560 x 2560 inverses per quantity), scaled to grad evals/s
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import fermion_matrix as fm
+        K = m.K(theta)
+        t0 = time.perf_counter()
+        fm.logdet_grad(K, m.dK, m.U, m.dt, m.L, fields[0])
+        fm.obs_grad(K, m.dK, m.U, m.dt, m.L, fields[0])
+        tc = time.perf_counter() - t0
+        cpu = {"value": 1.0 / tc, "unit": "grad evals/s",
+               "cores": os.cpu_count() or 1, "kind": "port",
+               "sample": f"one configuration with the explicit N L x N L fermion matrices "
+                         f"(numpy/OpenBLAS, {os.cpu_count()} host threads): log-det, <n>, "
+                         f"<docc> and their 131-parameter gradients, {tc:.1f} s"}
     if rank == 0:
         print(json.dumps({
             "metric": "grad evals/s", "value": n_cfg * args.steps * world / t_max,
@@ -334,7 +350,7 @@ def run_grad(args, rank, world, local):
                        "timing": "host clock around the complete evaluations (device sweeps, "
                                  "space-time Green's functions, host contractions)"},
             "gpu_launches": None, "e2e": None, "roofline": None,
-            "clocks": clk.summary(), "cpu_baseline": None,
+            "clocks": clk.summary(), "cpu_baseline": cpu,
         }))
 
 

@@ -31,35 +31,8 @@ def _fields(n_cfg, L, N, seed):
 
 def _explicit(model, theta, fields):
     """log |det O_up O_dn| and its gradient from the explicit fermion matrices"""
-    from scipy.linalg import expm, expm_frechet
-    from dqmc_b200 import gen
-    N, L, dt = model.N, model.L, model.dt
-    K = model.K(theta)
-    eK = expm(-dt * K)
-    dE = [expm_frechet(-dt * K, -dt * model.dK[k])[1] for k in range(model.n_params)]
-    lam = np.exp(0.5 * model.U * dt) + np.sqrt(np.expm1(model.U * dt))
-    el = np.array([1.0 / lam, lam])
-    ld, g = 0.0, np.zeros(model.n_params)
-    for spin in (0, 1):
-        h = fields if spin == 0 else 1 - fields
-        d = el[h]                                   # (L, N)
-        O = np.eye(N * L)
-        for l in range(L):
-            B = eK * d[l][None, :]
-            r, c = ((l + 1) % L) * N, l * N
-            O[r:r + N, c:c + N] += B if l == L - 1 else -B
-        sign, v = np.linalg.slogdet(O)
-        ld += v
-        Oi = np.linalg.inv(O)
-        for k in range(model.n_params):
-            tr = 0.0
-            for l in range(L):
-                dB = dE[k] * d[l][None, :]
-                r, c = ((l + 1) % L) * N, l * N
-                blk = Oi[c:c + N, r:r + N]
-                tr += np.sum(blk.T * (dB if l == L - 1 else -dB))
-            g[k] += tr
-    return ld, g
+    import fermion_matrix as fm
+    return fm.logdet_grad(model.K(theta), model.dK, model.U, model.dt, model.L, fields)
 
 
 @pytest.mark.parametrize("Nx,L,nmul", [(4, 8, 4), (4, 12, 3)])
@@ -116,37 +89,9 @@ def test_full_size_configuration(grad):
 
 def _explicit_obs(model, theta, fields):
     """<n>, <docc> and their gradients from the explicit space-time Green's
-    functions Gst = O^-1 of both spins: dGst = -Gst dO Gst"""
-    from scipy.linalg import expm, expm_frechet
-    N, L, dt = model.N, model.L, model.dt
-    K = model.K(theta)
-    eK = expm(-dt * K)
-    dE = [expm_frechet(-dt * K, -dt * model.dK[k])[1] for k in range(model.n_params)]
-    lam = np.exp(0.5 * model.U * dt) + np.sqrt(np.expm1(model.U * dt))
-    el = np.array([1.0 / lam, lam])
-    G, dG = [], []
-    for spin in (0, 1):
-        d = el[fields if spin == 0 else 1 - fields]
-        O = np.eye(N * L)
-        for l in range(L):
-            r, c = ((l + 1) % L) * N, l * N
-            O[r:r + N, c:c + N] += (1 if l == L - 1 else -1) * (eK * d[l][None, :])
-        Gi = np.linalg.inv(O)
-        G.append(np.diag(Gi).copy())
-        dd = []
-        for k in range(model.n_params):
-            dO = np.zeros_like(O)
-            for l in range(L):
-                r, c = ((l + 1) % L) * N, l * N
-                dO[r:r + N, c:c + N] = (1 if l == L - 1 else -1) * (dE[k] * d[l][None, :])
-            dd.append(-np.einsum("ij,jk,ki->i", Gi, dO, Gi))
-        dG.append(np.array(dd))
-    NL = N * L
-    n = ((1 - G[0]) + (1 - G[1])).sum() / NL
-    docc = ((1 - G[0]) * (1 - G[1])).sum() / NL
-    gn = -(dG[0] + dG[1]).sum(1) / NL
-    gd = (-(dG[0] * (1 - G[1])[None, :]) - ((1 - G[0])[None, :] * dG[1])).sum(1) / NL
-    return np.array([n, docc]), np.array([gn, gd])
+    functions of both spins"""
+    import fermion_matrix as fm
+    return fm.obs_grad(model.K(theta), model.dK, model.U, model.dt, model.L, fields)
 
 
 @pytest.mark.parametrize("Nx,L,nmul", [(4, 8, 4), (4, 6, 3)])
