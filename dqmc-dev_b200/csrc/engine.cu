@@ -260,6 +260,8 @@ struct EqWork {
 	T *G; long long g_stride;          // output
 	T *phi;                            // NB output phases
 	double *logdet;                    // NB, optional: log |det(I + C...C)|
+	const T *Pr; long long pr_stride;  // optional cache of the pair products
+	                                   // C_{(m+1)%F} C_m at Pr + b*pr_stride + m*N*N
 	unsigned *err;
 };
 
@@ -327,7 +329,9 @@ static int run_calc_eq_g(const EqWork<T> &w, int l0, cudaStream_t st, int *count
 	q.pvt = w.pvt; q.p_stride = N;
 	q.work = w.W; q.w_stride = NN;     // free while a QR runs
 	const int first = (F == 1) ? 1 : ((F - 1) % 2 == 1 ? 2 : 1);
-	if (first == 2) {
+	if (first == 2 && w.Pr) {
+		q.X = w.Pr + (size_t)l0 * NN; q.x_stride = w.pr_stride;
+	} else if (first == 2) {
 		eq_gemm(gargs<T>(N, N, N, NB, clu(l0 + 1), aCl, N, clu(l0), aCl, N, w.X, aI, N), st, count, ph);
 		q.X = w.X; q.x_stride = NN;
 	} else {
@@ -343,8 +347,13 @@ static int run_calc_eq_g(const EqWork<T> &w, int l0, cudaStream_t st, int *count
 	T *Tc = w.Tm, *Tn = w.Tm2;
 	while (m != l0) {
 		const int next = (m + 2) % F;
-		eq_gemm(gargs<T>(N, N, N, NB, clu(m + 1), aCl, N, clu(m), aCl, N, w.W, aI, N), st, count, ph);
-		eq_gemm(gargs<T>(N, N, N, NB, w.W, aI, N, w.Qm, aI, N, w.X, aI, N), st, count, ph);
+		if (w.Pr) {
+			eq_gemm(gargs<T>(N, N, N, NB, w.Pr + (size_t)m * NN, Addr{w.pr_stride, 0, 1}, N, w.Qm, aI, N,
+			                 w.X, aI, N), st, count, ph);
+		} else {
+			eq_gemm(gargs<T>(N, N, N, NB, clu(m + 1), aCl, N, clu(m), aCl, N, w.W, aI, N), st, count, ph);
+			eq_gemm(gargs<T>(N, N, N, NB, w.W, aI, N, w.Qm, aI, N, w.X, aI, N), st, count, ph);
+		}
 		m = next;
 		QrArgs<T> r = q;
 		r.mode = QR_PRESORT;
@@ -617,6 +626,7 @@ struct Group : GroupBase, ProfHook {
 	bool need_init = true;     // G must be recomputed from the fields before sweeping
 	DevBuf<T> phase, G, Cl, Qm, Tm, Tm2, Rs, X, W, Gh, acc_eq, acc_ue, phi, qdet;
 	DevBuf<T> Sg;                  // gradient sums, allocated by the first logdet_grad
+	DevBuf<T> Pr;                  // pair products C_{(m+1)%F} C_m, F >= 2
 	DevBuf<double> dR, ldet;       // UDT scales; log |det(I + B...B)| per item
 	DevBuf<int> pvt;
 	DevBuf<unsigned> err;
@@ -626,7 +636,7 @@ struct Group : GroupBase, ProfHook {
 	{
 		for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
 		DevBuf<T> *tb[] = {&expK, &iexpK, &ehK, &iehK, &peu, &ped, &phase, &G, &Cl, &Qm, &Tm,
-		                   &Tm2, &Rs, &X, &W, &Gh, &acc_eq, &acc_ue, &phi, &qdet, &Sg};
+		                   &Tm2, &Rs, &X, &W, &Gh, &acc_eq, &acc_ue, &phi, &qdet, &Sg, &Pr};
 		for (auto *b : tb) b->release();
 		DevBuf<int> *ib[] = {&i_off, &i_idx, &ij_off, &ij_idx, &bb_off, &bb_idx, &bonds, &hs,
 		                     &nacc, &n_eq, &n_ue, &pvt};
@@ -665,6 +675,7 @@ struct Group : GroupBase, ProfHook {
 		rc |= Rs.alloc(NB * NN); rc |= X.alloc(NB * NN); rc |= W.alloc(NB * NN);
 		rc |= Gh.alloc(NB * NN); rc |= dR.alloc((size_t)NB * N); rc |= pvt.alloc((size_t)NB * N);
 		rc |= ldet.alloc(NB);
+		if (F >= 2) rc |= Pr.alloc((size_t)NB * F * NN);
 		rc |= err.alloc(1);
 		eq_size = eq_acc_size(p.num_i, p.num_ij);
 		ue_size = p.period_uneqlt > 0 ? ue_acc_size(p.num_ij, p.num_bb, L, p.meas_bond_corr) : 0;
@@ -792,6 +803,16 @@ struct Group : GroupBase, ProfHook {
 		prof_end(0, fl, 3.0 * sizeof(T) * NN * NB * (nmul - 1));
 	}
 
+	// pair product m: C_{(m+1)%F} C_m of every item (the products that
+	// calc_eq_g's two-cluster groups start from)
+	void build_pair(int m)
+	{
+		const size_t NN = (size_t)N * N;
+		const Addr aC = per_item((long long)F * NN);
+		gemm(gargs<T>(N, N, N, NB, Cl.p + (size_t)((m + 1) % F) * NN, aC, N, Cl.p + (size_t)m * NN, aC, N,
+		              Pr.p + (size_t)m * NN, aC, N));
+	}
+
 	EqWork<T> eq_work()
 	{
 		EqWork<T> w;
@@ -803,12 +824,18 @@ struct Group : GroupBase, ProfHook {
 		w.G = G.p; w.g_stride = (long long)N * N;
 		w.phi = phi.p; w.err = err.p;
 		w.logdet = ldet.p;
+		w.Pr = Pr.p; w.pr_stride = (long long)F * N * N;
 		return w;
 	}
 
 	// G = (I + C_{l0-1} ... C_{l0})^-1 (cyclic), then the chain phases
 	int calc_eq_g(int l0)
 	{
+		// the only pair that calc_eq_g(l0) uses and whose clusters changed
+		// since it was formed is the one ending at cluster l0 - 1, the last
+		// rebuilt (its groups start at l0 (F even) or l0 + 1 (F odd) and
+		// step by two, always through (l0 - 2) mod F)
+		if (F >= 2) build_pair((l0 - 2 + F) % F);
 		int rc = run_calc_eq_g<T>(eq_work(), l0, st, &launch_count, profiling ? this : nullptr);
 		watchdog("calc_eq_g");
 		if (rc) return rc;
@@ -1110,6 +1137,7 @@ struct Group : GroupBase, ProfHook {
 		const long long tot = (long long)C * 2 * L * N;
 		k_diag_all<<<grid_for(tot), 256, 0, st>>>(N, L, C, el.p, hs.p, dv.p, dvi.p);
 		for (int f = 0; f < F; f++) build_cluster(f);
+		for (int m = 0; F >= 2 && m < F; m++) build_pair(m);
 		int rc = calc_eq_g(0);
 		if (rc) return rc;
 		draws(0);
