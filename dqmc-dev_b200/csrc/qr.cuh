@@ -690,6 +690,132 @@ struct RecArgs {
 	unsigned *err;
 };
 
+// The two triangular solves of the recombine for 8 real right-hand sides
+// c0 .. c0+7 (those < N) on the FP64 tensor cores, one warp: Y = D_b^-1 Q^H
+// with the LU's row order (perm), then L (unit lower) and U from M.  Rows go
+// by tiles of 8; the product of a tile's row of L (or U) with the tiles
+// already solved is a chain of m8n8k4 DMMAs (two accumulators), the 8 x 8
+// diagonal block is solved with shuffles.  Solved tiles are kept in the
+// B-fragment layout (lane: rows 4s + l%4, column l/4) for the later products.
+template <int RT>
+__device__ inline void recb_solve8(const double *M, int ld, const int *perm, const double *vsh,
+		const double *Q, double *G, int N, int c0, int lane)
+{
+	const int lr = lane & 3, lq = lane >> 2;
+	const int nt = (N + 7) / 8;
+	double yb[RT][2];
+	// C layout -> B layout of one tile: element (row r, col c) sits in lane
+	// 4 c + r % 4, k-step r / 4; lane (lq, lr) of the C layout holds rows lq,
+	// columns 2 lr + e
+	auto c_to_b = [&](double x0, double x1, double &b0, double &b1) {
+#pragma unroll
+		for (int sgrp = 0; sgrp < 2; sgrp++) {
+			// B lane (lr', lq') wants row 4 sgrp + lr', column lq': in C it is
+			// lane 4 (4 sgrp + lr') + lq' / 2, element lq' % 2
+			const int src = 4 * (4 * sgrp + lr) + (lq >> 1);
+			const double v0 = __shfl_sync(0xffffffffu, x0, src), v1 = __shfl_sync(0xffffffffu, x1, src);
+			const double v = (lq & 1) ? v1 : v0;
+			if (sgrp == 0) b0 = v; else b1 = v;
+		}
+	};
+	auto b_to_c = [&](double b0, double b1, double &x0, double &x1) {
+		// C lane (lq, lr), element e: row lq, column 2 lr + e, held by B lane
+		// 4 (2 lr + e) + lq % 4 in k-step lq / 4
+#pragma unroll
+		for (int e = 0; e < 2; e++) {
+			const int src = 4 * (2 * lr + e) + (lq & 3);
+			const double v0 = __shfl_sync(0xffffffffu, b0, src), v1 = __shfl_sync(0xffffffffu, b1, src);
+			const double v = (lq < 4) ? v0 : v1;
+			if (e == 0) x0 = v; else x1 = v;
+		}
+	};
+	const int cc = c0 + 2 * lr;
+	// forward: L y = P Y
+#pragma unroll
+	for (int t = 0; t < RT; t++) {
+		if (t >= nt) break;
+		const int r = 8 * t + lq;
+		double x[2];
+#pragma unroll
+		for (int e = 0; e < 2; e++) {
+			const int c = cc + e;
+			const int pr = (r < N) ? perm[r] : 0;
+			x[e] = (r < N && c < N) ? Q[c + (size_t)N * pr] * vsh[pr] : 0.0;
+		}
+		double a0[2] = {x[0], x[1]}, a1[2] = {0.0, 0.0};
+#pragma unroll
+		for (int u = 0; u < RT; u++) {
+			if (u >= t) break;
+#pragma unroll
+			for (int sgrp = 0; sgrp < 2; sgrp++) {
+				const int k = 8 * u + 4 * sgrp + lr;
+				const double l = (r < N) ? -M[r + (size_t)ld * k] : 0.0;
+				if (sgrp == 0) dmma(a0[0], a0[1], l, yb[u][0]);
+				else dmma(a1[0], a1[1], l, yb[u][1]);
+			}
+		}
+		x[0] = a0[0] + a1[0];
+		x[1] = a0[1] + a1[1];
+		// unit lower 8 x 8 block
+#pragma unroll
+		for (int q = 0; q < 7; q++) {
+			const double y0 = __shfl_sync(0xffffffffu, x[0], 4 * q + lr);
+			const double y1 = __shfl_sync(0xffffffffu, x[1], 4 * q + lr);
+			if (lq > q && r < N) {
+				const double l = M[r + (size_t)ld * (8 * t + q)];
+				x[0] -= l * y0;
+				x[1] -= l * y1;
+			}
+		}
+		c_to_b(x[0], x[1], yb[t][0], yb[t][1]);
+	}
+	// backward: U g = y
+#pragma unroll
+	for (int t = RT - 1; t >= 0; t--) {
+		if (t >= nt) continue;
+		const int r = 8 * t + lq;
+		double x[2];
+		b_to_c(yb[t][0], yb[t][1], x[0], x[1]);
+		double a0[2] = {x[0], x[1]}, a1[2] = {0.0, 0.0};
+#pragma unroll
+		for (int u = 0; u < RT; u++) {
+			if (u <= t || u >= nt) continue;
+#pragma unroll
+			for (int sgrp = 0; sgrp < 2; sgrp++) {
+				const int k = 8 * u + 4 * sgrp + lr;
+				const double uv = (r < N && k < N) ? -M[r + (size_t)ld * k] : 0.0;
+				if (sgrp == 0) dmma(a0[0], a0[1], uv, yb[u][0]);
+				else dmma(a1[0], a1[1], uv, yb[u][1]);
+			}
+		}
+		x[0] = a0[0] + a1[0];
+		x[1] = a0[1] + a1[1];
+		// upper 8 x 8 block, bottom up
+#pragma unroll
+		for (int q = 7; q >= 0; q--) {
+			const int jq = 8 * t + q;
+			double ujj = (jq < N) ? M[jq + (size_t)ld * jq] : 1.0;
+			if (ujj == 0.0) ujj = 1.0;
+			if (lq == q) {
+				x[0] /= ujj;
+				x[1] /= ujj;
+			}
+			const double y0 = __shfl_sync(0xffffffffu, x[0], 4 * q + lr);
+			const double y1 = __shfl_sync(0xffffffffu, x[1], 4 * q + lr);
+			if (lq < q && r < N && jq < N) {
+				const double uv = M[r + (size_t)ld * jq];
+				x[0] -= uv * y0;
+				x[1] -= uv * y1;
+			}
+		}
+		if (r < N) {
+			if (cc < N) G[r + (size_t)N * cc] = x[0];
+			if (cc + 1 < N) G[r + (size_t)N * (cc + 1)] = x[1];
+		}
+		c_to_b(x[0], x[1], yb[t][0], yb[t][1]);
+	}
+}
+
 // ----------------------------------------------- recombine in shared memory
 //
 // G = (D_b^-1 Q^H + D_s T)^-1 D_b^-1 Q^H (greens.c:157-178)
@@ -809,7 +935,13 @@ __global__ void __launch_bounds__(NW * 32) k_recb(RecArgs<T> a)
 
 	// right-hand sides Y = D_b^-1 Q^H, CB columns per pass of a warp
 	T *G = a.G + (size_t)item * a.g_stride;
-	for (int c0 = w * CB; c0 < N; c0 += NW * CB) {
+	constexpr bool TC = !is_cplx<T>::value && !GM;   // real, shared memory: DMMA tiles
+	if constexpr (TC) {
+		for (int c0 = 8 * w; c0 < N; c0 += 8 * NW)
+			recb_solve8<4 * RPL>((const double *)M, ld, perm, vsh, (const double *)Q, (double *)G, N, c0,
+			                     lane);
+	}
+	for (int c0 = w * CB; !TC && c0 < N; c0 += NW * CB) {
 		T y[CB][RPL];
 #pragma unroll
 		for (int b = 0; b < CB; b++) {
