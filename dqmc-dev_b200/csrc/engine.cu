@@ -43,7 +43,7 @@ static int launch_gemm_mode(const GemmArgs<T> &g, cudaStream_t st)
 	static bool attr = false;
 	if (!attr) {
 		if (cudaFuncSetAttribute(k_gemm<T, BM, BN, BK, WM, WN, ST, MODE>,
-		                         cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM_BYTES) != cudaSuccess)
+		                         cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM_MAX) != cudaSuccess)
 			return DQMC_E_ARG;
 		attr = true;
 	}
@@ -52,7 +52,7 @@ static int launch_gemm_mode(const GemmArgs<T> &g, cudaStream_t st)
 		GemmArgs<T> gc = g;
 		gc.b0 = b0;
 		dim3 grid((g.M + BM - 1) / BM, (g.N + BN - 1) / BN, min(65535, g.batch - b0));
-		k_gemm<T, BM, BN, BK, WM, WN, ST, MODE><<<grid, Cfg::THREADS, Cfg::SMEM_BYTES, st>>>(gc);
+		k_gemm<T, BM, BN, BK, WM, WN, ST, MODE><<<grid, Cfg::THREADS, Cfg::smem_bytes(MODE, g.K), st>>>(gc);
 	}
 	return 0;
 }
@@ -87,7 +87,7 @@ int launch_gemm(const GemmArgs<T> &g, cudaStream_t st)
 		return launch_gemm_cfg<T, 32, 32, 8, 2, 2, 3>(g, st);
 	} else {
 		if (p64 <= p48 && p64 <= p32) return launch_gemm_cfg<T, 64, 64, 16, 2, 2, 3>(g, st);
-		if (p48 <= p32) return launch_gemm_cfg<T, 48, 48, 16, 2, 2, 4>(g, st);
+		if (p48 <= p32) return launch_gemm_cfg<T, 48, 48, 16, 2, 2, 3>(g, st);
 		return launch_gemm_cfg<T, 32, 32, 16, 2, 2, 4>(g, st);
 	}
 }

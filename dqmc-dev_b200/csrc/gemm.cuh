@@ -103,8 +103,18 @@ struct GemmCfg {
 	static constexpr int TILE_B = BN * SB;
 	static constexpr int STAGE = TILE_A + TILE_B;     // elements of T
 	static constexpr int KMAX = 512;                  // largest K of the scale vectors
-	static constexpr int SMEM_BYTES = STAGES * STAGE * (int)sizeof(T)
-	                                  + (2 * KMAX + BM + BN) * (int)sizeof(double) + KMAX * 4;
+	static constexpr int RING_BYTES = STAGES * STAGE * (int)sizeof(T);
+	// the ring, then (modes with scale vectors or a gather only) per-k
+	// scales, per-k inverse scales, per-row and per-column scales and the
+	// gather rows, sized for this launch's K so that the CTAs of the plain
+	// modes hold only the ring
+	static constexpr int smem_bytes(int mode, int K)
+	{
+		return RING_BYTES + ((mode & (GM_A_DD | GM_B_ROWD | GM_B_COLD | GM_B_GATHER))
+		                         ? (2 * K + BM + BN) * (int)sizeof(double) + K * 4
+		                         : 0);
+	}
+	static constexpr int SMEM_MAX = RING_BYTES + (2 * KMAX + BM + BN) * (int)sizeof(double) + KMAX * 4;
 	static constexpr int WTM = BM / WM, WTN = BN / WN;
 	static constexpr int MT = WTM / 8, NT = WTN / 8;
 	static constexpr int A_PER_T = (BM * BK + THREADS - 1) / THREADS;
@@ -121,9 +131,9 @@ k_gemm(GemmArgs<T> g)
 	constexpr bool CX = Cfg::CX;
 	extern __shared__ __align__(16) unsigned char smraw[];
 	T *sm = (T *)smraw;
-	double *sdk = (double *)(smraw + STAGES * Cfg::STAGE * sizeof(T));   // per-k scale
-	double *sdk2 = sdk + Cfg::KMAX;                                       // per-k 1/d (A_DD)
-	double *sdr = sdk2 + Cfg::KMAX;                                       // per-row (A_DD)
+	double *sdk = (double *)(smraw + Cfg::RING_BYTES);                    // per-k scale
+	double *sdk2 = sdk + g.K;                                             // per-k 1/d (A_DD)
+	double *sdr = sdk2 + g.K;                                             // per-row (A_DD)
 	double *sdc = sdr + BM;                                               // per-column (B_COLD)
 	int *sgi = (int *)(sdc + BN);                                         // gather rows
 	const int b = g.b0 + blockIdx.z;
