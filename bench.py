@@ -492,7 +492,7 @@ def main():
     dom = max(ROOFLINE_KERNELS, key=lambda k: prof[k][0])
     d_ms, d_n, d_fl, d_by = prof[dom]
     achieved = d_fl / (d_ms / 1e3) / 1e12 if d_ms > 0 else 0.0
-    items = 2 * nch
+    items = 2 * nch / eng.lanes()      # chain-spin items of one launch (lane)
     traffic = TRAFFIC_PER_ITEM.get(dom)
 
     plain = plain_chain_rate(sims[0], local)
@@ -518,9 +518,13 @@ def main():
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "chains_per_gpu": nch,
+            "config": {"workload": WORKLOAD, "chains_per_gpu": nch, "lanes": eng.lanes(),
                        "l2": "inputs larger than L2 (about 2.6 MB of matrices per chain-spin)",
                        "sweep_profile_ms": sweep_ms,
+                       "sweep_profile_note": "kernel ms per class over one eager sweep with each "
+                                             "lane profiled alone, lanes one after another; the "
+                                             "timed sweeps overlap the lanes, so the sum exceeds "
+                                             "ms_per_step",
                        "plain_1chain_gpu": {"value": plain, "unit": METRIC,
                                             "batched_over_plain": value / world / plain
                                             if plain else None}},

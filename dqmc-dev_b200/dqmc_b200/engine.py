@@ -208,6 +208,10 @@ class Engine:
     def stream(self) -> int:
         return int(self.lib.dqmc_engine_stream(self.h) or 0)
 
+    def lanes(self) -> int:
+        """Number of sub-batches (each with its own stream) the chains run in."""
+        return int(self.lib.dqmc_engine_lanes(self.h))
+
     def pull(self):
         """Copy every chain's state and accumulators back into its SimData."""
         for c, s in enumerate(self.sims):

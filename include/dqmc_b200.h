@@ -73,9 +73,18 @@ typedef struct {
  * dqmc-dev_b200/csrc/meas.cuh: sign, then the datasets in data.h order). */
 int dqmc_acc_sizes(const dqmc_params *p, int *eq_size, int *ue_size);
 
+/* An engine advances n_chain chains of one parameter set (the batched form
+ * of the reference's one chain per process, main_1.c:27-60 and dqmc.c).
+ * It splits them into lanes, contiguous sub-batches with their own streams
+ * whose kernels overlap on the GPU: one lane per 64 chains, at most 4, or
+ * the value of the environment variable DQMC_LANES at creation.  Results do
+ * not depend on the split. */
 int dqmc_engine_create(const dqmc_params *p, int n_chain, int device,
 		dqmc_engine **out);
 void dqmc_engine_destroy(dqmc_engine *e);
+/* number of lanes the engine's chains are split into (no counterpart in the
+ * reference, which runs one chain per process) */
+int dqmc_engine_lanes(dqmc_engine *e);
 
 /* Per-chain state (host arrays, copied): exp_lambda[2N], del[2N] as in the
  * sim file, rng[17], hs[L*N] (hs[i + N*l]), and the sweep counter (equal
@@ -106,7 +115,8 @@ int dqmc_engine_get_acc(dqmc_engine *e, int chain, int *eq_n_sample, void *eq_ac
 int dqmc_engine_get_g(dqmc_engine *e, int chain, void *gu, void *gd, void *phase);
 /* total Metropolis accepts of a chain since creation */
 int dqmc_engine_accepts(dqmc_engine *e, int chain, long long *n);
-/* CUDA stream the engine queues on, as an opaque handle (cudaStream_t) */
+/* CUDA stream the engine queues on, as an opaque handle (cudaStream_t):
+ * every sweep forks from it to the lanes' streams and joins back to it */
 void *dqmc_engine_stream(dqmc_engine *e);
 /* number of kernels one sweep of the given kind launches */
 int dqmc_engine_launches_per_sweep(dqmc_engine *e, int meas_eq, int meas_ue);

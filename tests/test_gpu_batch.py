@@ -95,3 +95,67 @@ def test_wrapper_batch_ragged_equals_single(mods, tmp_path):
             if k.startswith("meas_eqlt/"):
                 np.testing.assert_allclose(np.asarray(db[k]), np.asarray(da[k]), rtol=1e-12,
                                            atol=1e-12, err_msg=k)
+
+
+def _group(gen, n, **kw):
+    """n chains of one parameter set, chain c from the master stream jumped c times"""
+    from dqmc_b200 import replicas
+    rngs = replicas.chain_streams(5, range(n))
+    d0 = gen.make_sim(init_rng=rngs[0], **kw)
+    out = [d0]
+    for r in rngs[1:]:
+        hs, rng = gen.initial_hs(r, kw["L"], kw["Nx"] * kw["Ny"])
+        d = dict(d0)
+        d["state/init_rng"], d["state/rng"], d["state/hs"] = r, rng, hs
+        out.append(d)
+    return out
+
+
+def _run_lanes(engine, dicts, lanes, monkeypatch):
+    monkeypatch.setenv("DQMC_LANES", str(lanes))
+    sims = [engine.SimData(dict(d)) for d in dicts]
+    e = engine.Engine(sims)
+    e.init()
+    e.sweeps(sims[0].p["n_sweep"])
+    e.pull()
+    assert e.errors() == 0
+    gs = [e.g(c) for c in range(len(sims))]
+    e.close()
+    return sims, gs
+
+
+def test_lanes_are_bit_identical(mods, monkeypatch):
+    """An engine split into lanes (sub-batches on their own streams, forked
+    from and joined to the engine's stream) gives every chain exactly the
+    state and measurements of the one-lane engine; 7 chains in 3 lanes of
+    3, 2 and 2, with unequal-time measurements."""
+    batch, engine, gen, simfile = mods
+    dicts = _group(gen, 7, Nx=4, Ny=4, U=4.0, dt=0.1, L=16, n_matmul=4, period_eqlt=4,
+                   period_uneqlt=1, n_delay=4, n_sweep_warm=1, n_sweep_meas=2)
+    one, g1 = _run_lanes(engine, dicts, 1, monkeypatch)
+    three, g3 = _run_lanes(engine, dicts, 3, monkeypatch)
+    for c, (a, b) in enumerate(zip(one, three)):
+        assert np.array_equal(a.hs, b.hs), c
+        assert np.array_equal(a.rng, b.rng), c
+        assert np.array_equal(a.eq_acc, b.eq_acc), c
+        assert np.array_equal(a.ue_acc, b.ue_acc), c
+        for x, y in zip(g1[c], g3[c]):
+            assert np.array_equal(x, y), c
+
+
+def test_lanes_gradients_match(mods, monkeypatch):
+    """logdet_grad and obs_grad of a 3-lane engine (lanes in parallel host
+    threads) against the one-lane engine, configuration by configuration."""
+    batch, engine, gen, simfile = mods
+    dicts = _group(gen, 5, Nx=4, Ny=4, U=4.0, dt=0.1, L=8, n_matmul=4, period_eqlt=4,
+                   n_sweep_warm=0, n_sweep_meas=1)
+    out = {}
+    for lanes in (1, 3):
+        monkeypatch.setenv("DQMC_LANES", str(lanes))
+        e = engine.Engine([engine.SimData(dict(d)) for d in dicts])
+        out[lanes] = (e.logdet_grad(), e.obs_grad())
+        e.close()
+    (ld1, S1), (o1, Z1) = out[1]
+    (ld3, S3), (o3, Z3) = out[3]
+    assert np.array_equal(ld1, ld3) and np.array_equal(S1, S3)
+    assert np.array_equal(o1, o3) and np.array_equal(Z1, Z3)
