@@ -557,7 +557,18 @@ static cudaError_t raise_smem(K kern, size_t bytes)
 template <typename T>
 static cudaError_t update_attr(size_t bytes)
 {
-	return raise_smem(k_update<T>, bytes);
+	const cudaError_t e = raise_smem(k_update<T>, bytes);
+	return e != cudaSuccess ? e : raise_smem(k_update_big<T>, bytes);
+}
+
+// the delayed update of a.nchain chains: 2 ceil(N/32) warps of tests and
+// one look-ahead warp per chain, in the launch form sized for that CTA
+template <typename T>
+static void launch_update(const UpdArgs<T> &a, size_t smem, cudaStream_t st)
+{
+	const int threads = 2 * ((a.N + 31) / 32 * 32) + 32;
+	if (threads <= 352) k_update<T><<<a.nchain, threads, smem, st>>>(a);
+	else k_update_big<T><<<a.nchain, threads, smem, st>>>(a);
 }
 
 struct GroupBase {
@@ -864,9 +875,8 @@ struct Group : GroupBase, ProfHook {
 		// the look-ahead warp draws the next slice, except when that is this
 		// slice again (L = 1), whose fields this kernel is still changing
 		a.next_slice = (L == 1) ? -1 : (l + 1) % L;
-		const int np = (N + 31) / 32 * 32;
 		prof_begin(1);
-		k_update<T><<<C, 2 * np + 32, update_smem_bytes<T>(N, kd, ldp), st>>>(a);
+		launch_update<T>(a, update_smem_bytes<T>(N, kd, ldp), st);
 		prof_end(PC_UPDATE, 0.0, 0.0);
 		launch_count++;
 		watchdog("k_update");
@@ -1657,15 +1667,16 @@ struct Lanes : GroupBase {
 };
 
 // lanes of an engine of n_chain chains: DQMC_LANES when set, else one lane
-// per 64 chains, at most 4 (at 256 chains of 12 x 12, two lanes run 9% and
-// four 11% more chain-sweeps per second than one)
+// per 32 chains, at most 4 (at 256 chains of 12 x 12, two lanes run 9% and
+// four 11% more chain-sweeps per second than one, eight no more than four;
+// 64 complex 10 x 10 chains run 3% faster in two lanes than in one)
 static int lane_count(int n_chain)
 {
 	if (const char *v = getenv("DQMC_LANES")) {
 		const int n = atoi(v);
 		if (n >= 1) return std::min(n, n_chain);
 	}
-	return std::max(1, std::min(4, n_chain / 64));
+	return std::max(1, std::min(4, n_chain / 32));
 }
 
 }  // namespace dq
@@ -1857,8 +1868,7 @@ static int seam_update(int batch, int N, int n_delay, const double *del, uint64_
 	a.N = N; a.L = 1; a.n_delay = kd; a.nchain = batch; a.slice = 0; a.ldp = ldp;
 	a.del = del; a.rng = rng; a.rng_ckpt = ck; a.hs = hs; a.G = (T *)G; a.phase = (T *)phase;
 	a.order = ord; a.u = uu; a.next_slice = -1;
-	const int np = (N + 31) / 32 * 32;
-	k_update<T><<<batch, 2 * np + 32, update_smem_bytes<T>(N, kd, ldp), st>>>(a);
+	launch_update<T>(a, update_smem_bytes<T>(N, kd, ldp), st);
 	CK(cudaGetLastError());
 	CK(cudaStreamSynchronize(st));
 	return 0;

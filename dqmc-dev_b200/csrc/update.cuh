@@ -125,7 +125,7 @@ __device__ inline void bar_metro(int nthreads)
 }
 
 template <typename T>
-__global__ void k_update(UpdArgs<T> a)
+__device__ __forceinline__ void update_chain(const UpdArgs<T> &a)
 {
 	constexpr bool CX = is_cplx<T>::value;
 	constexpr int PL = CX ? 2 : 1;
@@ -403,6 +403,21 @@ __global__ void k_update(UpdArgs<T> a)
 		a.phase[c] = s_phase;
 		if (a.n_accept) a.n_accept[c] += s_nacc;
 	}
+}
+
+// The delayed update, one CTA per chain.  k_update leaves the register
+// count to the compiler (two CTAs of N <= 160 share an SM); k_update_big
+// bounds it so that CTAs of up to 544 threads (N <= 256) can launch.
+template <typename T>
+__global__ void k_update(UpdArgs<T> a)
+{
+	update_chain(a);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(544, 1) k_update_big(UpdArgs<T> a)
+{
+	update_chain(a);
 }
 
 }  // namespace dq

@@ -347,10 +347,12 @@ def test_calc_eq_g_seam_large(eng, Nx, Ny, nflux, tmp_path):
             assert abs(dph.cpu().numpy()[0] - ph_o[0]) < 1e-12
 
 
-@pytest.mark.parametrize("Nx,Ny,nflux", [(12, 12, 0), (16, 16, 0), (10, 10, 1)])
+@pytest.mark.parametrize("Nx,Ny,nflux", [(12, 12, 0), (16, 16, 0), (10, 10, 1), (16, 16, 1)])
 def test_engine_large_matches_oracle(eng, Nx, Ny, nflux, tmp_path):
     """2 sweeps of a large chain (L = 20): HS fields and RNG bit-exact, G and
-    the equal-time measurements within tolerance of the oracle."""
+    the equal-time measurements within tolerance of the oracle.  16 x 16
+    runs the delayed update in CTAs of 544 threads (its large launch form),
+    real and complex."""
     path = _gen_case(tmp_path, Nx, Ny, U=4.0, mu=-1.0, dt=0.05, L=20, n_matmul=5, n_delay=16,
                      period_eqlt=5, n_sweep_warm=0, n_sweep_meas=2, nflux=nflux)
     o = Sim(path)
