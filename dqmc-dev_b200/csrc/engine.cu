@@ -1629,7 +1629,9 @@ struct Lanes : GroupBase {
 	}
 
 	// the gradient paths launch eagerly and wait on the host between steps:
-	// one host thread per lane keeps the lanes' work concurrent
+	// two host threads, each taking every second lane, keep two lanes' work
+	// concurrent (more threads ran slower: their allocations and device-wide
+	// waits serialise them)
 	template <typename F>
 	int per_lane(F f)
 	{
@@ -1638,9 +1640,14 @@ struct Lanes : GroupBase {
 		CK(cudaGetDevice(&dev));
 		std::vector<int> rc(g.size(), 0);
 		std::vector<std::thread> th;
-		for (size_t k = 0; k < g.size(); k++)
-			th.emplace_back([&, k] {
-				rc[k] = cudaSetDevice(dev) == cudaSuccess ? f(k) : DQMC_E_CUDA;
+		const size_t nth = std::min<size_t>(2, g.size());
+		for (size_t t = 0; t < nth; t++)
+			th.emplace_back([&, t] {
+				const bool ok = cudaSetDevice(dev) == cudaSuccess;
+				for (size_t k = t; k < g.size(); k += nth) {
+					rc[k] = ok ? f(k) : DQMC_E_CUDA;
+					if (rc[k]) break;
+				}
 			});
 		for (auto &t : th) t.join();
 		for (int r : rc) if (r) return r;
@@ -1667,16 +1674,18 @@ struct Lanes : GroupBase {
 };
 
 // lanes of an engine of n_chain chains: DQMC_LANES when set, else one lane
-// per 32 chains, at most 4 (at 256 chains of 12 x 12, two lanes run 9% and
+// per 64 chains, at most 4 (at 256 chains of 12 x 12, two lanes run 9% and
 // four 11% more chain-sweeps per second than one, eight no more than four;
-// 64 complex 10 x 10 chains run 3% faster in two lanes than in one)
+// 64 complex 10 x 10 chains run 3% faster in two lanes than in one, but
+// the gradients of 128 configurations of 8 x 8 run 182 evaluations/s in
+// two lanes, 173 in one and 72 in four)
 static int lane_count(int n_chain)
 {
 	if (const char *v = getenv("DQMC_LANES")) {
 		const int n = atoi(v);
 		if (n >= 1) return std::min(n, n_chain);
 	}
-	return std::max(1, std::min(4, n_chain / 32));
+	return std::max(1, std::min(4, n_chain / 64));
 }
 
 }  // namespace dq
