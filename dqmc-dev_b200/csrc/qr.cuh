@@ -697,13 +697,16 @@ struct RecArgs {
 // already solved is a chain of m8n8k4 DMMAs (two accumulators), the 8 x 8
 // diagonal block is solved with shuffles.  Solved tiles are kept in the
 // B-fragment layout (lane: rows 4s + l%4, column l/4) for the later products.
-template <int RT>
+// ys: this warp's slab of 64 ceil(N/8) doubles in shared memory.  Tile t
+// of the solution is kept there in B layout (ys[64 t + 32 s + lane], k-step
+// s), each lane reading back only what it wrote, so the slab needs no
+// synchronisation; holding the tiles in registers instead spills.
 __device__ inline void recb_solve8(const double *M, int ld, const int *perm, const double *vsh,
-		const double *Q, double *G, int N, int c0, int lane)
+		const double *Q, double *G, int N, int c0, int lane, double *ys)
 {
 	const int lr = lane & 3, lq = lane >> 2;
 	const int nt = (N + 7) / 8;
-	double yb[RT][2];
+	auto yb = [&](int u, int sgrp) -> double & { return ys[64 * u + 32 * sgrp + lane]; };
 	// C layout -> B layout of one tile: element (row r, col c) sits in lane
 	// 4 c + r % 4, k-step r / 4; lane (lq, lr) of the C layout holds rows lq,
 	// columns 2 lr + e
@@ -731,9 +734,8 @@ __device__ inline void recb_solve8(const double *M, int ld, const int *perm, con
 	};
 	const int cc = c0 + 2 * lr;
 	// forward: L y = P Y
-#pragma unroll
-	for (int t = 0; t < RT; t++) {
-		if (t >= nt) break;
+#pragma unroll 1
+	for (int t = 0; t < nt; t++) {
 		const int r = 8 * t + lq;
 		double x[2];
 #pragma unroll
@@ -743,15 +745,14 @@ __device__ inline void recb_solve8(const double *M, int ld, const int *perm, con
 			x[e] = (r < N && c < N) ? Q[c + (size_t)N * pr] * vsh[pr] : 0.0;
 		}
 		double a0[2] = {x[0], x[1]}, a1[2] = {0.0, 0.0};
-#pragma unroll
-		for (int u = 0; u < RT; u++) {
-			if (u >= t) break;
+#pragma unroll 4
+		for (int u = 0; u < t; u++) {
 #pragma unroll
 			for (int sgrp = 0; sgrp < 2; sgrp++) {
 				const int k = 8 * u + 4 * sgrp + lr;
 				const double l = (r < N) ? -M[r + (size_t)ld * k] : 0.0;
-				if (sgrp == 0) dmma(a0[0], a0[1], l, yb[u][0]);
-				else dmma(a1[0], a1[1], l, yb[u][1]);
+				if (sgrp == 0) dmma(a0[0], a0[1], l, yb(u, 0));
+				else dmma(a1[0], a1[1], l, yb(u, 1));
 			}
 		}
 		x[0] = a0[0] + a1[0];
@@ -767,25 +768,23 @@ __device__ inline void recb_solve8(const double *M, int ld, const int *perm, con
 				x[1] -= l * y1;
 			}
 		}
-		c_to_b(x[0], x[1], yb[t][0], yb[t][1]);
+		c_to_b(x[0], x[1], yb(t, 0), yb(t, 1));
 	}
 	// backward: U g = y
-#pragma unroll
-	for (int t = RT - 1; t >= 0; t--) {
-		if (t >= nt) continue;
+#pragma unroll 1
+	for (int t = nt - 1; t >= 0; t--) {
 		const int r = 8 * t + lq;
 		double x[2];
-		b_to_c(yb[t][0], yb[t][1], x[0], x[1]);
+		b_to_c(yb(t, 0), yb(t, 1), x[0], x[1]);
 		double a0[2] = {x[0], x[1]}, a1[2] = {0.0, 0.0};
-#pragma unroll
-		for (int u = 0; u < RT; u++) {
-			if (u <= t || u >= nt) continue;
+#pragma unroll 4
+		for (int u = t + 1; u < nt; u++) {
 #pragma unroll
 			for (int sgrp = 0; sgrp < 2; sgrp++) {
 				const int k = 8 * u + 4 * sgrp + lr;
 				const double uv = (r < N && k < N) ? -M[r + (size_t)ld * k] : 0.0;
-				if (sgrp == 0) dmma(a0[0], a0[1], uv, yb[u][0]);
-				else dmma(a1[0], a1[1], uv, yb[u][1]);
+				if (sgrp == 0) dmma(a0[0], a0[1], uv, yb(u, 0));
+				else dmma(a1[0], a1[1], uv, yb(u, 1));
 			}
 		}
 		x[0] = a0[0] + a1[0];
@@ -812,7 +811,7 @@ __device__ inline void recb_solve8(const double *M, int ld, const int *perm, con
 			if (cc < N) G[r + (size_t)N * cc] = x[0];
 			if (cc + 1 < N) G[r + (size_t)N * (cc + 1)] = x[1];
 		}
-		c_to_b(x[0], x[1], yb[t][0], yb[t][1]);
+		c_to_b(x[0], x[1], yb(t, 0), yb(t, 1));
 	}
 }
 
@@ -826,11 +825,34 @@ __device__ inline void recb_solve8(const double *M, int ld, const int *perm, con
 // registers (permutation, unit-lower forward, upper backward), and the
 // phase 1/phase(det G) = phase(det Q) phase(det M) sign(prod v).
 
+// the recombine's shared memory: M (unless in global memory), the scale
+// vectors and pivots, then (real M in shared memory) the solve slabs of
+// recb_solve_warps warps, as many as fit under RECB_SMEM_CAP, at least one
+constexpr size_t RECB_SMEM_CAP = 226 * 1024;
+
+template <typename T>
+__host__ __device__ inline size_t recb_base_bytes(int N, bool gm)
+{
+	// a multiple of 16 bytes, where the solve slabs start
+	return ((gm ? 0 : sizeof(T) * (size_t)qrb_ld(N) * N) + sizeof(double) * 2 * (size_t)N
+	        + sizeof(int) * 2 * (size_t)N + 64 + 15) & ~(size_t)15;
+}
+
+__host__ __device__ inline size_t recb_slab_bytes(int N) { return sizeof(double) * 64 * (size_t)((N + 7) / 8); }
+
+template <typename T>
+__host__ __device__ inline int recb_solve_warps(int N, bool gm)
+{
+	if (is_cplx<T>::value || gm) return 0;
+	const size_t base = recb_base_bytes<T>(N, gm), slab = recb_slab_bytes(N);
+	const size_t fit = base < RECB_SMEM_CAP ? (RECB_SMEM_CAP - base) / slab : 0;
+	return fit < 1 ? 1 : (fit > 16 ? 16 : (int)fit);
+}
+
 template <typename T>
 size_t recb_smem_bytes(int N, bool gm = false)
 {
-	return (gm ? 0 : sizeof(T) * (size_t)qrb_ld(N) * N) + sizeof(double) * 2 * (size_t)N
-	       + sizeof(int) * 2 * (size_t)N + 64;
+	return recb_base_bytes<T>(N, gm) + recb_slab_bytes(N) * recb_solve_warps<T>(N, gm);
 }
 
 template <typename T, int NW, int RPL, int CB, bool GM>
@@ -937,9 +959,12 @@ __global__ void __launch_bounds__(NW * 32) k_recb(RecArgs<T> a)
 	T *G = a.G + (size_t)item * a.g_stride;
 	constexpr bool TC = !is_cplx<T>::value && !GM;   // real, shared memory: DMMA tiles
 	if constexpr (TC) {
-		for (int c0 = 8 * w; c0 < N; c0 += 8 * NW)
-			recb_solve8<4 * RPL>((const double *)M, ld, perm, vsh, (const double *)Q, (double *)G, N, c0,
-			                     lane);
+		const int nws = min(NW, recb_solve_warps<T>(N, GM));
+		double *ys = (double *)(smraw + recb_base_bytes<T>(N, GM))
+		             + (size_t)64 * ((N + 7) / 8) * w;
+		for (int c0 = 8 * w; w < nws && c0 < N; c0 += 8 * nws)
+			recb_solve8((const double *)M, ld, perm, vsh, (const double *)Q, (double *)G, N, c0,
+			                     lane, ys);
 	}
 	for (int c0 = w * CB; !TC && c0 < N; c0 += NW * CB) {
 		T y[CB][RPL];
@@ -1014,22 +1039,29 @@ __global__ void __launch_bounds__(NW * 32) k_recb(RecArgs<T> a)
 			}
 		}
 	}
-	if (tid == 0) {
-		T ph = a.qdet ? a.qdet[item] : one<T>();
-		double vs = 1.0;
-		int nswap = 0;
-		for (int j = 0; j < N; j++) {
-			ph = ph * phase_of(M[j + (size_t)ld * j]);
-			vs *= (vsh[j] < 0.0) ? -1.0 : 1.0;
-			nswap += (ipiv[j] != j);
-		}
-		if (nswap & 1) ph = ph * -1.0;
-		a.phase[item] = ph * vs;
-		if (a.logdet) {
+	if (w == 0) {
+		// phase(det) = phase(det Q) prod phase(U_jj) sign(prod v_j) (-1)^swaps,
+		// each lane taking every 32nd j, then a butterfly over the warp
+		T ph = one<T>();
+		int neg = 0;
+		double l = 0.0;
+		for (int j = lane; j < N; j += 32) {
+			const T u = M[j + (size_t)ld * j];
+			ph = ph * phase_of(u);
+			neg ^= (vsh[j] < 0.0) ^ (ipiv[j] != j);
 			// G = M^-1 diag(v) Q^H: log |det G| = sum log |v_j| - sum log |U_jj|
-			double l = 0.0;
-			for (int j = 0; j < N; j++) l += log(absv(M[j + (size_t)ld * j])) - log(fabs(vsh[j]));
-			a.logdet[item] = l;
+			if (a.logdet) l += log(absv(u)) - log(fabs(vsh[j]));
+		}
+#pragma unroll
+		for (int o = 16; o > 0; o >>= 1) {
+			ph = ph * shfl_xor(ph, o);
+			neg ^= __shfl_xor_sync(0xffffffffu, neg, o);
+			l += __shfl_xor_sync(0xffffffffu, l, o);
+		}
+		if (lane == 0) {
+			if (a.qdet) ph = a.qdet[item] * ph;
+			a.phase[item] = neg ? ph * -1.0 : ph;
+			if (a.logdet) a.logdet[item] = l;
 		}
 	}
 }
