@@ -888,58 +888,92 @@ __global__ void __launch_bounds__(NW * 32) k_recb(RecArgs<T> a)
 	__syncthreads();
 
 	bool nan_seen = false, sing = false;
-	for (int j = 0; j < N; j++) {
-		if (w == 0) {
-			double best = -1.0;
-			int br = N;
-			for (int r = j + lane; r < N; r += 32) {
-				double m = absv(M[r + (size_t)ld * j]);
-				if (!(m >= 0.0)) {
-					m = -0.5;
-					nan_seen = true;
-				}
-				if (m > best) { best = m; br = r; }
+	// Pivot of column j (warp 0): the first largest |M[r, j]|, r >= j, as
+	// idamax; rows j and the pivot row swapped in column j only (the other
+	// columns swap them when step j reaches them); multipliers scaled.
+	auto pivot_col = [&](int j) {
+		double best = -1.0;
+		int br = N;
+		for (int r = j + lane; r < N; r += 32) {
+			double m = absv(M[r + (size_t)ld * j]);
+			if (!(m >= 0.0)) {
+				m = -0.5;
+				nan_seen = true;
 			}
-#pragma unroll
-			for (int o = 16; o > 0; o >>= 1) {
-				const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-				const int orr = __shfl_xor_sync(0xffffffffu, br, o);
-				if (ob > best || (ob == best && orr < br)) { best = ob; br = orr; }
-			}
-			if (br != j)
-				for (int c = lane; c < N; c += 32) {
-					const T t0 = M[j + (size_t)ld * c];
-					M[j + (size_t)ld * c] = M[br + (size_t)ld * c];
-					M[br + (size_t)ld * c] = t0;
-				}
-			if (lane == 0) ipiv[j] = br;
-			__syncwarp();
-			T piv = M[j + (size_t)ld * j];
-			if (re(piv) == 0.0 && im(piv) == 0.0) {
-				sing = true;
-				piv = one<T>();
-			}
-			const T ip = one<T>() / piv;
-			for (int r = j + 1 + lane; r < N; r += 32) M[r + (size_t)ld * j] *= ip;
+			if (m > best) { best = m; br = r; }
 		}
-		__syncthreads();
+#pragma unroll
+		for (int o = 16; o > 0; o >>= 1) {
+			const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+			const int orr = __shfl_xor_sync(0xffffffffu, br, o);
+			if (ob > best || (ob == best && orr < br)) { best = ob; br = orr; }
+		}
+		if (lane == 0) {
+			if (br != j) {
+				const T t0 = M[j + (size_t)ld * j];
+				M[j + (size_t)ld * j] = M[br + (size_t)ld * j];
+				M[br + (size_t)ld * j] = t0;
+			}
+			ipiv[j] = br;
+		}
+		__syncwarp();
+		T piv = M[j + (size_t)ld * j];
+		if (re(piv) == 0.0 && im(piv) == 0.0) {
+			sing = true;
+			piv = one<T>();
+		}
+		const T ip = one<T>() / piv;
+		for (int r = j + 1 + lane; r < N; r += 32) M[r + (size_t)ld * j] *= ip;
+	};
+	// Step j on column c > j (one warp): the row swap of step j, then the
+	// rank-1 update with the multipliers l of column j
+	auto update_col = [&](int j, int pj, int c, const T (&l)[RPL]) {
+		T *col = M + (size_t)ld * c;
+		if (lane == 0 && pj != j) {
+			const T t0 = col[j];
+			col[j] = col[pj];
+			col[pj] = t0;
+		}
+		__syncwarp();
+		const T u = col[j];
+#pragma unroll
+		for (int t = 0; t < RPL; t++) {
+			const int r = j + 1 + lane + 32 * t;
+			if (r < N) col[r] -= l[t] * u;
+		}
+	};
+	// One barrier per step: warp 0 updates column j + 1 and pivots it for
+	// the next step (look-ahead) while warps 1.. update the other columns and
+	// apply the step's row swap to the columns left of j (the L factor).
+	if (w == 0) pivot_col(0);
+	__syncthreads();
+	for (int j = 0; j < N; j++) {
+		const int pj = ipiv[j];
 		T l[RPL];
 #pragma unroll
 		for (int t = 0; t < RPL; t++) {
 			const int r = j + 1 + lane + 32 * t;
 			l[t] = (r < N) ? M[r + (size_t)ld * j] : zero<T>();
 		}
-		for (int c = j + 1 + w; c < N; c += NW) {
-			T *col = M + (size_t)ld * c;
-			const T u = col[j];
-#pragma unroll
-			for (int t = 0; t < RPL; t++) {
-				const int r = j + 1 + lane + 32 * t;
-				if (r < N) col[r] -= l[t] * u;
+		if (w == 0) {
+			if (j + 1 < N) {
+				update_col(j, pj, j + 1, l);
+				__syncwarp();
+				pivot_col(j + 1);
 			}
+		} else {
+			if (pj != j)
+				for (int c = tid - 32; c < j; c += blockDim.x - 32) {
+					const T t0 = M[j + (size_t)ld * c];
+					M[j + (size_t)ld * c] = M[pj + (size_t)ld * c];
+					M[pj + (size_t)ld * c] = t0;
+				}
+			for (int c = j + 1 + w; c < N; c += NW - 1) update_col(j, pj, c, l);
 		}
 		__syncthreads();
 	}
+	nan_seen = __any_sync(0xffffffffu, nan_seen);
+	sing = __any_sync(0xffffffffu, sing);
 	if (tid == 0) {
 		for (int r = 0; r < N; r++) perm[r] = r;
 		for (int j = 0; j < N; j++) {
