@@ -458,26 +458,32 @@ def main():
     value = nch * args.steps * world / t_max
     launches = eng.launches_per_sweep(True, False) * args.steps
 
-    # end to end through the C ABI with host buffers: per step, the chains'
-    # state goes host -> device, one sweep runs, state and measurements come back
-    L = lib.load()
+    # end to end through the C ABI with host buffers: per step, every chain's
+    # state goes from pinned host memory to the device in one batched call
+    # (dqmc_engine_set_chains), one sweep runs, and state plus accumulators
+    # come back in one call (dqmc_engine_get_chains); the downloaded state is
+    # the next step's input
     e2e_steps = 2
-    h2d = d2h = 0
     eng.pull()          # host copies of the state the device now holds
+
+    def pinned(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+
+    el_h, dl_h, rg_h, hs_h = (pinned(a) for a in eng.state_arrays())
+    rg_o, hs_o = pinned(np.zeros_like(rg_h)), pinned(np.zeros_like(hs_h))
+    eqn_o = pinned(np.zeros(nch, np.int32))
+    eq_o = pinned(np.zeros((nch,) + sims[0].eq_acc.shape, sims[0].eq_acc.dtype))
+    sweep = sims[0].sweep
+    h2d = el_h.nbytes + dl_h.nbytes + rg_h.nbytes + hs_h.nbytes
+    d2h = rg_o.nbytes + hs_o.nbytes + eqn_o.nbytes + eq_o.nbytes
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for k in range(e2e_steps):
-        for c, s in enumerate(sims):
-            lib.check(L.dqmc_engine_set_chain(eng.h, c, s.exp_lambda.ctypes.data,
-                                              s.del_.ctypes.data, s.rng.ctypes.data,
-                                              s.hs.ctypes.data, s.sweep), "set_chain")
-        log(f"e2e step {k}: state uploaded")
-        h2d = sum(s.exp_lambda.nbytes + s.del_.nbytes + s.rng.nbytes + s.hs.nbytes for s in sims)
+        eng.set_chains(el_h, dl_h, rg_h, hs_h, sweep)
         eng.sweeps(1, sync=True)
-        log(f"e2e step {k}: sweep done")
-        eng.pull()
-        log(f"e2e step {k}: state downloaded")
-        d2h = sum(s.rng.nbytes + s.hs.nbytes + s.eq_acc.nbytes + 8 for s in sims)
+        sweep = eng.get_chains(rg_o, hs_o, eqn_o, eq_o)
+        rg_h, rg_o = rg_o, rg_h
+        hs_h, hs_o = hs_o, hs_h
     t_e2e = max_over_ranks((time.perf_counter() - t0) / e2e_steps, world)
     e2e = nch * world / t_e2e
 

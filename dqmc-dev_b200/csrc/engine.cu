@@ -576,6 +576,11 @@ struct GroupBase {
 	virtual int set_chain(int c, const double *el, const double *del, const uint64_t *rng,
 	                      const int *hs, int sweep) = 0;
 	virtual int set_acc(int c, int eqn, const void *eq, int uen, const void *ue) = 0;
+	// chains [c0, c0 + n) at once, host arrays contiguous over those chains
+	virtual int set_chains(int c0, int n, const double *el, const double *del, const uint64_t *rng,
+	                       const int *hs, int sweep) = 0;
+	virtual int get_chains(int c0, int n, uint64_t *rng, int *hs, int *sweep, int *eqn, void *eq,
+	                       int *uen, void *ue) = 0;
 	virtual int init() = 0;
 	virtual int sweeps(int n, int sync) = 0;
 	virtual int get_chain(int c, uint64_t *rng, int *hs, int *sweep) = 0;
@@ -746,6 +751,42 @@ struct Group : GroupBase, ProfHook {
 		sweep = sw;
 		need_draws = true;
 		need_init = true;
+		return 0;
+	}
+
+	int set_chains(int c0, int n, const double *e, const double *d, const uint64_t *r, const int *h,
+	               int sw) override
+	{
+		if (c0 < 0 || n < 0 || c0 + n > C) return DQMC_E_ARG;
+		if (n == 0) return 0;
+		// stream-ordered after the queued sweeps that read these buffers
+		CK(cudaMemcpyAsync(el.p + (size_t)c0 * 2 * N, e, sizeof(double) * 2 * N * n, cudaMemcpyHostToDevice, st));
+		CK(cudaMemcpyAsync(del.p + (size_t)c0 * 2 * N, d, sizeof(double) * 2 * N * n, cudaMemcpyHostToDevice, st));
+		CK(cudaMemcpyAsync(rng.p + (size_t)c0 * 17, r, sizeof(uint64_t) * 17 * n, cudaMemcpyHostToDevice, st));
+		CK(cudaMemcpyAsync(hs.p + (size_t)c0 * L * N, h, sizeof(int) * L * N * n, cudaMemcpyHostToDevice, st));
+		CK(cudaStreamSynchronize(st));
+		sweep = sw;
+		need_draws = true;
+		need_init = true;
+		return 0;
+	}
+
+	int get_chains(int c0, int n, uint64_t *r, int *h, int *sw, int *eqn, void *eq, int *uen,
+	               void *uea) override
+	{
+		if (c0 < 0 || n < 0 || c0 + n > C) return DQMC_E_ARG;
+		if (sw) *sw = sweep;
+		if (n == 0) return 0;
+		// the state at the sweep boundary, before the look-ahead draws
+		if (r) CK(cudaMemcpyAsync(r, rng_ckpt.p + (size_t)c0 * 17, sizeof(uint64_t) * 17 * n, cudaMemcpyDeviceToHost, st));
+		if (h) CK(cudaMemcpyAsync(h, hs.p + (size_t)c0 * L * N, sizeof(int) * L * N * n, cudaMemcpyDeviceToHost, st));
+		if (eqn) CK(cudaMemcpyAsync(eqn, n_eq.p + c0, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
+		if (eq) CK(cudaMemcpyAsync(eq, acc_eq.p + (size_t)c0 * eq_size, sizeof(T) * eq_size * n, cudaMemcpyDeviceToHost, st));
+		if (ue_size) {
+			if (uen) CK(cudaMemcpyAsync(uen, n_ue.p + c0, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
+			if (uea) CK(cudaMemcpyAsync(uea, acc_ue.p + (size_t)c0 * ue_size, sizeof(T) * ue_size * n, cudaMemcpyDeviceToHost, st));
+		}
+		CK(cudaStreamSynchronize(st));
 		return 0;
 	}
 
@@ -1477,6 +1518,9 @@ struct Lanes : GroupBase {
 	cudaStream_t st = nullptr;
 	size_t s_elems = 0;           // N * N entries of T per spin (gradient outputs)
 	size_t elem = 0;              // sizeof(T)
+	size_t n_site = 0, hs_len = 0;          // N and L N per chain
+	size_t eq_bytes = 0, ue_bytes = 0;      // accumulator bytes per chain
+	int c0s() const { return c0.back(); }
 
 	~Lanes() override
 	{
@@ -1490,6 +1534,12 @@ struct Lanes : GroupBase {
 		n_lane = std::max(1, std::min(n_lane, n_chain));
 		s_elems = (size_t)p.N * p.N;
 		elem = p.cplx ? sizeof(zd) : sizeof(double);
+		n_site = (size_t)p.N;
+		hs_len = (size_t)p.L * p.N;
+		eq_bytes = elem * (size_t)eq_acc_size(p.num_i, p.num_ij);
+		ue_bytes = p.period_uneqlt > 0
+		                   ? elem * (size_t)ue_acc_size(p.num_ij, p.num_bb, p.L, p.meas_bond_corr)
+		                   : 0;
 		CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
 		ev.assign(n_lane + 1, nullptr);
 		for (auto &e : ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -1536,6 +1586,35 @@ struct Lanes : GroupBase {
 	{
 		const int k = lane(c);
 		return k < 0 ? DQMC_E_ARG : g[k]->set_acc(c, eqn, eq, uen, ue);
+	}
+	// every chain at once (first = 0, n = all): each lane its contiguous slice
+	int set_chains(int first, int n, const double *el, const double *del, const uint64_t *rng,
+	               const int *hs, int sweep) override
+	{
+		if (first != 0 || n != c0s()) return DQMC_E_ARG;
+		CK(cudaStreamSynchronize(st));
+		for (size_t k = 0; k < g.size(); k++) {
+			const size_t a = c0[k], m = c0[k + 1] - c0[k];
+			const int rc = g[k]->set_chains(0, (int)m, el + a * 2 * n_site, del + a * 2 * n_site,
+			                                rng + a * 17, hs + a * hs_len, sweep);
+			if (rc) return rc;
+		}
+		return 0;
+	}
+	int get_chains(int first, int n, uint64_t *rng, int *hs, int *sweep, int *eqn, void *eq, int *uen,
+	               void *ue) override
+	{
+		if (first != 0 || n != c0s()) return DQMC_E_ARG;
+		CK(cudaStreamSynchronize(st));
+		for (size_t k = 0; k < g.size(); k++) {
+			const size_t a = c0[k], m = c0[k + 1] - c0[k];
+			const int rc = g[k]->get_chains(
+				0, (int)m, rng ? rng + a * 17 : nullptr, hs ? hs + a * hs_len : nullptr, sweep,
+				eqn ? eqn + a : nullptr, eq ? (char *)eq + a * eq_bytes : nullptr, uen ? uen + a : nullptr,
+				ue ? (char *)ue + a * ue_bytes : nullptr);
+			if (rc) return rc;
+		}
+		return 0;
 	}
 	int get_chain(int c, uint64_t *rng, int *hs, int *sweep) override
 	{
@@ -1747,6 +1826,22 @@ int dqmc_engine_set_acc(dqmc_engine *e, int chain, int eq_n_sample, const void *
 {
 	if (!e) return DQMC_E_ARG;
 	return e->g->set_acc(chain, eq_n_sample, eq_acc, ue_n_sample, ue_acc);
+}
+
+int dqmc_engine_set_chains(dqmc_engine *e, const double *exp_lambda, const double *del,
+		const uint64_t *rng, const int *hs, int sweep)
+{
+	if (!e || !exp_lambda || !del || !rng || !hs) return DQMC_E_ARG;
+	const int n = ((Lanes *)e->g)->c0s();
+	return e->g->set_chains(0, n, exp_lambda, del, rng, hs, sweep);
+}
+
+int dqmc_engine_get_chains(dqmc_engine *e, uint64_t *rng, int *hs, int *sweep, int *eq_n_sample,
+		void *eq_acc, int *ue_n_sample, void *ue_acc)
+{
+	if (!e) return DQMC_E_ARG;
+	const int n = ((Lanes *)e->g)->c0s();
+	return e->g->get_chains(0, n, rng, hs, sweep, eq_n_sample, eq_acc, ue_n_sample, ue_acc);
 }
 
 int dqmc_engine_init(dqmc_engine *e) { return e ? e->g->init() : DQMC_E_ARG; }

@@ -226,6 +226,31 @@ class Engine:
                        "dqmc_engine_get_acc")
             s.eq_n, s.ue_n = en.value, un.value
 
+    def state_arrays(self):
+        """Contiguous host arrays of every chain's state, in chain order:
+        (exp_lambda [n, 2N], del [n, 2N], rng [n, 17], hs [n, L, N])."""
+        return (np.ascontiguousarray(np.stack([s.exp_lambda for s in self.sims])),
+                np.ascontiguousarray(np.stack([s.del_ for s in self.sims])),
+                np.ascontiguousarray(np.stack([s.rng for s in self.sims])),
+                np.ascontiguousarray(np.stack([s.hs for s in self.sims])))
+
+    def set_chains(self, exp_lambda, del_, rng, hs, sweep: int):
+        """Every chain's state from contiguous host arrays in one call
+        (dqmc_engine_set_chains)."""
+        _lib.check(self.lib.dqmc_engine_set_chains(self.h, exp_lambda.ctypes.data, del_.ctypes.data,
+                                                   rng.ctypes.data, hs.ctypes.data, int(sweep)),
+                   "dqmc_engine_set_chains")
+
+    def get_chains(self, rng, hs, eq_n, eq_acc, ue_n=None, ue_acc=None) -> int:
+        """Every chain's state and accumulators into contiguous host arrays
+        in one call (dqmc_engine_get_chains); returns the sweep counter."""
+        sw = np.zeros(1, np.int32)
+        p = lambda a: None if a is None else a.ctypes.data
+        _lib.check(self.lib.dqmc_engine_get_chains(self.h, p(rng), p(hs), p(sw), p(eq_n),
+                                                   p(eq_acc), p(ue_n), p(ue_acc)),
+                   "dqmc_engine_get_chains")
+        return int(sw[0])
+
     def g(self, c: int):
         s = self.sims[c]
         gu = np.zeros(s.N * s.N, s.nt)

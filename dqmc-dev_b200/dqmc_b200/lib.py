@@ -26,7 +26,8 @@ EXPORTS = [
     "dqmc_engine_destroy", "dqmc_engine_set_chain", "dqmc_engine_set_acc",
     "dqmc_engine_init", "dqmc_engine_sweeps", "dqmc_engine_sync", "dqmc_engine_errors",
     "dqmc_engine_get_chain", "dqmc_engine_get_acc", "dqmc_engine_get_g",
-    "dqmc_engine_accepts", "dqmc_engine_stream", "dqmc_engine_lanes", "dqmc_engine_launches_per_sweep",
+    "dqmc_engine_accepts", "dqmc_engine_stream", "dqmc_engine_lanes",
+    "dqmc_engine_set_chains", "dqmc_engine_get_chains", "dqmc_engine_launches_per_sweep",
     "dqmc_engine_profile_sweep", "dqmc_engine_logdet_grad", "dqmc_engine_obs_grad",
     "dqmc_gpu_gemm", "dqmc_gpu_calc_eq_g", "dqmc_gpu_update_delayed", "dqmc_gpu_mul_seq",
     "dqmc_gpu_calc_eq_g_noalloc",
@@ -81,6 +82,8 @@ def load(path: str | None = None):
         "dqmc_engine_accepts": (i, [vp, i, C.POINTER(C.c_longlong)]),
         "dqmc_engine_stream": (vp, [vp]),
         "dqmc_engine_lanes": (i, [vp]),
+        "dqmc_engine_set_chains": (i, [vp, vp, vp, vp, vp, i]),
+        "dqmc_engine_get_chains": (i, [vp, vp, vp, vp, vp, vp, vp, vp]),
         "dqmc_engine_launches_per_sweep": (i, [vp, i, i]),
         "dqmc_engine_profile_sweep": (i, [vp, i, i, C.POINTER(C.c_double), i]),
         "dqmc_engine_logdet_grad": (i, [vp, vp, vp]),

@@ -96,6 +96,22 @@ int dqmc_engine_set_chain(dqmc_engine *e, int chain, const double *exp_lambda,
 int dqmc_engine_set_acc(dqmc_engine *e, int chain, int eq_n_sample,
 		const void *eq_acc, int ue_n_sample, const void *ue_acc);
 
+/* Every chain's state at once (no counterpart in the reference, whose
+ * process holds one chain): the arrays of dqmc_engine_set_chain for all
+ * n_chain chains, contiguous in chain order: exp_lambda[n_chain][2N],
+ * del[n_chain][2N], rng[n_chain][17], hs[n_chain][L*N].  One copy per array
+ * and lane instead of one call per chain.  G is recomputed before the next
+ * sweep, as after dqmc_engine_set_chain. */
+int dqmc_engine_set_chains(dqmc_engine *e, const double *exp_lambda,
+		const double *del, const uint64_t *rng, const int *hs, int sweep);
+/* Every chain's state and accumulators at once, the counterpart of
+ * dqmc_engine_get_chain plus dqmc_engine_get_acc for all chains: rng[n][17],
+ * hs[n][L*N], eq_n_sample[n], eq_acc[n][eq_size], ue_n_sample[n],
+ * ue_acc[n][ue_size] (the last two only with unequal-time measurements);
+ * any pointer may be NULL. */
+int dqmc_engine_get_chains(dqmc_engine *e, uint64_t *rng, int *hs, int *sweep,
+		int *eq_n_sample, void *eq_acc, int *ue_n_sample, void *ue_acc);
+
 /* Computes the initial G of every chain (dqmc.c:188-220). */
 int dqmc_engine_init(dqmc_engine *e);
 

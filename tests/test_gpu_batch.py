@@ -159,3 +159,48 @@ def test_lanes_gradients_match(mods, monkeypatch):
     (ld3, S3), (o3, Z3) = out[3]
     assert np.array_equal(ld1, ld3) and np.array_equal(S1, S3)
     assert np.array_equal(o1, o3) and np.array_equal(Z1, Z3)
+
+
+def test_batched_state_calls_match_per_chain(mods, monkeypatch):
+    """dqmc_engine_set_chains / get_chains (every chain in one call, lanes
+    split across) against dqmc_engine_set_chain / get_chain / get_acc chain
+    by chain: the same state in, bit-identical state and accumulators out."""
+    batch, engine, gen, simfile = mods
+    monkeypatch.setenv("DQMC_LANES", "2")
+    dicts = _group(gen, 5, Nx=4, Ny=4, U=4.0, dt=0.1, L=16, n_matmul=4, period_eqlt=4,
+                   n_delay=4, n_sweep_warm=1, n_sweep_meas=4)
+    one = [engine.SimData(dict(d)) for d in dicts]
+    e1 = engine.Engine(one)
+    e1.init()
+    e1.sweeps(2)
+    e1.pull()
+    # a second engine takes that state in one call and both run two more sweeps
+    two = [s.clone() for s in one]
+    e2 = engine.Engine(two)
+    assert e2.lanes() == 2
+    el, dl, rg, hs = e1.state_arrays()
+    e2.set_chains(el, dl, rg, hs, one[0].sweep)
+    for c, s in enumerate(one):
+        from dqmc_b200 import lib
+        lib.check(e1.lib.dqmc_engine_set_chain(e1.h, c, s.exp_lambda.ctypes.data, s.del_.ctypes.data,
+                                               s.rng.ctypes.data, s.hs.ctypes.data, s.sweep),
+                  "set_chain")
+        lib.check(e1.lib.dqmc_engine_set_acc(e1.h, c, 0, None, 0, None), "set_acc")
+        e2.lib.dqmc_engine_set_acc(e2.h, c, 0, None, 0, None)
+    e1.sweeps(2)
+    e2.sweeps(2)
+    e1.pull()
+    n = len(one)
+    rg2, hs2 = np.zeros_like(rg), np.zeros_like(hs)
+    eqn2 = np.zeros(n, np.int32)
+    eq2 = np.zeros((n,) + one[0].eq_acc.shape, one[0].eq_acc.dtype)
+    sw = e2.get_chains(rg2, hs2, eqn2, eq2)
+    assert sw == one[0].sweep
+    for c, s in enumerate(one):
+        assert np.array_equal(rg2[c], s.rng), c
+        assert np.array_equal(hs2[c], s.hs), c
+        assert eqn2[c] == s.eq_n, c
+        assert np.array_equal(eq2[c], s.eq_acc), c
+    assert e1.errors() == 0 and e2.errors() == 0
+    e1.close()
+    e2.close()
