@@ -1753,18 +1753,18 @@ struct Lanes : GroupBase {
 };
 
 // lanes of an engine of n_chain chains: DQMC_LANES when set, else one lane
-// per 64 chains, at most 4 (at 256 chains of 12 x 12, two lanes run 9% and
-// four 11% more chain-sweeps per second than one, eight no more than four;
-// 64 complex 10 x 10 chains run 3% faster in two lanes than in one, but
-// the gradients of 128 configurations of 8 x 8 run 182 evaluations/s in
-// two lanes, 173 in one and 72 in four)
-static int lane_count(int n_chain)
+// per 64 real or 32 complex chains, at most 4 (at 256 chains of 12 x 12,
+// two lanes run 9% and four 11% more chain-sweeps per second than one,
+// eight no more than four; 64 complex 10 x 10 chains run 3% faster in two
+// lanes than in one; the real gradients of 128 configurations of 8 x 8 run
+// 182 evaluations/s in two lanes, 173 in one and 72 in four)
+static int lane_count(int n_chain, bool cplx)
 {
 	if (const char *v = getenv("DQMC_LANES")) {
 		const int n = atoi(v);
 		if (n >= 1) return std::min(n, n_chain);
 	}
-	return std::max(1, std::min(4, n_chain / 64));
+	return std::max(1, std::min(4, n_chain / (cplx ? 32 : 64)));
 }
 
 }  // namespace dq
@@ -1798,7 +1798,7 @@ int dqmc_engine_create(const dqmc_params *p, int n_chain, int device, dqmc_engin
 	}
 	if (device >= 0 && cudaSetDevice(device) != cudaSuccess) return DQMC_E_CUDA;
 	auto *g = new Lanes();
-	const int rc = g->create(*p, n_chain, lane_count(n_chain));
+	const int rc = g->create(*p, n_chain, lane_count(n_chain, p->cplx != 0));
 	if (rc) {
 		delete g;
 		return rc;
