@@ -1,19 +1,24 @@
 """Benchmark: batched DQMC chain-sweeps/s on one node.
 
-Workload (per GPU): 256 independent chains of the single-band Hubbard model
-on a 12x12 square lattice (N = 144), t = 1, U = 4, mu = -1, beta = 6,
-dtau = 0.05 (L = 120), n_matmul = 10, n_delay = 16, equal-time measurements
-every 8 slices, FP64 throughout.  Chains differ by RNG stream (splitmix64 of
-the seed, one 2^512 jump per chain) and so by their HS fields.  A step is one
-sweep of every chain; value = chains x steps / device time.
+Default workload (per GPU): 256 independent chains of the single-band
+Hubbard model on a 12x12 square lattice (N = 144), t = 1, U = 4, mu = -1,
+beta = 6, dtau = 0.05 (L = 120), n_matmul = 10, n_delay = 16, equal-time
+measurements every 8 slices, FP64 throughout.  Chains differ by RNG stream
+(splitmix64 of the seed, one 2^512 jump per chain) and so by their HS
+fields.  A step is one sweep of every chain; value = chains x steps /
+device time.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload batch256|c1|uneq8x8|complex64|ragged64|grad128]
 
-With N > 1 (torchrun, one rank per GPU) each rank runs its own 256 chains
-(weak scaling, no collective on the data path); times are max over ranks.
-`--impl reference` times the reference's own C build (oracle/_ref/dqmc_1_r,
-the reference src/ compiled against OpenBLAS) on the host cores, as the
-reference deploys it: one process per two cores, two OpenMP threads each.
+With N > 1 each rank (one process per GPU; bench.py starts them itself
+through torch.distributed.run when WORLD_SIZE is unset) runs its own block
+of chains (weak scaling, no collective on the data path); times are the
+maximum over ranks.  `--impl reference` times the reference's own C build
+(oracle/_ref/dqmc_1_{r,c}, the reference src/ compiled against OpenBLAS) on
+the host cores, as the reference deploys it: one process per two cores, two
+OpenMP threads each.  The other workloads are the further benchmark
+configurations, one JSON line each.
 """
 from __future__ import annotations
 
@@ -21,6 +26,7 @@ import argparse
 import json
 import os
 import shutil
+import socket
 import subprocess
 import sys
 import tempfile
@@ -31,28 +37,60 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "dqmc-dev_b200"))
 
-CFG = dict(Nx=12, Ny=12, U=4.0, mu=-1.0, tp=0.0, dt=0.05, L=120, n_matmul=10, n_delay=16,
-           period_eqlt=8)
-CHAINS = 256
 SEED = 1000
 METRIC = "chain-sweeps/s"
-WORKLOAD = ("256 chains x 12x12 square Hubbard (N=144), U=4, mu=-1, beta=6, dtau=0.05 "
-            "(L=120), n_matmul=10, n_delay=16, eqlt every 8 slices, FP64")
 
+# single-parameter-set workloads: chains per GPU, generator arguments, the
+# description, and the reference build's sweeps per process for a bounded
+# CPU sample (about 5-30 s)
+WORKLOADS = {
+    "batch256": dict(
+        chains=256,
+        cfg=dict(Nx=12, Ny=12, U=4.0, mu=-1.0, tp=0.0, dt=0.05, L=120, n_matmul=10, n_delay=16,
+                 period_eqlt=8),
+        desc="256 chains x 12x12 square Hubbard (N=144), U=4, mu=-1, beta=6, dtau=0.05 "
+             "(L=120), n_matmul=10, n_delay=16, eqlt every 8 slices, FP64",
+        ref_sweeps=30),
+    "c1": dict(
+        chains=1,
+        cfg=dict(Nx=4, Ny=4, U=4.0, mu=0.0, tp=0.0, dt=0.1, L=40, n_matmul=5, n_delay=8,
+                 period_eqlt=8),
+        desc="1 chain x 4x4 square Hubbard, U=4, mu=0, beta=4, dtau=0.1 (L=40), n_matmul=5, "
+             "n_delay=8, eqlt every 8 slices, FP64 (the plain single-chain configuration)",
+        ref_sweeps=4000),
+    "uneq8x8": dict(
+        chains=1,
+        cfg=dict(Nx=8, Ny=8, tp=-0.25, U=6.0, mu=-0.5, dt=0.1, L=80, n_matmul=8, n_delay=16,
+                 period_eqlt=8, period_uneqlt=4),
+        desc="1 chain x 8x8 square Hubbard, t'=-0.25, U=6, mu=-0.5, beta=8, dtau=0.1 (L=80), "
+             "n_matmul=8, n_delay=16, eqlt every 8 slices, unequal-time every 4 sweeps, FP64",
+        ref_sweeps=200),
+    "complex64": dict(
+        chains=64,
+        cfg=dict(Nx=10, Ny=10, U=4.0, mu=0.0, dt=0.1, L=50, n_matmul=5, n_delay=16, nflux=1,
+                 period_eqlt=5, period_uneqlt=1, meas_bond_corr=1),
+        desc="64 chains x 10x10 square Hubbard with one flux quantum (Peierls phases, "
+             "complex128), U=4, mu=0, beta=5, dtau=0.1 (L=50), n_matmul=5, eqlt every 5 "
+             "slices, unequal-time with current-current bond correlators every sweep",
+        ref_sweeps=20),
+}
 
 # launch classes of the engine's per-launch profile whose algorithmic FLOPs
-# are counted (8/3 N^3 per item for the QRs with explicit Q and for the
-# recombine's LU solve, 2 M N K per GEMM), with the kernel behind each
+# are counted (2 M N K per GEMM; 8/3 N^3 per item for the QRs with explicit
+# Q and for the recombine's LU solve; the update's flush and panel products
+# from its accepts), with the kernel behind each
 ROOFLINE_KERNELS = {
     "gemm": "k_gemm (batched FP64 DMMA: wraps, cluster products, half wraps, UDT products)",
+    "update": "k_update (delayed rank-k Metropolis update: panel products and DMMA flush)",
     "qr_presort": "k_qrb (pre-sorted blocked Householder QR with explicit Q, calc_eq_g)",
     "qr_pivot": "k_qrp (column-pivoted Householder QR with explicit Q, calc_eq_g)",
     "recombine": "k_recb (LU solve G = (D_b^-1 Q^H + D_s T)^-1 D_b^-1 Q^H)",
 }
 # DRAM bytes (read + write) per chain-spin item of one launch, from ncu
-# captures of these kernels at 64 items on the same 12x12 model
-TRAFFIC_PER_ITEM = {"gemm": 172848, "qr_presort": 168068, "qr_pivot": 166916,
-                    "recombine": 333636}
+# captures of these kernels on the 12x12 model (profiles/), scaled by the
+# items of a launch; other workloads report null
+TRAFFIC_PER_ITEM = {"batch256": {"gemm": 172848, "qr_presort": 168068, "qr_pivot": 166916,
+                                 "recombine": 333636, "update": 170852}}
 
 T0 = time.time()
 
@@ -62,37 +100,49 @@ def log(msg):
     print(f"[bench {time.time() - T0:7.1f}s] {msg}", file=sys.stderr, flush=True)
 
 
-def sim_dicts(chains, seed, n_sweep):
-    """Sim data of the given global chains of the job: chain c starts from
-    the master stream of `seed` jumped c times (dqmc_b200.replicas)."""
-    from dqmc_b200 import gen, replicas
-    rngs = replicas.chain_streams(seed, chains)
-    d0 = gen.make_sim(init_rng=rngs[0], n_sweep_warm=0, n_sweep_meas=n_sweep, **CFG)
-    out = [d0]
-    N, L = CFG["Nx"] * CFG["Ny"], CFG["L"]
-    for r in rngs[1:]:
-        hs, rng = gen.initial_hs(r, L, N)
-        d = dict(d0)
-        d["state/init_rng"], d["state/rng"], d["state/hs"] = r, rng, hs
-        out.append(d)
-    return out
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
 
 
-def dist_setup(gpus):
+def spawn_ranks(gpus):
+    """`--gpus N` without a launcher: start N ranks of this same command
+    through torch.distributed.run (one process per GPU) and return its exit
+    status."""
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={gpus}", "--master-addr=127.0.0.1",
+           f"--master-port={_free_port()}", os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
+def dist_setup():
     rank, world = int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", 0))
     if world > 1:
         import datetime
 
+        import torch
         import torch.distributed as dist
-        dist.init_process_group("nccl" if gpus > 0 else "gloo",
+        dist.init_process_group("nccl" if torch.cuda.is_available() else "gloo",
                                 timeout=datetime.timedelta(seconds=600))
     return rank, world, local
 
 
+def dist_done(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def reduce_device():
+    import torch
+    return "cuda" if torch.cuda.is_available() else "cpu"
+
+
 def max_over_ranks(x, world):
     from dqmc_b200 import replicas
-    return replicas.max_over_ranks(x, world, device="cuda")
+    return replicas.max_over_ranks(x, world, device=reduce_device())
 
 
 def barrier(world):
@@ -174,11 +224,39 @@ def fp64_peak():
     return 2 * n ** 3 / best / 1e12
 
 
-def reference_rate(n_proc, sweeps, seed=1):
-    """Aggregate chain-sweeps/s of the reference C build: n_proc processes of
-    dqmc_1_r (2 OpenMP threads, OpenBLAS 1 thread) on independent chains."""
+# ---------------------------------------------------------------- inputs
+
+def _restream(base, rngs):
+    """copies of one sim dict with chain c's own RNG stream and fields"""
     from dqmc_b200 import gen
-    exe = os.path.join(ROOT, "oracle", "_ref", "dqmc_1_r")
+    N, L = int(base["params/N"]), int(base["params/L"])
+    out = [base]
+    for r in rngs[1:]:
+        hs, rng = gen.initial_hs(r, L, N)
+        d = dict(base)
+        d["state/init_rng"], d["state/rng"], d["state/hs"] = r, rng, hs
+        out.append(d)
+    return out
+
+
+def sim_dicts(wl, chains, n_sweep):
+    """Sim data of the given global chains of the job: chain c starts from
+    the master stream of SEED jumped c times (dqmc_b200.replicas)."""
+    from dqmc_b200 import gen, replicas
+    rngs = replicas.chain_streams(SEED, chains)
+    base = gen.make_sim(init_rng=rngs[0], n_sweep_warm=0, n_sweep_meas=n_sweep, **wl["cfg"])
+    return _restream(base, rngs)
+
+
+# ------------------------------------------------------- reference (CPU)
+
+def reference_rate(cfg, n_proc, sweeps, seed=1):
+    """Aggregate chain-sweeps/s of the reference C build: n_proc processes of
+    dqmc_1_{r,c} (2 OpenMP threads, OpenBLAS 1 thread) on independent chains
+    of the model `cfg`."""
+    from dqmc_b200 import gen
+    cplx = cfg.get("nflux", 0) != 0
+    exe = os.path.join(ROOT, "oracle", "_ref", "dqmc_1_c" if cplx else "dqmc_1_r")
     if not os.path.exists(exe):
         raise RuntimeError(f"reference build missing: {exe}")
     tmp = tempfile.mkdtemp()
@@ -186,7 +264,7 @@ def reference_rate(n_proc, sweeps, seed=1):
     os.chdir(tmp)
     try:
         paths = gen.create_batch(Nfiles=n_proc, prefix="ref", seed=seed, n_sweep_warm=0,
-                                 n_sweep_meas=sweeps, **CFG)
+                                 n_sweep_meas=sweeps, **cfg)
         env = dict(os.environ, OPENBLAS_NUM_THREADS="1", OMP_NUM_THREADS="2")
         t0 = time.perf_counter()
         procs = [subprocess.Popen([exe, "-b", "-l", f"{p}.log", p], env=env,
@@ -202,26 +280,51 @@ def reference_rate(n_proc, sweeps, seed=1):
     return n_proc * sweeps / t, t
 
 
+def cpu_procs():
+    return max(1, (os.cpu_count() or 2) // 2)
+
+
+def ref_sample(wl, n_proc, sweeps, t):
+    cplx = wl["cfg"].get("nflux", 0) != 0
+    c = wl["cfg"]
+    return (f"{n_proc} processes of the reference dqmc_1_{'c' if cplx else 'r'} x {sweeps} "
+            f"sweeps of one {c['Nx']}x{c['Ny']} L={c['L']} chain each (2 OpenMP threads, "
+            f"OpenBLAS 1 thread), {t:.1f} s")
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return
-    cores = os.cpu_count() or 2
-    n_proc = max(1, cores // 2)
-    sweeps = max(1, args.steps)
-    rate, t = reference_rate(n_proc, sweeps)
+    if args.workload == "grad128":
+        from_grad = grad_cpu_baseline()
+        print(json.dumps({
+            "metric": "grad evals/s", "value": from_grad["value"], "unit": "grad evals/s",
+            "n_gpus": args.gpus, "steps": 1, "warmup": 0, "ms_per_step": 1e3 / from_grad["value"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": GRAD_DESC, "cpu": True}, "cpu_baseline": from_grad,
+            "e2e": {"value": from_grad["value"], "unit": "grad evals/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}))
+        return
+    wl = WORKLOADS.get(args.workload, WORKLOADS["batch256"])
+    n_proc = cpu_procs()
+    sweeps = max(1, args.steps) * max(1, wl["ref_sweeps"] // 30)
+    rate, t = reference_rate(wl["cfg"], n_proc, sweeps)
     line = {
         "metric": METRIC, "value": rate, "unit": METRIC, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * t / sweeps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "c128" if wl["cfg"].get("nflux", 0) else "f64", "data": "synthetic",
         "impl": "reference",
-        "config": {"workload": WORKLOAD, "chains": n_proc, "cpu": True},
+        "config": {"workload": wl["desc"], "chains": n_proc, "cpu": True},
         "cpu_baseline": {"value": rate, "unit": METRIC, "cores": n_proc * 2, "kind": "reference",
-                         "sample": f"{n_proc} dqmc_1_r processes x {sweeps} sweeps of one "
-                                   f"12x12 L=120 chain each (2 OpenMP threads, OpenBLAS 1 thread)"},
+                         "sample": ref_sample(wl, n_proc, sweeps, t)},
         "e2e": {"value": rate, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
 
+
+# ----------------------------------------------------------- GPU helpers
 
 def plain_chain_rate(sim, device, warm=2, timed=3):
     """chain-sweeps/s of the plain single-chain GPU path: one chain of the
@@ -246,8 +349,179 @@ def plain_chain_rate(sim, device, warm=2, timed=3):
         e.close()
 
 
-# further workloads of the benchmark configurations, one JSON line each:
-# builder(n_sweep) -> list of sim dicts, description
+def profile_mix(eng, period_uneqlt):
+    """Per-class (ms, launches, flops, bytes) of an average sweep: one eager
+    equal-time sweep, and with unequal-time measurements every p sweeps one
+    such sweep too, weighted (p - 1) / p and 1 / p."""
+    prof = eng.profile_sweep(True, False)
+    if period_uneqlt <= 0:
+        return prof
+    ue = eng.profile_sweep(True, True)
+    w = 1.0 / period_uneqlt
+    return {k: tuple((1 - w) * a + w * b for a, b in zip(prof[k], ue[k])) for k in prof}
+
+
+def roofline(prof, items, workload, peak, ms_per_step):
+    """The dominant launch class by event time among those with counted
+    FLOPs: its FLOPs over its time against the FP64 DGEMM peak, and the
+    whole sweep's FLOPs over the timed sweep."""
+    cls = [k for k in ROOFLINE_KERNELS if prof[k][0] > 0 and prof[k][2] > 0]
+    dom = max(cls, key=lambda k: prof[k][0])
+    d_ms, d_n, d_fl, _ = prof[dom]
+    achieved = d_fl / (d_ms / 1e3) / 1e12
+    traffic = TRAFFIC_PER_ITEM.get(workload, {}).get(dom)
+    sweep_fl = sum(prof[k][2] for k in ROOFLINE_KERNELS)
+    sweep_tf = sweep_fl / (ms_per_step / 1e3) / 1e12
+    return {"bound": "tensor", "kernel": ROOFLINE_KERNELS[dom], "class": dom,
+            "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": achieved / peak if peak else None,
+            "traffic": traffic * items if traffic else None,
+            "traffic_unit": "bytes per launch (DRAM read + write)",
+            "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json "
+                           "carries no FP64 figure)",
+            "launches_per_sweep": int(round(d_n)),
+            "ms_per_launch": d_ms / d_n if d_n else None,
+            "class_ms_per_sweep": {k: prof[k][0] for k in prof},
+            "class_tflops": {k: prof[k][2] / (prof[k][0] / 1e3) / 1e12
+                             for k in ROOFLINE_KERNELS if prof[k][0] > 0 and prof[k][2] > 0},
+            "sweep": {"flops": sweep_fl, "achieved": sweep_tf,
+                      "frac": sweep_tf / peak if peak else None,
+                      "note": "counted FLOPs of every class over the timed ms_per_step"}}
+
+
+def e2e_rate(eng, sims, steps, world):
+    """chain-sweeps/s through the C ABI with host buffers: per step, every
+    chain's state goes from pinned host memory to the device in one batched
+    call (dqmc_engine_set_chains), one sweep runs, and state plus
+    accumulators come back in one call (dqmc_engine_get_chains); the
+    downloaded state is the next step's input."""
+    import torch
+    eng.pull()          # host copies of the state the device now holds
+    n = len(sims)
+
+    def pinned(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+
+    el_h, dl_h, rg_h, hs_h = (pinned(a) for a in eng.state_arrays())
+    rg_o, hs_o = pinned(np.zeros_like(rg_h)), pinned(np.zeros_like(hs_h))
+    eqn_o = pinned(np.zeros(n, np.int32))
+    eq_o = pinned(np.zeros((n,) + sims[0].eq_acc.shape, sims[0].eq_acc.dtype))
+    ue = sims[0].p["period_uneqlt"] > 0
+    uen_o = pinned(np.zeros(n, np.int32)) if ue else None
+    ue_o = pinned(np.zeros((n,) + sims[0].ue_acc.shape, sims[0].ue_acc.dtype)) if ue else None
+    sweep = sims[0].sweep
+    h2d = el_h.nbytes + dl_h.nbytes + rg_h.nbytes + hs_h.nbytes
+    d2h = rg_o.nbytes + hs_o.nbytes + eqn_o.nbytes + eq_o.nbytes
+    if ue:
+        d2h += uen_o.nbytes + ue_o.nbytes
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        eng.set_chains(el_h, dl_h, rg_h, hs_h, sweep)
+        eng.sweeps(1, sync=True)
+        sweep = eng.get_chains(rg_o, hs_o, eqn_o, eq_o, uen_o, ue_o)
+        rg_h, rg_o = rg_o, rg_h
+        hs_h, hs_o = hs_o, hs_h
+    t = max_over_ranks((time.perf_counter() - t0) / steps, world)
+    return {"value": n * world / t, "unit": METRIC, "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "steps": steps}
+
+
+def run_engine_workload(args, rank, world, local):
+    """One parameter set of chains in one engine: K graph-replayed sweeps
+    timed with CUDA events on the engine's stream, then the end-to-end leg,
+    a per-launch profile, the roofline, and the reference build's rate."""
+    import torch
+    torch.cuda.set_device(local)
+    from dqmc_b200 import engine, replicas
+    wl = WORKLOADS[args.workload]
+    nch = args.chains if args.chains else wl["chains"]
+    e2e_steps = max(10, args.e2e_steps)
+    total = args.warmup + args.steps + e2e_steps + 4
+    dicts = sim_dicts(wl, replicas.shard(nch * world, rank, world), n_sweep=total)
+    log(f"generated {nch} chains")
+    sims = [engine.SimData(d) for d in dicts]
+    eng = engine.Engine(sims, device=local)
+    eng.init()
+    log("initial G done")
+    stream = torch.cuda.ExternalStream(eng.stream())
+    pu = sims[0].p["period_uneqlt"]
+
+    # warm-up (also captures the sweep graphs of every kind the timed run uses)
+    for _ in range(args.warmup):
+        eng.sweeps(1, sync=True)
+    log("warm-up done")
+
+    barrier(world)
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        eng.sweeps(args.steps, sync=False)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    t_dev = ev0.elapsed_time(ev1) / 1e3
+    assert eng.errors() == 0, "device error word set"
+    t_max = max_over_ranks(t_dev, world)
+    log(f"timed sweeps done: {1e3 * t_dev / args.steps:.2f} ms per sweep")
+    value = nch * args.steps * world / t_max
+    kinds = [eng.launches_per_sweep(True, False)]
+    if pu > 0:
+        kinds.append(eng.launches_per_sweep(True, True))
+    launches = int(round(args.steps * (kinds[0] * (1 - 1 / pu) + kinds[1] / pu))) if pu > 0 \
+        else kinds[0] * args.steps
+
+    e2e = e2e_rate(eng, sims, e2e_steps, world)
+    log("e2e done")
+    prof = profile_mix(eng, pu)
+    log("profile sweep done")
+    peak = fp64_peak()
+    items = 2 * nch / eng.lanes()      # chain-spin items of one launch (lane)
+    rl = roofline(prof, items, args.workload, peak, 1e3 * t_max / args.steps)
+
+    plain = None
+    if args.workload == "batch256":
+        plain = plain_chain_rate(sims[0], local)
+        log("plain single-chain sweeps done")
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            n_proc = cpu_procs()
+            rate, t = reference_rate(wl["cfg"], n_proc, wl["ref_sweeps"])
+            log("cpu baseline done")
+            cpu = {"value": rate, "unit": METRIC, "cores": 2 * n_proc, "kind": "reference",
+                   "sample": ref_sample(wl, n_proc, wl["ref_sweeps"], t)}
+        except Exception as ex:  # noqa: BLE001
+            cpu = {"value": None, "unit": METRIC, "cores": 0, "kind": "reference",
+                   "sample": f"not run: {ex}"}
+
+    if rank == 0:
+        cfg = {"workload": wl["desc"], "chains_per_gpu": nch, "lanes": eng.lanes(),
+               "l2": "inputs larger than L2" if nch * 2 * 20 * sims[0].N ** 2 * 8 > 126e6
+                     else "inputs fit L2 (one small chain): L2 is not flushed",
+               "sweep_profile_note": "kernel ms per class over one eager sweep with each lane "
+                                     "profiled alone, lanes one after another; the timed sweeps "
+                                     "overlap the lanes, so the sum can exceed ms_per_step"}
+        if plain is not None:
+            cfg["plain_1chain_gpu"] = {"value": plain, "unit": METRIC,
+                                       "batched_over_plain": value / world / plain}
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "c128" if sims[0].cplx else "f64", "data": "synthetic",
+            "config": cfg, "gpu_launches": launches, "e2e": e2e, "roofline": rl,
+            "clocks": clk.summary(), "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    eng.close()
+
+
+# ------------------------------------------------------ ragged and grad
+
 def _ragged64(n_sweep):
     from dqmc_b200 import gen
     return gen.make_ragged(64, SEED, n_sweep_warm=0, n_sweep_meas=n_sweep, period_eqlt=10), (
@@ -256,40 +530,71 @@ def _ragged64(n_sweep):
         "autotuned per lattice size, eqlt every 10 slices, FP64")
 
 
-def _complex64(n_sweep):
-    from dqmc_b200 import gen, replicas
-    rngs = replicas.chain_streams(SEED, range(64))
-    base = gen.make_sim(Nx=10, Ny=10, U=4.0, mu=0.0, dt=0.1, L=50, n_matmul=5, n_delay=16,
-                        nflux=1, period_eqlt=5, period_uneqlt=1, meas_bond_corr=1,
-                        n_sweep_warm=0, n_sweep_meas=n_sweep, init_rng=rngs[0])
-    return _restream(base, rngs, 100, 50), (
-        "64 chains x 10x10 square Hubbard with one flux quantum (Peierls phases, complex128), "
-        "U=4, mu=0, beta=5, dtau=0.1 (L=50), n_matmul=5, eqlt every 5 slices, unequal-time "
-        "(with current-current bond correlators) every sweep")
+def run_ragged(args, rank, world, local):
+    """The ragged mix as parameter groups (one engine and stream each): K
+    sweeps of every chain, timed on the host around synchronised sweeps
+    because several streams take part."""
+    import torch
+    torch.cuda.set_device(local)
+    from dqmc_b200 import batch
+    from dqmc_b200 import engine
+    dicts, desc = _ragged64(args.warmup + args.steps + 2)
+    sims = [engine.SimData(d) for d in dicts]
+    log(f"generated {len(sims)} chains")
+    rb = batch.RaggedBatch(sims, device=local, autotune=True)
+    rb.init()
+    rb.sweeps(args.warmup)
+    barrier(world)
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        t0 = time.perf_counter()
+        rb.sweeps(args.steps)
+        torch.cuda.synchronize()
+        t = time.perf_counter() - t0
+    barrier(world)
+    assert rb.errors() == 0, "device error word set"
+    t_max = max_over_ranks(t, world)
+    launches = sum(e.launches_per_sweep(True, False) for e in rb.engines) * args.steps
+    rb.close()
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": len(sims) * args.steps * world / t_max, "unit": METRIC,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": desc, "chains_per_gpu": len(sims), "groups": len(rb.groups),
+                       "delay_rank": {str(k): v for k, v in rb.delay.items()},
+                       "timing": "host clock around device-synchronised sweeps (several streams)"},
+            "gpu_launches": launches, "e2e": None, "roofline": None,
+            "clocks": clk.summary(), "cpu_baseline": None,
+        }))
 
 
-def _uneq8x8(n_sweep):
-    from dqmc_b200 import gen, replicas
-    rngs = replicas.chain_streams(SEED, range(1))
-    return [gen.make_sim(Nx=8, Ny=8, tp=-0.25, U=6.0, mu=-0.5, dt=0.1, L=80, n_matmul=8,
-                         n_delay=16, period_eqlt=8, period_uneqlt=4, n_sweep_warm=0,
-                         n_sweep_meas=n_sweep, init_rng=rngs[0])], (
-        "1 chain x 8x8 square Hubbard, t'=-0.25, U=6, mu=-0.5, beta=8, dtau=0.1 (L=80), "
-        "n_matmul=8, n_delay=16, eqlt every 8 slices, unequal-time every 4 sweeps, FP64")
+GRAD_DESC = ("128 fixed HS field configurations, 8x8 square, t=1, t'=-0.2, U=4, mu=-0.3, "
+             "beta=4, dtau=0.1 (L=40); one grad eval = log|det M_up M_dn|, <n>, <docc> and their "
+             "gradients in t, t', mu and 128 bond hoppings for one configuration")
 
 
-def _restream(base, rngs, N, L):
-    from dqmc_b200 import gen
-    out = [base]
-    for r in rngs[1:]:
-        hs, rng = gen.initial_hs(r, L, N)
-        d = dict(base)
-        d["state/init_rng"], d["state/rng"], d["state/hs"] = r, rng, hs
-        out.append(d)
-    return out
-
-
-EXTRA = {"ragged64": _ragged64, "complex64": _complex64, "uneq8x8": _uneq8x8, "grad128": None}
+def grad_cpu_baseline():
+    """the explicit fermion-matrix method on the host: one configuration
+    (two 2560 x 2560 inverses per quantity), scaled to grad evals/s"""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import fermion_matrix as fm
+    from dqmc_b200 import grad
+    draw = np.random.Generator(np.random.PCG64(SEED))
+    fields = draw.integers(0, 2, size=(1, 40, 64)).astype(np.int32)
+    m = grad.SquareModel(8, 8, U=4.0, dt=0.1, L=40, fields=fields, n_matmul=8)
+    theta = np.concatenate([[1.0, -0.2, -0.3], np.zeros(128)])
+    K = m.K(theta)
+    t0 = time.perf_counter()
+    fm.logdet_grad(K, m.dK, m.U, m.dt, m.L, fields[0])
+    fm.obs_grad(K, m.dK, m.U, m.dt, m.L, fields[0])
+    tc = time.perf_counter() - t0
+    return {"value": 1.0 / tc, "unit": "grad evals/s", "cores": os.cpu_count() or 1,
+            "kind": "port",
+            "sample": f"one configuration with the explicit N L x N L fermion matrices "
+                      f"(numpy/OpenBLAS, {os.cpu_count()} host threads): log-det, <n>, <docc> "
+                      f"and their 131-parameter gradients, {tc:.1f} s"}
 
 
 def run_grad(args, rank, world, local):
@@ -297,7 +602,8 @@ def run_grad(args, rank, world, local):
     (uniform +-1 from the seed) of the 8x8 model, t=1, t'=-0.2, U=4,
     mu=-0.3, beta=4, dtau=0.1 (L=40).  A step evaluates, for every
     configuration, log |det M_up M_dn|, <n> and <docc> and their gradients
-    with respect to t, t', mu and the 128 bond hoppings (131 parameters)."""
+    with respect to t, t', mu and the 128 bond hoppings (131 parameters),
+    through the public Python API (host arrays in, host arrays out)."""
     import torch
     torch.cuda.set_device(local)
     from dqmc_b200 import grad, replicas
@@ -323,76 +629,35 @@ def run_grad(args, rank, world, local):
     t_max = max_over_ranks(t, world)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        # the explicit fermion-matrix method on the host: one configuration
-        # (two 2560 x 2560 inverses per quantity), scaled to grad evals/s
-        sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        import fermion_matrix as fm
-        K = m.K(theta)
-        t0 = time.perf_counter()
-        fm.logdet_grad(K, m.dK, m.U, m.dt, m.L, fields[0])
-        fm.obs_grad(K, m.dK, m.U, m.dt, m.L, fields[0])
-        tc = time.perf_counter() - t0
-        cpu = {"value": 1.0 / tc, "unit": "grad evals/s",
-               "cores": os.cpu_count() or 1, "kind": "port",
-               "sample": f"one configuration with the explicit N L x N L fermion matrices "
-                         f"(numpy/OpenBLAS, {os.cpu_count()} host threads): log-det, <n>, "
-                         f"<docc> and their 131-parameter gradients, {tc:.1f} s"}
+        cpu = grad_cpu_baseline()
+    value = n_cfg * args.steps * world / t_max
+    h2d = fields.nbytes + theta.nbytes
+    d2h = n_cfg * (3 + 3 * 131) * 8
     if rank == 0:
         print(json.dumps({
-            "metric": "grad evals/s", "value": n_cfg * args.steps * world / t_max,
+            "metric": "grad evals/s", "value": value,
             "unit": "grad evals/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "128 fixed HS field configurations, 8x8 square, t=1, t'=-0.2, "
-                                   "U=4, mu=-0.3, beta=4, dtau=0.1 (L=40); one grad eval = "
-                                   "log|det M_up M_dn|, <n>, <docc> and their gradients in t, t', "
-                                   "mu and 128 bond hoppings for one configuration",
-                       "timing": "host clock around the complete evaluations (device sweeps, "
-                                 "space-time Green's functions, host contractions)"},
-            "gpu_launches": None, "e2e": None, "roofline": None,
-            "clocks": clk.summary(), "cpu_baseline": cpu,
+            "config": {"workload": GRAD_DESC,
+                       "timing": "host clock around the complete evaluations through the public "
+                                 "API (host fields and parameters in, host values and gradients "
+                                 "out)"},
+            "gpu_launches": None,
+            "e2e": {"value": value, "unit": "grad evals/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h,
+                    "note": "the value itself is measured end to end on the host clock"},
+            "roofline": None, "clocks": clk.summary(), "cpu_baseline": cpu,
         }))
 
 
-def run_extra(args, rank, world, local):
-    """One of the further benchmark workloads as a ragged batch (one engine
-    and stream per parameter group): K sweeps of every chain, timed on the
-    host around synchronised sweeps because several streams take part."""
-    import torch
-    torch.cuda.set_device(local)
-    from dqmc_b200 import batch, engine
-    dicts, desc = EXTRA[args.workload](args.warmup + args.steps + 2)
-    sims = [engine.SimData(d) for d in dicts]
-    log(f"generated {len(sims)} chains")
-    rb = batch.RaggedBatch(sims, device=local, autotune=args.workload == "ragged64")
-    rb.init()
-    rb.sweeps(args.warmup)
+def launch_check(rank, world):
+    """The multi-rank plumbing alone (used by the CPU tests): every rank
+    joins, the maximum over ranks is taken, rank 0 reports the world."""
+    m = max_over_ranks(float(rank), world)
     barrier(world)
-    torch.cuda.synchronize()
-    with Clocks(local) as clk:
-        t0 = time.perf_counter()
-        rb.sweeps(args.steps)
-        torch.cuda.synchronize()
-        t = time.perf_counter() - t0
-    barrier(world)
-    assert rb.errors() == 0, "device error word set"
-    t_max = max_over_ranks(t, world)
-    launches = sum(max(e.launches_per_sweep(True, False), e.launches_per_sweep(True, True))
-                   for e in rb.engines) * args.steps
-    rb.close()
     if rank == 0:
-        print(json.dumps({
-            "metric": METRIC, "value": len(sims) * args.steps * world / t_max, "unit": METRIC,
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None,
-            "dtype": "c128" if sims[0].cplx else "f64", "data": "synthetic",
-            "config": {"workload": desc, "chains_per_gpu": len(sims), "groups": len(rb.groups),
-                       "delay_rank": {str(k): v for k, v in rb.delay.items()},
-                       "timing": "host clock around device-synchronised sweeps (several streams)"},
-            "gpu_launches": launches, "e2e": None, "roofline": None,
-            "clocks": clk.summary(), "cpu_baseline": None,
-        }))
+        print(json.dumps({"n_gpus": world, "max_rank": m}))
 
 
 def main():
@@ -401,159 +666,30 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--chains", type=int, default=CHAINS)
+    ap.add_argument("--chains", type=int, default=0, help="chains per GPU (0: the workload's)")
+    ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="batch256", choices=["batch256"] + sorted(EXTRA),
+    ap.add_argument("--workload", default="batch256",
+                    choices=sorted(WORKLOADS) + ["ragged64", "grad128"],
                     help="batch256: the headline (default); the others print their own line")
+    ap.add_argument("--launch-check", action="store_true", help=argparse.SUPPRESS)
     args = ap.parse_args()
-    rank, world, local = dist_setup(args.gpus)
-    if args.impl == "ours" and args.workload != "batch256":
-        (run_grad if args.workload == "grad128" else run_extra)(args, rank, world, local)
-        if world > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
-        return
-    if args.impl == "reference":
-        run_reference_arm(args, rank, world)
-        if world > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
-        return
-
-    import torch
-    torch.cuda.set_device(local)
-    from dqmc_b200 import engine, lib
-
-    nch = args.chains
-    total = args.warmup + args.steps + 4
-    # this rank's block of the job's nch * world chains (weak scaling)
-    from dqmc_b200 import replicas
-    dicts = sim_dicts(replicas.shard(nch * world, rank, world), seed=SEED, n_sweep=total)
-    log(f"generated {nch} chains")
-    sims = [engine.SimData(d) for d in dicts]
-    eng = engine.Engine(sims, device=local)
-    eng.init()
-    log("initial G done")
-    stream = torch.cuda.ExternalStream(eng.stream())
-
-    # warm-up (also captures the sweep graph)
-    for _ in range(args.warmup):
-        eng.sweeps(1, sync=True)
-        log("warm-up sweep done")
-
-    # timed region: K sweeps, device time on the engine's stream
-    barrier(world)
-    torch.cuda.synchronize()
-    with Clocks(local) as clk:
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        ev0.record(stream)
-        eng.sweeps(args.steps, sync=False)
-        ev1.record(stream)
-        torch.cuda.synchronize()
-    barrier(world)
-    t_dev = ev0.elapsed_time(ev1) / 1e3
-    assert eng.errors() == 0, "device error word set"
-    t_max = max_over_ranks(t_dev, world)
-    log(f"timed sweeps done: {1e3 * t_dev / args.steps:.1f} ms per sweep")
-    value = nch * args.steps * world / t_max
-    launches = eng.launches_per_sweep(True, False) * args.steps
-
-    # end to end through the C ABI with host buffers: per step, every chain's
-    # state goes from pinned host memory to the device in one batched call
-    # (dqmc_engine_set_chains), one sweep runs, and state plus accumulators
-    # come back in one call (dqmc_engine_get_chains); the downloaded state is
-    # the next step's input
-    e2e_steps = 2
-    eng.pull()          # host copies of the state the device now holds
-
-    def pinned(a):
-        return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
-
-    el_h, dl_h, rg_h, hs_h = (pinned(a) for a in eng.state_arrays())
-    rg_o, hs_o = pinned(np.zeros_like(rg_h)), pinned(np.zeros_like(hs_h))
-    eqn_o = pinned(np.zeros(nch, np.int32))
-    eq_o = pinned(np.zeros((nch,) + sims[0].eq_acc.shape, sims[0].eq_acc.dtype))
-    sweep = sims[0].sweep
-    h2d = el_h.nbytes + dl_h.nbytes + rg_h.nbytes + hs_h.nbytes
-    d2h = rg_o.nbytes + hs_o.nbytes + eqn_o.nbytes + eq_o.nbytes
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for k in range(e2e_steps):
-        eng.set_chains(el_h, dl_h, rg_h, hs_h, sweep)
-        eng.sweeps(1, sync=True)
-        sweep = eng.get_chains(rg_o, hs_o, eqn_o, eq_o)
-        rg_h, rg_o = rg_o, rg_h
-        hs_h, hs_o = hs_o, hs_h
-    t_e2e = max_over_ranks((time.perf_counter() - t0) / e2e_steps, world)
-    e2e = nch * world / t_e2e
-
-    log("e2e done")
-    # per-launch profile of one more sweep (eager launches with events)
-    prof = eng.profile_sweep(True, False)
-    log("profile sweep done")
-    peak = fp64_peak()
-    sweep_ms = {k: v[0] for k, v in prof.items()}
-    sweep_ms["sum"] = sum(v[0] for v in prof.values())
-    # the dominant kernel among the launch classes with counted FLOPs
-    dom = max(ROOFLINE_KERNELS, key=lambda k: prof[k][0])
-    d_ms, d_n, d_fl, d_by = prof[dom]
-    achieved = d_fl / (d_ms / 1e3) / 1e12 if d_ms > 0 else 0.0
-    items = 2 * nch / eng.lanes()      # chain-spin items of one launch (lane)
-    traffic = TRAFFIC_PER_ITEM.get(dom)
-
-    plain = plain_chain_rate(sims[0], local)
-    log("plain single-chain sweeps done")
-
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        try:
-            cores = os.cpu_count() or 2
-            n_proc = max(1, cores // 2)
-            rate, t = reference_rate(n_proc, 30)
-            log("cpu baseline done")
-            cpu = {"value": rate, "unit": METRIC, "cores": 2 * n_proc, "kind": "reference",
-                   "sample": f"{n_proc} processes of the reference dqmc_1_r x 30 sweeps of one "
-                             f"12x12 L=120 chain each, {t:.1f} s"}
-        except Exception as ex:  # noqa: BLE001
-            cpu = {"value": None, "unit": METRIC, "cores": 0, "kind": "reference",
-                   "sample": f"not run: {ex}"}
-
-    if rank == 0:
-        line = {
-            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "chains_per_gpu": nch, "lanes": eng.lanes(),
-                       "l2": "inputs larger than L2 (about 2.6 MB of matrices per chain-spin)",
-                       "sweep_profile_ms": sweep_ms,
-                       "sweep_profile_note": "kernel ms per class over one eager sweep with each "
-                                             "lane profiled alone, lanes one after another; the "
-                                             "timed sweeps overlap the lanes, so the sum exceeds "
-                                             "ms_per_step",
-                       "plain_1chain_gpu": {"value": plain, "unit": METRIC,
-                                            "batched_over_plain": value / world / plain
-                                            if plain else None}},
-            "gpu_launches": launches,
-            "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h},
-            "roofline": {"bound": "tensor", "kernel": ROOFLINE_KERNELS[dom],
-                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak if peak else None,
-                         "traffic": traffic * items if traffic else None,
-                         "traffic_unit": "bytes per launch (DRAM read + write)",
-                         "peak_source": "cuBLAS DGEMM 8192^3 measured in this run "
-                                        "(MEASURED_PEAKS.json carries no FP64 figure)",
-                         "launches_per_sweep": int(d_n),
-                         "ms_per_launch": d_ms / d_n if d_n else None},
-            "clocks": clk.summary(),
-            "cpu_baseline": cpu,
-        }
-        print(json.dumps(line))
-    eng.close()
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(spawn_ranks(args.gpus))
+    rank, world, local = dist_setup()
+    try:
+        if args.launch_check:
+            launch_check(rank, world)
+        elif args.impl == "reference":
+            run_reference_arm(args, rank, world)
+        elif args.workload == "grad128":
+            run_grad(args, rank, world, local)
+        elif args.workload == "ragged64":
+            run_ragged(args, rank, world, local)
+        else:
+            run_engine_workload(args, rank, world, local)
+    finally:
+        dist_done(world)
 
 
 if __name__ == "__main__":

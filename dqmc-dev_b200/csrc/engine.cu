@@ -5,7 +5,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
-#include <ctime>
+#include <chrono>
 #include <unistd.h>
 #include <cstring>
 #include <map>
@@ -15,9 +15,8 @@
 #include <vector>
 
 #include "dqmc_b200.h"
-#include "gemm.cuh"
+#include "launch.cuh"
 #include "meas.cuh"
-#include "qr.cuh"
 #include "update.cuh"
 #include "uneq.cuh"
 
@@ -38,62 +37,6 @@ static inline Addr per_spin(long long stride) { return Addr{0, stride, 2}; }
 
 // ------------------------------------------------------------------ launches
 
-template <typename T, int BM, int BN, int BK, int WM, int WN, int ST, int MODE>
-static int launch_gemm_mode(const GemmArgs<T> &g, cudaStream_t st)
-{
-	using Cfg = GemmCfg<T, BM, BN, BK, WM, WN, ST>;
-	static bool attr = false;
-	if (!attr) {
-		if (cudaFuncSetAttribute(k_gemm<T, BM, BN, BK, WM, WN, ST, MODE>,
-		                         cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM_MAX) != cudaSuccess)
-			return DQMC_E_ARG;
-		attr = true;
-	}
-	// the grid's z extent is at most 65535: larger batches take several launches
-	for (int b0 = 0; b0 < g.batch; b0 += 65535) {
-		GemmArgs<T> gc = g;
-		gc.b0 = b0;
-		dim3 grid((g.M + BM - 1) / BM, (g.N + BN - 1) / BN, min(65535, g.batch - b0));
-		k_gemm<T, BM, BN, BK, WM, WN, ST, MODE><<<grid, Cfg::THREADS, Cfg::smem_bytes(MODE, g.K), st>>>(gc);
-	}
-	return 0;
-}
-
-template <typename T, int BM, int BN, int BK, int WM, int WN, int ST>
-static int launch_gemm_cfg(const GemmArgs<T> &g, cudaStream_t st)
-{
-	switch (g.mode) {
-	case 0: return launch_gemm_mode<T, BM, BN, BK, WM, WN, ST, 0>(g, st);
-	case GM_A_DD: return launch_gemm_mode<T, BM, BN, BK, WM, WN, ST, GM_A_DD>(g, st);
-	case GM_B_ROWD: return launch_gemm_mode<T, BM, BN, BK, WM, WN, ST, GM_B_ROWD>(g, st);
-	case GM_B_COLD: return launch_gemm_mode<T, BM, BN, BK, WM, WN, ST, GM_B_COLD>(g, st);
-	case GM_B_IDENT: return launch_gemm_mode<T, BM, BN, BK, WM, WN, ST, GM_B_IDENT>(g, st);
-	case GM_A_UPPER | GM_B_GATHER:
-		return launch_gemm_mode<T, BM, BN, BK, WM, WN, ST, GM_A_UPPER | GM_B_GATHER>(g, st);
-	default: return DQMC_E_ARG;
-	}
-}
-
-// tile choice: least padded area, larger tiles on ties
-template <typename T>
-int launch_gemm(const GemmArgs<T> &g, cudaStream_t st)
-{
-	// the scale vectors and gather indices of these modes are staged per K
-	const bool k_staged = g.mode & (GM_A_DD | GM_B_ROWD | GM_B_GATHER);
-	if ((k_staged && g.K > 512) || g.M < 1 || g.N < 1 || g.K < 1 || g.batch < 1) return DQMC_E_ARG;
-	auto pad = [&](int t) { return (long long)((g.M + t - 1) / t * t) * ((g.N + t - 1) / t * t); };
-	const long long p64 = pad(64), p48 = pad(48), p32 = pad(32);
-	if constexpr (is_cplx<T>::value) {
-		if (p64 <= p48 && p64 <= p32) return launch_gemm_cfg<T, 64, 64, 8, 4, 2, 3>(g, st);
-		if (p48 <= p32) return launch_gemm_cfg<T, 48, 48, 8, 2, 2, 3>(g, st);
-		return launch_gemm_cfg<T, 32, 32, 8, 2, 2, 3>(g, st);
-	} else {
-		if (p64 <= p48 && p64 <= p32) return launch_gemm_cfg<T, 64, 64, 16, 2, 2, 3>(g, st);
-		if (p48 <= p32) return launch_gemm_cfg<T, 48, 48, 16, 2, 2, 3>(g, st);
-		return launch_gemm_cfg<T, 32, 32, 16, 2, 2, 4>(g, st);
-	}
-}
-
 template <typename T>
 static GemmArgs<T> gargs(int M, int N, int K, int batch, const T *A, Addr aA, int lda,
 		const T *B, Addr aB, int ldb, T *C, Addr aC, int ldc, T alpha = one<T>(),
@@ -109,85 +52,6 @@ static GemmArgs<T> gargs(int M, int N, int K, int batch, const T *A, Addr aA, in
 	g.aD = Addr{0, 0, 1};
 	g.aG = Addr{0, 0, 1};
 	return g;
-}
-
-// largest N the per-matrix factorisations (QR, recombine) support: the
-// shared-memory form while N x N fits there, the global-memory form (working
-// matrix in the caller's per-item workspace, L2-resident) up to 256
-template <typename T> constexpr int max_dense_n() { return 256; }
-
-// rows per lane of a warp column: 32 * RPL >= N
-#define DQ_RPL(X) X(32, 1) X(64, 2) X(96, 3) X(128, 4) X(160, 5) X(192, 6) X(224, 7) X(256, 8)
-
-// 226 KB leaves room for the kernels' static shared memory
-static const size_t SMEM_FIT = 226 * 1024;
-
-template <typename K, typename Args>
-static int launch_dense(K kern, const Args &a, size_t sm, size_t &attr, cudaStream_t st)
-{
-	if (sm > attr) {
-		if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
-			return DQMC_E_ARG;
-		attr = sm;
-	}
-	kern<<<a.batch, 512, sm, st>>>(a);
-	return 0;
-}
-
-template <typename T, int RPL, bool GM>
-static int launch_qr_rpl(const QrArgs<T> &a, cudaStream_t st)
-{
-	constexpr int NW = 16, NBK = 8;
-	if (a.mode == QR_PRESORT) {
-		static size_t attr = 0;
-		return launch_dense(k_qrb<T, NW, NBK, RPL, GM>, a, qrb_smem_bytes<T, NBK>(a.N, GM), attr, st);
-	}
-	static size_t attr = 0;
-	return launch_dense(k_qrp<T, NW, NBK, RPL, GM>, a, qrp_smem_bytes<T, NBK>(a.N, GM), attr, st);
-}
-
-template <typename T, bool GM>
-static int launch_qr_gm(const QrArgs<T> &a, cudaStream_t st)
-{
-#define X(NMAX, R) if (a.N <= NMAX) return launch_qr_rpl<T, R, GM>(a, st);
-	DQ_RPL(X)
-#undef X
-	return DQMC_E_ARG;
-}
-
-template <typename T>
-int launch_qr(const QrArgs<T> &a, cudaStream_t st)
-{
-	if (a.N < 1 || a.N > max_dense_n<T>()) return DQMC_E_ARG;
-	const size_t sm = a.mode == QR_PRESORT ? qrb_smem_bytes<T, 8>(a.N) : qrp_smem_bytes<T, 8>(a.N);
-	if (sm <= SMEM_FIT) return launch_qr_gm<T, false>(a, st);
-	if (!a.work) return DQMC_E_ARG;
-	return launch_qr_gm<T, true>(a, st);
-}
-
-template <typename T, int RPL, bool GM>
-static int launch_rec_rpl(const RecArgs<T> &a, cudaStream_t st)
-{
-	static size_t attr = 0;
-	return launch_dense(k_recb<T, 16, RPL, 3, GM>, a, recb_smem_bytes<T>(a.N, GM), attr, st);
-}
-
-template <typename T, bool GM>
-static int launch_rec_gm(const RecArgs<T> &a, cudaStream_t st)
-{
-#define X(NMAX, R) if (a.N <= NMAX) return launch_rec_rpl<T, R, GM>(a, st);
-	DQ_RPL(X)
-#undef X
-	return DQMC_E_ARG;
-}
-
-template <typename T>
-int launch_rec(const RecArgs<T> &a, cudaStream_t st)
-{
-	if (a.N < 1 || a.N > max_dense_n<T>()) return DQMC_E_ARG;
-	if (recb_smem_bytes<T>(a.N) <= SMEM_FIT) return launch_rec_gm<T, false>(a, st);
-	if (!a.work) return DQMC_E_ARG;
-	return launch_rec_gm<T, true>(a, st);
 }
 
 // ------------------------------------------------------- small helper kernels
@@ -537,23 +401,6 @@ __global__ void k_yhat(int N, int L, int NB, const T *Y, const double *dv, T *Yh
 	}
 }
 
-// The dynamic shared-memory limit of a kernel is one setting per function,
-// shared by every engine of the process: only ever raise it, so that a group
-// created later with smaller needs cannot shrink it below what an earlier
-// group's launches (and captured graphs) rely on.
-template <typename K>
-static cudaError_t raise_smem(K kern, size_t bytes)
-{
-	static std::mutex mu;
-	static std::map<const void *, size_t> cur;
-	std::lock_guard<std::mutex> lk(mu);
-	size_t &c = cur[(const void *)kern];
-	if (bytes <= c) return cudaSuccess;
-	const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-	if (e == cudaSuccess) c = bytes;
-	return e;
-}
-
 template <typename T>
 static cudaError_t update_attr(size_t bytes)
 {
@@ -615,7 +462,9 @@ struct Group : GroupBase, ProfHook {
 	int watchdog(const char *what)
 	{
 		if (!debug_sync) return 0;
-		const double t0 = (double)clock() / CLOCKS_PER_SEC;
+		// wall time: a CPU-time clock would run fast while other host
+		// threads (the gradient paths' lane threads) are busy
+		const auto t0 = std::chrono::steady_clock::now();
 		for (;;) {
 			const cudaError_t e = cudaStreamQuery(st);
 			if (e == cudaSuccess) return 0;
@@ -624,7 +473,7 @@ struct Group : GroupBase, ProfHook {
 				fflush(stderr);
 				_exit(4);
 			}
-			if ((double)clock() / CLOCKS_PER_SEC - t0 > 10.0) {
+			if (std::chrono::steady_clock::now() - t0 > std::chrono::seconds(10)) {
 				fprintf(stderr, "dqmc_b200 watchdog: %s (sweep %d) did not finish in 10 s\n", what, sweep);
 				fflush(stderr);
 				_exit(3);
@@ -747,6 +596,8 @@ struct Group : GroupBase, ProfHook {
 		CK(cudaMemcpy(el.p + (size_t)c * 2 * N, e, sizeof(double) * 2 * N, cudaMemcpyHostToDevice));
 		CK(cudaMemcpy(del.p + (size_t)c * 2 * N, d, sizeof(double) * 2 * N, cudaMemcpyHostToDevice));
 		CK(cudaMemcpy(rng.p + (size_t)c * 17, r, sizeof(uint64_t) * 17, cudaMemcpyHostToDevice));
+		// get_chain reports rng_ckpt: it must show the state just set
+		CK(cudaMemcpy(rng_ckpt.p + (size_t)c * 17, r, sizeof(uint64_t) * 17, cudaMemcpyHostToDevice));
 		CK(cudaMemcpy(hs.p + (size_t)c * L * N, h, sizeof(int) * L * N, cudaMemcpyHostToDevice));
 		sweep = sw;
 		need_draws = true;
@@ -763,6 +614,7 @@ struct Group : GroupBase, ProfHook {
 		CK(cudaMemcpyAsync(el.p + (size_t)c0 * 2 * N, e, sizeof(double) * 2 * N * n, cudaMemcpyHostToDevice, st));
 		CK(cudaMemcpyAsync(del.p + (size_t)c0 * 2 * N, d, sizeof(double) * 2 * N * n, cudaMemcpyHostToDevice, st));
 		CK(cudaMemcpyAsync(rng.p + (size_t)c0 * 17, r, sizeof(uint64_t) * 17 * n, cudaMemcpyHostToDevice, st));
+		CK(cudaMemcpyAsync(rng_ckpt.p + (size_t)c0 * 17, r, sizeof(uint64_t) * 17 * n, cudaMemcpyHostToDevice, st));
 		CK(cudaMemcpyAsync(hs.p + (size_t)c0 * L * N, h, sizeof(int) * L * N * n, cudaMemcpyHostToDevice, st));
 		CK(cudaStreamSynchronize(st));
 		sweep = sw;
@@ -1286,14 +1138,30 @@ struct Group : GroupBase, ProfHook {
 			draws(0);
 			need_draws = false;
 		}
+		// the update's work follows from its accepts: count them around the sweep
+		std::vector<int> acc0(C), acc1(C);
+		CK(cudaMemcpyAsync(acc0.data(), nacc.p, sizeof(int) * C, cudaMemcpyDeviceToHost, st));
+		CK(cudaStreamSynchronize(st));
 		profiling = true;
 		precs.clear();
 		int rc = enqueue_sweep(meq, mue);
 		profiling = false;
 		if (rc) return rc;
+		CK(cudaMemcpyAsync(acc1.data(), nacc.p, sizeof(int) * C, cudaMemcpyDeviceToHost, st));
 		CK(cudaStreamSynchronize(st));
 		sweep++;
 		for (int i = 0; i < ncls * 4; i++) out[i] = 0.0;
+		if (PC_UPDATE < ncls) {
+			// per accept and spin: one rank-1 column of the flush G += A B^T
+			// (2 N^2) and the two panel products of the new column (2 N k
+			// each, k = 0 .. kd-1 within a panel: 2 N (kd - 1) on average);
+			// G read and written once per slice, chain and spin
+			double a = 0.0;
+			for (int c = 0; c < C; c++) a += (double)(acc1[c] - acc0[c]);
+			const double cx = is_cplx<T>::value ? 4.0 : 1.0;
+			out[PC_UPDATE * 4 + 2] = 2.0 * cx * a * (2.0 * N * N + 2.0 * N * (kd - 1));
+			out[PC_UPDATE * 4 + 3] = 2.0 * 2.0 * sizeof(T) * (double)N * N * C * L;
+		}
 		// calc_eq_g records nest the gemm records: count gemms inside a
 		// calc_eq_g window only under class 2
 		for (size_t i = 0; i < precs.size(); i++) {
@@ -1303,8 +1171,10 @@ struct Group : GroupBase, ProfHook {
 			if (r.cls < ncls) {
 				out[r.cls * 4 + 0] += ms;
 				out[r.cls * 4 + 1] += 1;
-				out[r.cls * 4 + 2] += r.flops;
-				out[r.cls * 4 + 3] += r.bytes;
+				if (r.cls != PC_UPDATE) {
+					out[r.cls * 4 + 2] += r.flops;
+					out[r.cls * 4 + 3] += r.bytes;
+				}
 			}
 		}
 		for (cudaEvent_t e : pev) cudaEventDestroy(e);

@@ -142,7 +142,11 @@ int dqmc_engine_launches_per_sweep(dqmc_engine *e, int meas_eq, int meas_ue);
  * k = 0 total ms, 1 launches, 2 algorithmic FLOPs, 3 operand bytes, for the
  * launch classes c = 0 batched GEMM (calc_eq_g's included), 1 delayed
  * update, 2 column-pivoted QR, 3 unequal-time G (its GEMMs under 0),
- * 4 measurements, 5 pre-sorted QR, 6 recombine (LU solve of G). */
+ * 4 measurements, 5 pre-sorted QR, 6 recombine (LU solve of G).  The
+ * update's FLOPs are counted from the sweep's accepts: per accept and spin
+ * 2 N^2 (its column of the flush) + 2 N (n_delay - 1) (the panel products,
+ * on average), times 4 for complex; its bytes are one read and one write
+ * of G per slice, chain and spin. */
 int dqmc_engine_profile_sweep(dqmc_engine *e, int meas_eq, int meas_ue, double *out,
 		int n_class);
 
@@ -209,9 +213,11 @@ int dqmc_gpu_mul_seq(int batch, int N, int n, int spin, int cplx,
 		void *stream);
 
 /* Size of the fixed device scratch of dqmc_gpu_calc_eq_g_noalloc (16 MiB).
- * A call needs 6*batch*N*N*sizeof(num) + batch*N*12 + batch*sizeof(num)
- * bytes, each part rounded up to 256: e.g. up to 80 problems of N = 64 or
- * 16 problems of N = 144 (real), 13 problems of N = 112 (complex). */
+ * A call needs six parts of batch*N*N*sizeof(num) bytes, one of batch*N*8,
+ * one of batch*N*4, one of batch*sizeof(num) and 256 for the error word,
+ * each part rounded up to a multiple of 256.  That admits at most 84
+ * problems of N = 64 or 16 of N = 144 (real), and 17 of N = 100 or 13 of
+ * N = 112 (complex). */
 #define DQMC_NOALLOC_SCRATCH_BYTES (16 << 20)
 
 /* dqmc_gpu_calc_eq_g without any device allocation; no counterpart in the

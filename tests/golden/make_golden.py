@@ -1,7 +1,7 @@
 """Regenerate the golden fixtures under tests/golden/.
 
-Runs in the development container only (it reads the reference at
-REF_ROOT, default /root/reference):
+Runs where the reference checkout is present only (it reads it at
+$DQMC_REF_ROOT, default: a "reference" folder beside this repository):
 
 * sim inputs come from the reference generator util/gen_1band_unified_hub.py
   (create_batch), run with the h5py/git stand-ins in _stubs/ so that it writes
@@ -24,7 +24,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF_ROOT = os.environ.get("REF_ROOT", "/root/reference")
+REF_ROOT = os.environ.get("DQMC_REF_ROOT", os.path.join(ROOT, "..", "reference"))
 sys.path.insert(0, os.path.join(HERE, "_stubs"))
 sys.path.insert(0, os.path.join(REF_ROOT, "util"))
 sys.path.insert(0, os.path.join(REF_ROOT, "test"))

@@ -71,3 +71,17 @@ def test_oracle_matches_reference_build(golden, case, tmp_path):
             if key in ref.files:
                 np.testing.assert_allclose(v, ref[key].reshape(-1), rtol=1e-9, atol=1e-10,
                                            err_msg=k)
+
+
+def test_kagome_exact_g_fixture(golden, tmp_path):
+    """The 50-digit G of the kagome case after five sweeps
+    (tests/golden/make_kagome_exact.py) belongs to the fields the oracle
+    reaches, and it shows where the FP64 error of that ill-conditioned case
+    lies: the oracle's stabilised G, which follows the reference's LAPACK
+    path (greens.c:69-208), is a few 1e-9 away from it in the up spin."""
+    z = np.load(os.path.join(golden, "kat_kagome", "g_exact_5.npz"))
+    o = Sim(_copy_case(golden, "kat_kagome", tmp_path))
+    gu, gd, _ = o.run(stop_sweep=int(z["sweeps"]))
+    assert np.array_equal(o.hs.reshape(o.L, o.N), z["hs"])
+    err = max(np.max(np.abs(gu - z["gu"])), np.max(np.abs(gd - z["gd"])))
+    assert 1e-10 < err < 1e-8

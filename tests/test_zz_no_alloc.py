@@ -90,6 +90,26 @@ def test_noalloc_matches_allocating(lib, cplx):
         assert np.max(np.abs(ph_n - ph_a)) < PHASE_TOL
 
 
+@pytest.mark.parametrize("F,l", [(5, 3), (1, 0)])
+def test_noalloc_odd_cluster_counts(lib, F, l):
+    """An odd F starts the stabilised chain from one cluster read straight
+    from C (no pair product in the scratch), and F = 1 is that cluster
+    alone: both paths through the static scratch agree with the allocating
+    entry point, again on two calls in a row."""
+    import torch
+    h = lib.load()
+    rng = np.random.default_rng(20261204 + F)
+    for cplx in (False, True):
+        Cm = _clusters(rng, 6, 5 * F * 2, F, 4.0, 0.1, cplx, 3)
+        for _ in range(2):
+            rc_a, g_a, ph_a = _call(h.dqmc_gpu_calc_eq_g, torch, Cm, l)
+            rc_n, g_n, ph_n = _call(h.dqmc_gpu_calc_eq_g_noalloc, torch, Cm, l)
+            assert rc_a == 0 and rc_n == 0
+            assert np.all(np.isfinite(g_n))
+            assert np.max(np.abs(g_n - g_a)) < G_TOL
+            assert np.max(np.abs(ph_n - ph_a)) < PHASE_TOL
+
+
 def test_noalloc_rejects_oversize(lib):
     h = lib.load()
     N = 144
