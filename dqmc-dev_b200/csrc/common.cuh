@@ -110,6 +110,7 @@ enum : unsigned {
 	DQ_ERR_SIZE = 1u << 0,     // a size beyond what the kernel was built for
 	DQ_ERR_SINGULAR = 1u << 1, // zero pivot in the final solve
 	DQ_ERR_NAN = 1u << 2,      // non-finite value detected
+	DQ_ERR_TIMEOUT = 1u << 3,  // a bounded wait on another CTA ran out
 };
 
 }  // namespace dq

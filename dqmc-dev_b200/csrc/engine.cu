@@ -18,6 +18,7 @@
 #include "launch.cuh"
 #include "meas.cuh"
 #include "update.cuh"
+#include "update_cl.cuh"
 #include "uneq.cuh"
 
 namespace dq {
@@ -401,18 +402,45 @@ __global__ void k_yhat(int N, int L, int NB, const T *Y, const double *dv, T *Yh
 	}
 }
 
-template <typename T>
-static cudaError_t update_attr(size_t bytes)
+// The delayed update holds G in shared memory (k_update_cl, one CTA per
+// chain and spin in clusters of two) when one spin's G and panels fit there;
+// otherwise one CTA per chain works on G in global memory (k_update).
+// DQMC_UPDATE=cta selects the latter for every size.
+static bool update_cl_allowed()
 {
+	static const bool on = [] {
+		const char *v = getenv("DQMC_UPDATE");
+		return !(v && strcmp(v, "cta") == 0);
+	}();
+	return on;
+}
+
+template <typename T>
+static bool update_cl_fits(int N, int kd)
+{
+	return update_cl_allowed() && N <= 480 && update_cl_smem_bytes<T>(N, kd) <= 226 * 1024;
+}
+
+template <typename T>
+static cudaError_t update_attr(int N, int kd, size_t bytes)
+{
+	if (update_cl_fits<T>(N, kd)) return raise_smem(k_update_cl<T>, update_cl_smem_bytes<T>(N, kd));
 	const cudaError_t e = raise_smem(k_update<T>, bytes);
 	return e != cudaSuccess ? e : raise_smem(k_update_big<T>, bytes);
 }
 
-// the delayed update of a.nchain chains: 2 ceil(N/32) warps of tests and
-// one look-ahead warp per chain, in the launch form sized for that CTA
+// the delayed update of a.nchain chains: on chip, two CTAs of ceil(N/32)
+// test warps and one look-ahead warp per chain; else one CTA of
+// 2 ceil(N/32) warps of tests and one look-ahead warp per chain, in the
+// launch form sized for that CTA
 template <typename T>
 static void launch_update(const UpdArgs<T> &a, size_t smem, cudaStream_t st)
 {
+	if (update_cl_fits<T>(a.N, a.n_delay)) {
+		const int threads = (a.N + 31) / 32 * 32 + 32;
+		k_update_cl<T><<<2 * a.nchain, threads, update_cl_smem_bytes<T>(a.N, a.n_delay), st>>>(a);
+		return;
+	}
 	const int threads = 2 * ((a.N + 31) / 32 * 32) + 32;
 	if (threads <= 352) k_update<T><<<a.nchain, threads, smem, st>>>(a);
 	else k_update_big<T><<<a.nchain, threads, smem, st>>>(a);
@@ -581,7 +609,7 @@ struct Group : GroupBase, ProfHook {
 		kd = p.n_delay < 1 ? 1 : p.n_delay;
 		ldp = (N + 15) / 16 * 16 + 4;
 		while (kd > 1 && update_smem_bytes<T>(N, kd, ldp) > 200 * 1024) kd /= 2;
-		CK(update_attr<T>(update_smem_bytes<T>(N, kd, ldp)));
+		CK(update_attr<T>(N, kd, update_smem_bytes<T>(N, kd, ldp)));
 		CK(cudaDeviceSynchronize());
 		return 0;
 	}
@@ -1830,7 +1858,7 @@ static int seam_update(int batch, int N, int n_delay, const double *del, uint64_
 	int kd = n_delay;
 	const int ldp = (N + 15) / 16 * 16 + 4;
 	while (kd > 1 && update_smem_bytes<T>(N, kd, ldp) > 200 * 1024) kd /= 2;
-	CK(update_attr<T>(update_smem_bytes<T>(N, kd, ldp)));
+	CK(update_attr<T>(N, kd, update_smem_bytes<T>(N, kd, ldp)));
 	Scratch<T> sc;
 	uint64_t *ck = sc.template get<uint64_t>((size_t)batch * 17);
 	int *ord = sc.template get<int>((size_t)batch * 2 * N);

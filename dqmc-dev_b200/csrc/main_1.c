@@ -2,6 +2,9 @@
  * dqmc_1: single sim file CLI.  Same options and exit status as the
  * reference's src/main_1.c:20-114 (-t max wall seconds, -n dry run,
  * -l log file, -b benchmark mode; exit status = dqmc_wrapper's return).
+ * -t is converted to the nanoseconds dqmc_wrapper takes, so the limit is
+ * the number of seconds the option's help text promises (the reference's
+ * main_1.c:103 passes the number unconverted, as nanoseconds).
  */
 #include <argp.h>
 #include <stdbool.h>
@@ -50,5 +53,5 @@ int main(int argc, char **argv)
 {
 	struct arguments a = {0, NULL, false, false, NULL};
 	argp_parse(&argp, argc, argv, 0, 0, &a);
-	return dqmc_wrapper(a.file, a.log_file, a.time, a.dry_run, a.bench);
+	return dqmc_wrapper(a.file, a.log_file, (int64_t)a.time * 1000000000LL, a.dry_run, a.bench);
 }

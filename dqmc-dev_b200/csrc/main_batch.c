@@ -53,7 +53,7 @@ int main(int argc, char **argv)
 	struct arguments a = {0, NULL, false, 0, NULL};
 	argp_parse(&argp, argc, argv, 0, 0, &a);
 	int *status = calloc(a.n, sizeof(int));
-	const int rc = dqmc_wrapper_batch(a.n, (const char *const *)a.files, a.log_file, a.time,
+	const int rc = dqmc_wrapper_batch(a.n, (const char *const *)a.files, a.log_file, (int64_t)a.time * 1000000000LL,
 	                                  a.bench, status);
 	for (int i = 0; i < a.n; i++) printf("%s %d\n", a.files[i], status[i]);
 	free(status);

@@ -60,11 +60,12 @@ struct stopper {
 	int first;
 };
 
-/* sig.c:70-127: -1 when max_time is reached, the signal number on a signal */
+/* sig.c:70-127: -1 when max_time (nanoseconds after the call began, as the
+ * reference's time_wall ticks) is reached, the signal number on a signal */
 static int check_stop(struct stopper *s, int sweep, int n_sweep_warm, int n_sweep)
 {
 	const int64_t now = time_wall();
-	if (s->max_time > 0 && now >= s->wall_start + s->max_time * 1000000000LL) stop_flag = -1;
+	if (s->max_time > 0 && now >= s->wall_start + s->max_time) stop_flag = -1;
 	if (s->t_first == 0) {
 		s->first = sweep;
 		s->t_first = now;

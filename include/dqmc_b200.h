@@ -35,7 +35,10 @@ enum {
  * of the reference (src/dqmc.h:9-10, body src/dqmc.c:525-671): same
  * arguments, same log lines, same return codes (-1 failure, 0 complete,
  * 1 partial: stopped by signal or max_time), same checkpoint and
- * partial_write protocol.  The sim file is the DQSF container written by the
+ * partial_write protocol.  max_time is in nanoseconds after the call
+ * starts (0: no limit), the unit of the reference's time_wall ticks
+ * (src/sig.c:76, src/time_.h:6); the dqmc_1 and dqmc_stack CLIs convert
+ * their -t seconds.  The sim file is the DQSF container written by the
  * generator (dqmc_b200/gen.py or the reference generator under the DQSF
  * h5py stand-in).
  * ------------------------------------------------------------------------ */
@@ -46,7 +49,8 @@ int dqmc_wrapper(const char *sim_file, const char *log_file,
  * with equal parameters share kernel launches).  status[i] receives what
  * dqmc_wrapper would have returned for file i.  Returns the worst status.
  * No reference counterpart; the reference runs such lists one file per
- * process through its stack job board (src/main_stack.c:399-479). */
+ * process through its stack job board (src/main_stack.c:399-479).
+ * max_time in nanoseconds, as for dqmc_wrapper. */
 int dqmc_wrapper_batch(int n_files, const char *const *sim_files,
 		const char *log_file, const int64_t max_time, const bool bench,
 		int *status);

@@ -142,3 +142,26 @@ class Sim:
 
     def hs2d(self):
         return self.hs.reshape(self.L, self.N)
+
+
+_exact = {}
+
+
+def exact_g(sim: "Sim", spin: int) -> np.ndarray:
+    """Quad-precision G = (I + B_{L-1} ... B_0)^-1 of one spin for the sim's
+    current fields (oracle/exact_g.c), as an N x N array."""
+    key = bool(sim.cplx)
+    if key not in _exact:
+        path = os.path.join(ORACLE_DIR, "libexact_c.so" if key else "libexact_r.so")
+        if not os.path.exists(path):
+            raise RuntimeError(f"quad-precision G not built: {path} (run make -C oracle)")
+        _exact[key] = C.CDLL(path)
+    N, L = sim.N, sim.L
+    ek = sim.a["exp_Ku"] if spin == 0 else sim.a["exp_Kd"]
+    g = np.zeros(N * N, sim.nt)
+    rc = _exact[key].exact_g(N, L, C.c_void_p(ek.ctypes.data),
+                             C.c_void_p(sim.a["exp_lambda"].ctypes.data),
+                             C.c_void_p(sim.hs.ctypes.data), spin, C.c_void_p(g.ctypes.data))
+    if rc:
+        raise RuntimeError(f"exact_g failed: {rc}")
+    return g.reshape(N, N).T

@@ -134,6 +134,7 @@ def _report(name, first_div, n_sweep, worst):
     print(json.dumps(line))
     out = os.environ.get("DQMC_PARITY_OUT")
     if out:
+        out = os.path.join(ROOT, out) if not os.path.isabs(out) else out
         with open(out, "a") as f:
             f.write(json.dumps(line) + "\n")
 
