@@ -1,12 +1,13 @@
-"""Sim-file generator for the single-band Hubbard model on the square lattice.
+"""Sim-file generator for the single-band Hubbard model on the square,
+triangular, honeycomb and kagome lattices.
 
 A restatement of the reference generator's create_1 / create_batch
-(util/gen_1band_unified_hub.py:265-1200, with H_periodic_square and
-make_peierls_mat of util/tight_binding.py:4-136 and the RNG helpers of
+(util/gen_1band_unified_hub.py:265-1200, with the periodic hopping
+matrices and Peierls phases of util/tight_binding.py:4-432 and the RNG helpers of
 util/gen_util_shared.py:5-66) that needs neither h5py nor git, so chains can
 be generated wherever the engine runs.  It writes the datasets the engine
 and the reference's sweep read -- the same names, dtypes, shapes and values
-as the reference generator for the square lattice -- except the two-bond
+as the reference generator -- except the two-bond
 family (bond2s, map_b2*, pp_*, used only by the thermal and two-bond
 correlators) and the plaquette-pair maps, which are omitted.
 
@@ -93,14 +94,36 @@ def initial_hs(rng_state: np.ndarray, L: int, N: int):
 
 
 # ----------------------------------------------------------- lattice
-def peierls_square(Nx: int, Ny: int, nflux: int, alpha: float = 0.5) -> np.ndarray:
-    """Peierls phase matrix of a uniform field through the Nx x Ny torus,
-    following make_peierls_mat (util/tight_binding.py:4-78) for the square
-    lattice: phases of the displacement d from site i to j, with the
-    boundary-wrap correction of the string gauge."""
+LATTICE = {
+    # primitive vectors a1, a2 and the unit-cell area
+    "square": (np.array((1, 0)), np.array((0, 1)), 1),
+    "triangular": (np.array((0.5, np.sqrt(3) / 2)), np.array((-0.5, np.sqrt(3) / 2)),
+                   np.sqrt(3) / 2),
+}
+NORB = {"square": 1, "triangular": 1, "honeycomb": 2, "kagome": 3}
+
+
+def peierls(Nx: int, Ny: int, lattice: str, nflux: int, alpha: float = 0.5,
+            r_to=np.array((0, 0)), r_from=np.array((0, 0))) -> np.ndarray:
+    """Peierls phases exp(i p phi) of a uniform field B through the Nx x Ny
+    torus of the Bravais lattice `lattice`, nflux flux quanta in all
+    (p = 2 pi nflux / (area of the torus)).
+
+    Gauge: A(r) = B (-alpha y, beta x), beta = 1 - alpha.  Hopping from the
+    site at cell c_i + r_from to the site at cell c_j + r_to, with c_j = c_i
+    + d for a displacement d in the central range, the straight-line
+    integral of A is -alpha m_y d_x + beta m_x d_y (m the midpoint, d the
+    displacement of the two positions).  When c_j lies outside the torus it
+    is the wrapped cell c_j' = c_j - o, o = o1 a1 + o2 a2; the magnetic
+    translation by o adds the gauge transform A_o . (r_j + r_j')/2 with
+    A_o = (-alpha o_y, beta o_x), and the product o1 o2 (beta a2x a1y -
+    alpha a1x a2y) that keeps the string of translations single-valued.
+    Entry [j', i] = exp(i p (interior - (wrap + extra))).  The expression
+    order is fixed: sim files written with these phases must equal the
+    reference generator's bit for bit."""
+    a1, a2, unit_area = LATTICE[lattice]
     beta = 1 - alpha
-    a1, a2 = np.array((1.0, 0.0)), np.array((0.0, 1.0))
-    pref = 2 * np.pi * nflux / (Nx * Ny)
+    pref = 2 * np.pi * nflux / (unit_area * Nx * Ny)
     phi = np.zeros((Ny * Nx, Ny * Nx))
     for dy in range((1 - Ny) // 2, (1 + Ny) // 2):
         for dx in range((1 - Nx) // 2, (1 + Nx) // 2):
@@ -109,18 +132,23 @@ def peierls_square(Nx: int, Ny: int, nflux: int, alpha: float = 0.5) -> np.ndarr
                     jy, jx = iy + dy, ix + dx
                     jjy, jjx = jy % Ny, jx % Nx
                     o1, o2 = jx - jjx, jy - jjy
-                    ir = ix * a1 + iy * a2
-                    jr = jx * a1 + jy * a2
-                    jjr = jjx * a1 + jjy * a2
-                    dr = jr - ir
-                    mr = (ir + jr) / 2
+                    ri = ix * a1 + iy * a2 + r_from
+                    rj = jx * a1 + jy * a2 + r_to
+                    rjj = jjx * a1 + jjy * a2 + r_to
+                    dr = rj - ri
+                    mr = (ri + rj) / 2
                     a_off = np.array((-alpha * (o1 * a1[1] + o2 * a2[1]),
                                       beta * (o1 * a1[0] + o2 * a2[0])))
                     interior = -alpha * mr[1] * dr[0] + beta * mr[0] * dr[1]
-                    wrap = np.dot(a_off, 0.5 * (jr + jjr))
+                    wrap = np.dot(a_off, 0.5 * (rj + rjj))
                     extra = o1 * o2 * (beta * a2[0] * a1[1] - alpha * a1[0] * a2[1])
                     phi[jjx + Nx * jjy, ix + Nx * iy] = interior + (-1) * (wrap + extra)
     return np.exp(1j * pref * phi)
+
+
+def peierls_square(Nx: int, Ny: int, nflux: int, alpha: float = 0.5) -> np.ndarray:
+    """Peierls phases of the square lattice (see peierls)."""
+    return peierls(Nx, Ny, "square", nflux, alpha)
 
 
 def hopping_square(Nx: int, Ny: int, t: float = 1.0, tp: float = 0.0, nflux: int = 0):
@@ -139,8 +167,112 @@ def hopping_square(Nx: int, Ny: int, t: float = 1.0, tp: float = 0.0, nflux: int
             tij[ix1 + Nx * iy1, ix + Nx * iy] += -tp
             tij[ix1 + Nx * iy, ix + Nx * iy1] += -tp
             tij[ix + Nx * iy1, ix1 + Nx * iy] += -tp
-    peierls = peierls_square(Nx, Ny, nflux)
-    return tij * peierls, peierls
+    ph = peierls_square(Nx, Ny, nflux)
+    return tij * ph, ph
+
+
+def hopping_triangular(Nx: int, Ny: int, t: float = 1.0, nflux: int = 0):
+    """Nearest-neighbour hopping of the triangular lattice (a1 = (1/2,
+    sqrt3/2), a2 = (-1/2, sqrt3/2): neighbours along x, y and x - y in cell
+    indices) with periodic boundaries, and its Peierls phases
+    (H_periodic_triangular, util/tight_binding.py:182-225)."""
+    N = Nx * Ny
+    tij = np.zeros((N, N), dtype=np.complex128)
+    for iy in range(Ny):
+        for ix in range(Nx):
+            iy1, ix1 = (iy + 1) % Ny, (ix + 1) % Nx
+            tij[ix1 + Nx * iy, ix + Nx * iy] += -t
+            tij[ix + Nx * iy, ix1 + Nx * iy] += -t
+            tij[ix + Nx * iy1, ix + Nx * iy] += -t
+            tij[ix + Nx * iy, ix + Nx * iy1] += -t
+            tij[ix1 + Nx * iy, ix + Nx * iy1] += -t
+            tij[ix + Nx * iy1, ix1 + Nx * iy] += -t
+    ph = peierls(Nx, Ny, "triangular", nflux)
+    return tij * ph, ph
+
+
+def hopping_honeycomb(Nx: int, Ny: int, t: float = 1.0, nflux: int = 0):
+    """Honeycomb lattice: sublattice A (orbital 0) and B (orbital 1) on the
+    triangular Bravais lattice, B at offset (0, -1/sqrt3) from A, each A
+    bonded to the B of its own cell and of the cells +a1 (y) and +a2 (x)
+    (H_periodic_honeycomb, util/tight_binding.py:228-325, t' = 0).  The
+    A-A and B-B blocks take the Bravais phases, the A-B blocks the phases
+    with the B offset."""
+    C = Nx * Ny
+    tij = np.zeros((2 * C, 2 * C), dtype=np.complex128)
+    for iy in range(Ny):
+        for ix in range(Nx):
+            iy1, ix1 = (iy + 1) % Ny, (ix + 1) % Nx
+            tij[ix + Nx * iy1 + C, ix + Nx * iy] += -t
+            tij[ix1 + Nx * iy + C, ix + Nx * iy] += -t
+            tij[ix + Nx * iy + C, ix + Nx * iy] += -t
+            tij[ix + Nx * iy, ix + Nx * iy1 + C] += -t
+            tij[ix + Nx * iy, ix1 + Nx * iy + C] += -t
+            tij[ix + Nx * iy, ix + Nx * iy + C] += -t
+    p_diag = peierls(Nx, Ny, "triangular", nflux)
+    p_off = peierls(Nx, Ny, "triangular", nflux, r_to=np.array((0, -1 / np.sqrt(3))))
+    K = tij.copy()
+    P = np.full((2 * C, 2 * C), np.nan, dtype=np.complex128)
+    P[:C, :C] = p_diag
+    P[C:, C:] = p_diag
+    P[:C, C:] = p_off.T.conj()
+    P[C:, :C] = p_off
+    K[:C, :C] *= p_diag
+    K[C:, C:] *= p_diag
+    K[:C, C:] *= p_off.T.conj()
+    K[C:, :C] *= p_off
+    return K, P
+
+
+def hopping_kagome(Nx: int, Ny: int, t: float = 1.0, nflux: int = 0):
+    """Kagome lattice: three sites per triangular cell, A (orbital 0) at the
+    cell origin, B (1) at (1/4, -sqrt3/4) and C (2) at (-1/4, -sqrt3/4);
+    bonds A-B within the cell and to the B of the cell +a1, A-C within the
+    cell and to the A of the cell -a2, B-C within the cell and to the C of
+    the cell +a2 -a1 (H_periodic_kagome, util/tight_binding.py:328-432,
+    t' = 0).  Each block takes the phases of its two sublattice offsets."""
+    C = Nx * Ny
+    tij = np.zeros((3 * C, 3 * C), dtype=np.complex128)
+    for iy in range(Ny):
+        for ix in range(Nx):
+            iy1, ix1 = (iy + 1) % Ny, (ix + 1) % Nx
+            iyn1, ixn1 = (iy - 1) % Ny, (ix - 1) % Nx
+            tij[ix + Nx * iy1 + C, ix + Nx * iy] += -t
+            tij[ix + Nx * iy + C, ix + Nx * iy] += -t
+            tij[ix + Nx * iy, ix + Nx * iy1 + C] += -t
+            tij[ix + Nx * iy, ix + Nx * iy + C] += -t
+            tij[ixn1 + Nx * iy, ix + Nx * iy + 2 * C] += -t
+            tij[ix + Nx * iy, ix + Nx * iy + 2 * C] += -t
+            tij[ix + Nx * iy + 2 * C, ixn1 + Nx * iy] += -t
+            tij[ix + Nx * iy + 2 * C, ix + Nx * iy] += -t
+            tij[ix1 + Nx * iyn1 + 2 * C, ix + Nx * iy + C] += -t
+            tij[ix + Nx * iy + 2 * C, ix + Nx * iy + C] += -t
+            tij[ix + Nx * iy + C, ix1 + Nx * iyn1 + 2 * C] += -t
+            tij[ix + Nx * iy + C, ix + Nx * iy + 2 * C] += -t
+    off_b = np.array((1 / 4, -np.sqrt(3) / 4))
+    off_c = np.array((-1 / 4, -np.sqrt(3) / 4))
+    p_01 = peierls(Nx, Ny, "triangular", nflux, r_to=off_b, r_from=np.array((0, 0)))
+    p_20 = peierls(Nx, Ny, "triangular", nflux, r_to=0, r_from=off_c)
+    p_12 = peierls(Nx, Ny, "triangular", nflux, r_to=off_c, r_from=off_b)
+    K = tij.copy()
+    P = np.full((3 * C, 3 * C), np.nan, dtype=np.complex128)
+    p_diag = peierls(Nx, Ny, "triangular", nflux)
+    P[0:C, 0:C] = p_diag
+    P[C:2 * C, C:2 * C] = p_diag
+    P[2 * C:3 * C, 2 * C:3 * C] = p_diag
+    P[0:C, C:2 * C] = p_01.T.conj()
+    P[C:2 * C, 0:C] = p_01
+    P[2 * C:3 * C, 0:C] = p_20.T.conj()
+    P[0:C, 2 * C:3 * C] = p_20
+    P[2 * C:3 * C, C:2 * C] = p_12
+    P[C:2 * C, 2 * C:3 * C] = p_12.T.conj()
+    K[C:2 * C, 0:C] *= p_01
+    K[0:C, C:2 * C] *= p_01.T.conj()
+    K[2 * C:3 * C, 0:C] *= p_20.T.conj()
+    K[0:C, 2 * C:3 * C] *= p_20
+    K[2 * C:3 * C, C:2 * C] *= p_12
+    K[C:2 * C, 2 * C:3 * C] *= p_12.T.conj()
+    return K, P
 
 
 def square_maps(Nx: int, Ny: int, tp: float):
@@ -195,9 +327,68 @@ def square_maps(Nx: int, Ny: int, tp: float):
     m["plaqs"] = plaqs
     m["map_plaq"] = np.repeat(np.arange(2, dtype=np.int32), N)
     m["num_plaq"], m["num_plaq_accum"], m["degen_plaq"] = 2 * N, 2, N
+    m["plaq_per_cell"] = 2
     # sizes of the two-bond family (its maps are not written)
     m["num_b2"], m["num_b2_accum"], m["degen_b2"] = b2ps * N, b2ps, N
     m["num_b2b2"], m["num_bb2"], m["num_b2b"] = b2ps * b2ps * N, bps * b2ps * N, b2ps * bps * N
+    m["degen_bb2"] = m["degen_b2b"] = m["degen_b2b2"] = N
+    return m
+
+
+def orbital_maps(geometry: str, Nx: int, Ny: int, tp: float):
+    """Measurement maps of the triangular, honeycomb and kagome lattices with
+    translation symmetry, as the reference generator writes them
+    (gen_1band_unified_hub.py:44-260, 694-895): per-orbital site classes,
+    pair classes by displacement and the two orbitals, the plaquettes of the
+    triangular and kagome lattices.  The bond, bond-site and bond-bond maps
+    of these lattices are placeholders there (bonds and maps all zero,
+    degeneracies zero), and are the same placeholders here."""
+    if tp != 0.0:
+        raise NotImplementedError("t' on the triangular, honeycomb and kagome lattices")
+    norb = NORB[geometry]
+    C = Nx * Ny
+    N = norb * C
+    bps = {"triangular": 3, "honeycomb": 3, "kagome": 4}[geometry]
+    b2ps = 4
+    m = {}
+    m["map_i"] = np.repeat(np.arange(norb, dtype=np.int32), C)
+    m["num_i"], m["degen_i"] = norb, C
+    map_ij = np.zeros((N, N), dtype=np.int32)
+    for jo in range(norb):
+        for jy in range(Ny):
+            for jx in range(Nx):
+                for io in range(norb):
+                    for iy in range(Ny):
+                        for ix in range(Nx):
+                            k = (ix - jx) % Nx + Nx * ((iy - jy) % Ny) + C * io + C * norb * jo
+                            map_ij[jx + Nx * jy + C * jo, ix + Nx * iy + C * io] = k
+    m["map_ij"], m["num_ij"], m["degen_ij"] = map_ij, norb * norb * C, C
+    m["bonds"], m["num_b"], m["bps"], m["b2ps"] = (np.zeros((2, bps * N), dtype=np.int32),
+                                                   bps * N, bps, b2ps)
+    m["map_b"] = np.tile(np.arange(bps, dtype=np.int32), (N, 1)).T.flatten()
+    m["num_b_accum"], m["degen_b"] = bps, N
+    m["map_bs"], m["num_bs"], m["degen_bs"] = np.zeros((N, bps * N), dtype=np.int32), bps * N, 0
+    m["map_bb"], m["num_bb"], m["degen_bb"] = (np.zeros((bps * N, bps * N), dtype=np.int32),
+                                               bps * bps * N, 0)
+    ppc = 1 if geometry == "honeycomb" else 2
+    plaqs = np.zeros((3, ppc * C), dtype=np.int32)
+    for iy in range(Ny):
+        for ix in range(Nx):
+            i = ix + Nx * iy
+            iy1, ix1 = (iy + 1) % Ny, (ix + 1) % Nx
+            if geometry == "triangular":
+                plaqs[:, i] = (i, ix1 + Nx * iy, ix + Nx * iy1)
+                plaqs[:, i + C] = (ix1 + Nx * iy, ix1 + Nx * iy1, ix + Nx * iy1)
+            elif geometry == "kagome":
+                plaqs[:, i] = (i, i + 2 * C, i + C)
+                plaqs[:, i + C] = (i, ix1 + Nx * iy + 2 * C, ix + Nx * iy1 + C)
+    m["plaqs"] = plaqs
+    m["map_plaq"] = np.repeat(np.arange(ppc, dtype=np.int32), C)
+    m["num_plaq"], m["num_plaq_accum"], m["degen_plaq"] = ppc * C, ppc, C
+    m["plaq_per_cell"] = ppc
+    m["num_b2"], m["num_b2_accum"], m["degen_b2"] = b2ps * N, b2ps, N
+    m["num_b2b2"], m["num_bb2"], m["num_b2b"] = b2ps * b2ps * N, bps * b2ps * N, b2ps * bps * N
+    m["degen_bb2"] = m["degen_b2b"] = m["degen_b2b2"] = 0
     return m
 
 
@@ -205,43 +396,53 @@ def square_maps(Nx: int, Ny: int, tp: float):
 def make_sim(Nx=4, Ny=4, mu=0.0, tp=0.0, U=6.0, dt=0.1, L=40, nflux=0, h=0.0,
              n_delay=16, n_matmul=8, n_sweep_warm=200, n_sweep_meas=2000, period_eqlt=8,
              period_uneqlt=0, checkpoint_every=10000, meas_bond_corr=0, seed=None,
-             init_rng=None) -> dict:
-    """All datasets of one square-lattice sim file (create_1,
-    gen_1band_unified_hub.py:265-1160) as a dict name -> array."""
+             init_rng=None, geometry="square") -> dict:
+    """All datasets of one sim file (create_1,
+    gen_1band_unified_hub.py:265-1160) as a dict name -> array, for the
+    square, triangular, honeycomb or kagome lattice (periodic boundaries;
+    t' on the square lattice only, as the reference generator)."""
     assert L % n_matmul == 0 and L % period_eqlt == 0
+    if geometry not in NORB:
+        raise NotImplementedError(f"geometry {geometry}")
     cplx = nflux != 0
     nt = np.complex128 if cplx else np.float64
     if init_rng is None:
         init_rng = seed_splitmix64(0 if seed is None else seed)
-    N = Nx * Ny
+    N = NORB[geometry] * Nx * Ny
     hs, rng = initial_hs(init_rng, L, N)
-    m = square_maps(Nx, Ny, tp)
-    K, peierls = hopping_square(Nx, Ny, 1.0, tp, nflux)
+    if geometry == "square":
+        m = square_maps(Nx, Ny, tp)
+        K, ph = hopping_square(Nx, Ny, 1.0, tp, nflux)
+    else:
+        m = orbital_maps(geometry, Nx, Ny, tp)
+        K, ph = {"triangular": hopping_triangular, "honeycomb": hopping_honeycomb,
+                 "kagome": hopping_kagome}[geometry](Nx, Ny, 1.0, nflux)
     if not cplx:
-        K, peierls = K.real, peierls.real
+        K, ph = K.real, ph.real
     Ku = K.copy()
     Kd = K.copy()
     for i in range(N):
         Ku[i, i] -= mu - h
         Kd[i, i] -= mu + h
-    U_i = U * np.ones(1, dtype=np.float64)
+    U_i = U * np.ones(m["num_i"], dtype=np.float64)
     exp_lmbd = np.exp(0.5 * U_i * dt) + np.sqrt(np.expm1(U_i * dt))
     map_i = m["map_i"]
     d = {
         "metadata/commit": GEN_ID, "metadata/version": 0.1,
         "metadata/model": "Hubbard (complex)" if cplx else "Hubbard",
-        "metadata/Nx": Nx, "metadata/Ny": Ny, "metadata/Norb": 1, "metadata/bps": m["bps"],
-        "metadata/b2ps": m["b2ps"], "metadata/plaq_per_cell": 2, "metadata/U": U,
+        "metadata/Nx": Nx, "metadata/Ny": Ny, "metadata/Norb": NORB[geometry],
+        "metadata/bps": m["bps"], "metadata/b2ps": m["b2ps"],
+        "metadata/plaq_per_cell": m["plaq_per_cell"], "metadata/U": U,
         "metadata/t'": tp, "metadata/t''": 0.0, "metadata/nflux": nflux, "metadata/twistx": 0,
         "metadata/twisty": 0, "metadata/mu": mu, "metadata/h": h, "metadata/beta": L * dt,
-        "metadata/trans_sym": 1, "metadata/geometry": "square", "metadata/bc": 1,
+        "metadata/trans_sym": 1, "metadata/geometry": geometry, "metadata/bc": 1,
     }
     i32 = lambda v: np.array(v, dtype=np.int32)  # noqa: E731
     p = {
         "N": i32(N), "L": i32(L), "Nx": i32(Nx), "Ny": i32(Ny),
         "map_i": map_i, "map_ij": m["map_ij"], "bonds": m["bonds"], "plaqs": m["plaqs"],
         "map_plaq": m["map_plaq"], "map_b": m["map_b"], "map_bs": m["map_bs"],
-        "map_bb": m["map_bb"], "peierlsu": peierls, "peierlsd": peierls.copy(),
+        "map_bb": m["map_bb"], "peierlsu": ph, "peierlsd": ph.copy(),
         "Ku": Ku, "Kd": Kd, "U": U_i, "dt": np.array(dt, dtype=np.float64),
         "n_matmul": i32(n_matmul), "n_delay": i32(n_delay), "n_sweep_warm": i32(n_sweep_warm),
         "n_sweep_meas": i32(n_sweep_meas), "period_eqlt": i32(period_eqlt),
@@ -257,8 +458,8 @@ def make_sim(Nx=4, Ny=4, mu=0.0, tp=0.0, U=6.0, dt=0.1, L=40, nflux=0, h=0.0,
         "degen_i": i32(m["degen_i"]), "degen_ij": i32(m["degen_ij"]),
         "degen_plaq": i32(m["degen_plaq"]), "degen_b": i32(m["degen_b"]),
         "degen_b2": i32(m["degen_b2"]), "degen_bs": i32(m["degen_bs"]),
-        "degen_bb": i32(m["degen_bb"]), "degen_bb2": i32(N), "degen_b2b": i32(N),
-        "degen_b2b2": i32(N),
+        "degen_bb": i32(m["degen_bb"]), "degen_bb2": i32(m["degen_bb2"]),
+        "degen_b2b": i32(m["degen_b2b"]), "degen_b2b2": i32(m["degen_b2b2"]),
         "exp_Ku": expm(-dt * Ku), "exp_Kd": expm(-dt * Kd),
         "inv_exp_Ku": expm(dt * Ku), "inv_exp_Kd": expm(dt * Kd),
         "exp_halfKu": expm(-dt / 2 * Ku), "exp_halfKd": expm(-dt / 2 * Kd),

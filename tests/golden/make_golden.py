@@ -12,7 +12,7 @@ $DQMC_REF_ROOT, default: a "reference" folder beside this repository):
 * hs_ref.npz holds the reference test suite's golden HS fields
   (test/hs_ref.py), for the 4-geometry known-answer test.
 
-Usage:  python tests/golden/make_golden.py
+Usage:  python tests/golden/make_golden.py [case ...]
 """
 import os
 import shutil
@@ -76,6 +76,13 @@ GEN_CASES = {
                          dt=0.1, L=10, n_matmul=5, n_delay=8, period_eqlt=5),
     "gen_sq4_h": dict(geometry="square", seed=9, Nx=4, Ny=6, U=3.0, mu=0.2, h=0.1,
                       dt=0.05, L=20, n_matmul=10, n_delay=8, period_eqlt=10),
+    # Peierls phases with sublattice offsets on the other lattices
+    "gen_tri_flux": dict(geometry="triangular", seed=31, Nx=4, Ny=4, nflux=1, U=4.0,
+                         mu=-0.2, dt=0.1, L=10, n_matmul=5, n_delay=8, period_eqlt=5),
+    "gen_hc_flux": dict(geometry="honeycomb", seed=32, Nx=3, Ny=3, nflux=1, U=4.0,
+                        dt=0.1, L=10, n_matmul=5, n_delay=8, period_eqlt=5),
+    "gen_kag_flux": dict(geometry="kagome", seed=33, Nx=3, Ny=3, nflux=2, U=4.0,
+                         mu=0.3, dt=0.1, L=10, n_matmul=5, n_delay=8, period_eqlt=5),
 }
 
 
@@ -119,7 +126,20 @@ def run_reference(case_dir, cplx):
     np.savez(os.path.join(case_dir, "ref_out.npz"), **out)
 
 
-def main():
+def main(only=()):
+    """all fixtures, or only the named cases"""
+    if only:
+        for name in only:
+            if name in GEN_CASES:
+                generate(os.path.join(HERE, name), GEN_CASES[name])
+                compact(os.path.join(HERE, name))
+            else:
+                kw = CASES[name]
+                generate(os.path.join(HERE, name), kw)
+                run_reference(os.path.join(HERE, name), cplx=kw.get("nflux", 0) != 0)
+                compact(os.path.join(HERE, name))
+            print("case", name, "done")
+        return
     subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
     np.savez(os.path.join(HERE, "hs_ref.npz"),
              **{f"init_{g}": hs_ref.hs_init[g] for g in GEOMETRIES},
@@ -145,4 +165,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -26,6 +26,14 @@ CASES = {
                        n_matmul=4, n_delay=4, period_eqlt=4, period_uneqlt=2,
                        meas_bond_corr=1, n_sweep_warm=4, n_sweep_meas=8),
     "kat_square": dict(seed=1234, n_sweep_warm=20, n_sweep_meas=20),
+    **{f"kat_{g}": dict(geometry=g, seed=1234, n_sweep_warm=20, n_sweep_meas=20)
+       for g in ("triangular", "honeycomb", "kagome")},
+    "gen_tri_flux": dict(geometry="triangular", seed=31, Nx=4, Ny=4, nflux=1, U=4.0, mu=-0.2,
+                         dt=0.1, L=10, n_matmul=5, n_delay=8, period_eqlt=5),
+    "gen_hc_flux": dict(geometry="honeycomb", seed=32, Nx=3, Ny=3, nflux=1, U=4.0, dt=0.1,
+                        L=10, n_matmul=5, n_delay=8, period_eqlt=5),
+    "gen_kag_flux": dict(geometry="kagome", seed=33, Nx=3, Ny=3, nflux=2, U=4.0, mu=0.3,
+                         dt=0.1, L=10, n_matmul=5, n_delay=8, period_eqlt=5),
 }
 SKIP = {"metadata/commit", "params_file"}
 
