@@ -402,41 +402,42 @@ __global__ void k_yhat(int N, int L, int NB, const T *Y, const double *dv, T *Yh
 	}
 }
 
-// The delayed update holds G in shared memory (k_update_cl, one CTA per
-// chain and spin in clusters of two) when one spin's G and panels fit there;
-// otherwise one CTA per chain works on G in global memory (k_update).
-// DQMC_UPDATE=cta selects the latter for every size.
-static bool update_cl_allowed()
+// The delayed update runs as one CTA per chain with G in global memory
+// (k_update).  DQMC_UPDATE=cluster selects the form with G held in shared
+// memory (k_update_cl, one CTA per chain and spin in clusters of two) where
+// one spin's G and panels fit there.  That form cuts the latency of a slice
+// by about 30% (12 x 12, 64 chains) but holds a whole SM per CTA and pays a
+// cross-CTA exchange per accept, so at 256 chains it takes 2.8 times the
+// SM-time of k_update and the whole sweep ran 13% slower; it stays opt-in.
+// (read when an engine is created, or a seam called)
+static bool update_cl_requested()
 {
-	static const bool on = [] {
-		const char *v = getenv("DQMC_UPDATE");
-		return !(v && strcmp(v, "cta") == 0);
-	}();
-	return on;
+	const char *v = getenv("DQMC_UPDATE");
+	return v && strcmp(v, "cluster") == 0;
 }
 
 template <typename T>
 static bool update_cl_fits(int N, int kd)
 {
-	return update_cl_allowed() && N <= 480 && update_cl_smem_bytes<T>(N, kd) <= 226 * 1024;
+	return N <= 480 && update_cl_smem_bytes<T>(N, kd) <= 226 * 1024;
 }
 
 template <typename T>
-static cudaError_t update_attr(int N, int kd, size_t bytes)
+static cudaError_t update_attr(int N, int kd, size_t bytes, bool cl)
 {
-	if (update_cl_fits<T>(N, kd)) return raise_smem(k_update_cl<T>, update_cl_smem_bytes<T>(N, kd));
+	if (cl) return raise_smem(k_update_cl<T>, update_cl_smem_bytes<T>(N, kd));
 	const cudaError_t e = raise_smem(k_update<T>, bytes);
 	return e != cudaSuccess ? e : raise_smem(k_update_big<T>, bytes);
 }
 
-// the delayed update of a.nchain chains: on chip, two CTAs of ceil(N/32)
-// test warps and one look-ahead warp per chain; else one CTA of
+// the delayed update of a.nchain chains: on chip (cl), two CTAs of
+// ceil(N/32) test warps and one look-ahead warp per chain; else one CTA of
 // 2 ceil(N/32) warps of tests and one look-ahead warp per chain, in the
 // launch form sized for that CTA
 template <typename T>
-static void launch_update(const UpdArgs<T> &a, size_t smem, cudaStream_t st)
+static void launch_update(const UpdArgs<T> &a, size_t smem, cudaStream_t st, bool cl)
 {
-	if (update_cl_fits<T>(a.N, a.n_delay)) {
+	if (cl) {
 		const int threads = (a.N + 31) / 32 * 32 + 32;
 		k_update_cl<T><<<2 * a.nchain, threads, update_cl_smem_bytes<T>(a.N, a.n_delay), st>>>(a);
 		return;
@@ -479,6 +480,7 @@ struct Group : GroupBase, ProfHook {
 	int N, L, F, nmul;
 	int sweep = 0;
 	int kd = 0, ldp = 0;   // delayed-update flush period and panel ld
+	bool upd_cl = false;   // delayed update with G on chip (k_update_cl)
 	int eq_size = 0, ue_size = 0;
 	cudaStream_t st = nullptr;
 	std::map<int, cudaGraphExec_t> graphs;
@@ -609,7 +611,8 @@ struct Group : GroupBase, ProfHook {
 		kd = p.n_delay < 1 ? 1 : p.n_delay;
 		ldp = (N + 15) / 16 * 16 + 4;
 		while (kd > 1 && update_smem_bytes<T>(N, kd, ldp) > 200 * 1024) kd /= 2;
-		CK(update_attr<T>(N, kd, update_smem_bytes<T>(N, kd, ldp)));
+		upd_cl = update_cl_requested() && update_cl_fits<T>(N, kd);
+		CK(update_attr<T>(N, kd, update_smem_bytes<T>(N, kd, ldp), upd_cl));
 		CK(cudaDeviceSynchronize());
 		return 0;
 	}
@@ -797,7 +800,7 @@ struct Group : GroupBase, ProfHook {
 		// slice again (L = 1), whose fields this kernel is still changing
 		a.next_slice = (L == 1) ? -1 : (l + 1) % L;
 		prof_begin(1);
-		launch_update<T>(a, update_smem_bytes<T>(N, kd, ldp), st);
+		launch_update<T>(a, update_smem_bytes<T>(N, kd, ldp), st, upd_cl);
 		prof_end(PC_UPDATE, 0.0, 0.0);
 		launch_count++;
 		watchdog("k_update");
@@ -1858,7 +1861,8 @@ static int seam_update(int batch, int N, int n_delay, const double *del, uint64_
 	int kd = n_delay;
 	const int ldp = (N + 15) / 16 * 16 + 4;
 	while (kd > 1 && update_smem_bytes<T>(N, kd, ldp) > 200 * 1024) kd /= 2;
-	CK(update_attr<T>(N, kd, update_smem_bytes<T>(N, kd, ldp)));
+	const bool cl = update_cl_requested() && update_cl_fits<T>(N, kd);
+	CK(update_attr<T>(N, kd, update_smem_bytes<T>(N, kd, ldp), cl));
 	Scratch<T> sc;
 	uint64_t *ck = sc.template get<uint64_t>((size_t)batch * 17);
 	int *ord = sc.template get<int>((size_t)batch * 2 * N);
@@ -1870,7 +1874,7 @@ static int seam_update(int batch, int N, int n_delay, const double *del, uint64_
 	a.N = N; a.L = 1; a.n_delay = kd; a.nchain = batch; a.slice = 0; a.ldp = ldp;
 	a.del = del; a.rng = rng; a.rng_ckpt = ck; a.hs = hs; a.G = (T *)G; a.phase = (T *)phase;
 	a.order = ord; a.u = uu; a.next_slice = -1;
-	launch_update<T>(a, update_smem_bytes<T>(N, kd, ldp), st);
+	launch_update<T>(a, update_smem_bytes<T>(N, kd, ldp), st, cl);
 	CK(cudaGetLastError());
 	CK(cudaStreamSynchronize(st));
 	return 0;
