@@ -55,6 +55,85 @@ int get_memory_req(const char *file)
 struct ientry { const char *name; int *dst; size_t n; };
 struct nentry { const char *name; num *dst; size_t n; };
 
+/* Every array measurement dataset of data.c:441-522 with the toggle that
+ * enables it: the one list that allocation, read, save and free walk (the
+ * scalar n_sample and sign are handled beside it). */
+#define MEAS_MAX 64
+struct mentry { const char *name; num **dst; size_t n; int on; };
+
+static int meas_table(struct sim_data *sim, struct mentry *m)
+{
+	const struct params *p = &sim->p;
+	struct meas_eqlt *e = &sim->m_eq;
+	struct meas_uneqlt *u = &sim->m_ue;
+	const size_t L = p->L, ni = p->num_i, nij = p->num_ij, nbb = p->num_bb, nbs = p->num_bs;
+	const size_t nba = p->num_b_accum, nb2a = p->num_b2_accum, npa = p->num_plaq_accum;
+	const size_t nb2b = p->num_b2b, nbb2 = p->num_bb2, nb2b2 = p->num_b2b2;
+	const int ue = p->period_uneqlt > 0;
+	int k = 0;
+#define M(nm, ptr, cnt, cond) m[k++] = (struct mentry){nm, &(ptr), (cnt), (cond)}
+	M("meas_eqlt/density", e->density, ni, 1);
+	M("meas_eqlt/density_u", e->density_u, ni, 1);
+	M("meas_eqlt/density_d", e->density_d, ni, 1);
+	M("meas_eqlt/double_occ", e->double_occ, ni, 1);
+	M("meas_eqlt/g00", e->g00, nij, 1);
+	M("meas_eqlt/g00_u", e->g00_u, nij, 1);
+	M("meas_eqlt/g00_d", e->g00_d, nij, 1);
+	M("meas_eqlt/nn", e->nn, nij, 1);
+	M("meas_eqlt/xx", e->xx, nij, 1);
+	M("meas_eqlt/zz", e->zz, nij, 1);
+	M("meas_eqlt/pair_sw", e->pair_sw, nij, 1);
+	M("meas_eqlt/uuuu", e->uuuu, nij * nij, p->meas_gen_suscept);
+	M("meas_eqlt/dddd", e->dddd, nij * nij, p->meas_gen_suscept);
+	M("meas_eqlt/dduu", e->dduu, nij * nij, p->meas_gen_suscept);
+	M("meas_eqlt/uudd", e->uudd, nij * nij, p->meas_gen_suscept);
+	M("meas_eqlt/chi", e->chi, npa, p->meas_chiral);
+	M("meas_eqlt/kk", e->kk, nbb, p->meas_energy_corr);
+	M("meas_eqlt/kv", e->kv, nbs, p->meas_energy_corr);
+	M("meas_eqlt/kn", e->kn, nbs, p->meas_energy_corr);
+	M("meas_eqlt/vv", e->vv, nij, p->meas_energy_corr);
+	M("meas_eqlt/vn", e->vn, nij, p->meas_energy_corr);
+	M("meas_eqlt/j", e->j, nba, p->meas_local_JQ);
+	M("meas_eqlt/jn", e->jn, nba, p->meas_local_JQ);
+	M("meas_eqlt/j2", e->j2, nb2a, p->meas_local_JQ);
+	M("meas_uneqlt/gt0", u->gt0, nij * L, ue);
+	M("meas_uneqlt/gt0_u", u->gt0_u, nij * L, ue);
+	M("meas_uneqlt/gt0_d", u->gt0_d, nij * L, ue);
+	M("meas_uneqlt/nn", u->nn, nij * L, ue);
+	M("meas_uneqlt/xx", u->xx, nij * L, ue);
+	M("meas_uneqlt/zz", u->zz, nij * L, ue);
+	M("meas_uneqlt/pair_sw", u->pair_sw, nij * L, ue);
+	M("meas_uneqlt/uuuu", u->uuuu, nij * nij * L, ue && p->meas_gen_suscept);
+	M("meas_uneqlt/dddd", u->dddd, nij * nij * L, ue && p->meas_gen_suscept);
+	M("meas_uneqlt/dduu", u->dduu, nij * nij * L, ue && p->meas_gen_suscept);
+	M("meas_uneqlt/uudd", u->uudd, nij * nij * L, ue && p->meas_gen_suscept);
+	M("meas_uneqlt/pair_bb", u->pair_bb, nbb * L, ue && (p->meas_bond_corr || p->meas_pair_bb_only));
+	M("meas_uneqlt/jj", u->jj, nbb * L, ue && p->meas_bond_corr);
+	M("meas_uneqlt/jsjs", u->jsjs, nbb * L, ue && p->meas_bond_corr);
+	M("meas_uneqlt/kk", u->kk, nbb * L, ue && p->meas_bond_corr);
+	M("meas_uneqlt/ksks", u->ksks, nbb * L, ue && p->meas_bond_corr);
+	M("meas_uneqlt/j2jn", u->j2jn, nb2b * L, ue && p->meas_thermal);
+	M("meas_uneqlt/jnj2", u->jnj2, nbb2 * L, ue && p->meas_thermal);
+	M("meas_uneqlt/jnjn", u->jnjn, nbb * L, ue && p->meas_thermal);
+	M("meas_uneqlt/jnj", u->jnj, nbb * L, ue && p->meas_thermal);
+	M("meas_uneqlt/jjn", u->jjn, nbb * L, ue && p->meas_thermal);
+	M("meas_uneqlt/pair_b2b2", u->pair_b2b2, nb2b2 * L, ue && p->meas_2bond_corr);
+	M("meas_uneqlt/j2j2", u->j2j2, nb2b2 * L, ue && p->meas_2bond_corr);
+	M("meas_uneqlt/j2j", u->j2j, nb2b * L, ue && p->meas_2bond_corr);
+	M("meas_uneqlt/jj2", u->jj2, nbb2 * L, ue && p->meas_2bond_corr);
+	M("meas_uneqlt/js2js2", u->js2js2, nb2b2 * L, ue && p->meas_2bond_corr);
+	M("meas_uneqlt/k2k2", u->k2k2, nb2b2 * L, ue && p->meas_2bond_corr);
+	M("meas_uneqlt/ks2ks2", u->ks2ks2, nb2b2 * L, ue && p->meas_2bond_corr);
+	M("meas_uneqlt/kv", u->kv, nbs * L, ue && p->meas_energy_corr);
+	M("meas_uneqlt/kn", u->kn, nbs * L, ue && p->meas_energy_corr);
+	M("meas_uneqlt/vv", u->vv, nij * L, ue && p->meas_energy_corr);
+	M("meas_uneqlt/vn", u->vn, nij * L, ue && p->meas_energy_corr);
+	M("meas_uneqlt/nem_nnnn", u->nem_nnnn, nbb * L, ue && p->meas_nematic_corr);
+	M("meas_uneqlt/nem_ssss", u->nem_ssss, nbb * L, ue && p->meas_nematic_corr);
+#undef M
+	return k;
+}
+
 int sim_data_read_alloc(struct sim_data *sim)
 {
 	dqsf_file *fp;
@@ -102,22 +181,11 @@ int sim_data_read_alloc(struct sim_data *sim)
 	for (size_t i = 0; i < sizeof(scalars) / sizeof(scalars[0]); i++)
 		RD(dqsf_read_int(fp, scalars[i].name, scalars[i].dst, 1));
 
-	/* The two-bond family (bond2s, map_b2*, pp_*) only feeds the thermal and
-	 * two-bond correlators (meas.c:1076-1360), which this layer does not
-	 * carry; files without it run with num_b2 = 0. */
+	/* the two-bond family (bond2s, map_b2*, pp_*) feeds only the thermal and
+	 * two-bond correlators; files written without it run with num_b2 = 0 */
 	if (!dqsf_has(fp, "params/bond2s") || !dqsf_has(fp, "params/map_b2b2")) p->num_b2 = 0;
-	const size_t N = p->N, L = p->L, num_i = p->num_i, num_ij = p->num_ij;
+	const size_t N = p->N, L = p->L;
 	const size_t num_b = p->num_b, num_b2 = p->num_b2, num_plaq = p->num_plaq;
-	const size_t num_bb = p->num_bb;
-	if (p->meas_gen_suscept || p->meas_chiral || p->meas_energy_corr ||
-	    p->meas_local_JQ || p->meas_thermal || p->meas_2bond_corr ||
-	    p->meas_nematic_corr || p->meas_pair_bb_only) {
-		/* the reference's extra toggles work here too, but the data layer
-		 * below only carries the always-on and bond-correlator datasets */
-		fprintf(stderr, "data_dqsf: measurement toggle not supported by this layer\n");
-		dqsf_close(fp);
-		return DQSF_RW_FAIL;
-	}
 	p->map_i = my_calloc(N * sizeof(int));
 	p->map_ij = my_calloc(N * N * sizeof(int));
 	p->bonds = my_calloc(num_b * 2 * sizeof(int));
@@ -148,35 +216,10 @@ int sim_data_read_alloc(struct sim_data *sim)
 	p->exp_lambda = my_calloc(N * 2 * sizeof(double));
 	p->del = my_calloc(N * 2 * sizeof(double));
 	sim->s.hs = my_calloc(N * L * sizeof(int));
-	struct meas_eqlt *me = &sim->m_eq;
-	me->density = my_calloc(num_i * sizeof(num));
-	me->density_u = my_calloc(num_i * sizeof(num));
-	me->density_d = my_calloc(num_i * sizeof(num));
-	me->double_occ = my_calloc(num_i * sizeof(num));
-	me->g00 = my_calloc(num_ij * sizeof(num));
-	me->g00_u = my_calloc(num_ij * sizeof(num));
-	me->g00_d = my_calloc(num_ij * sizeof(num));
-	me->nn = my_calloc(num_ij * sizeof(num));
-	me->xx = my_calloc(num_ij * sizeof(num));
-	me->zz = my_calloc(num_ij * sizeof(num));
-	me->pair_sw = my_calloc(num_ij * sizeof(num));
-	struct meas_uneqlt *mu = &sim->m_ue;
-	if (p->period_uneqlt > 0) {
-		mu->gt0 = my_calloc(num_ij * L * sizeof(num));
-		mu->gt0_u = my_calloc(num_ij * L * sizeof(num));
-		mu->gt0_d = my_calloc(num_ij * L * sizeof(num));
-		mu->nn = my_calloc(num_ij * L * sizeof(num));
-		mu->xx = my_calloc(num_ij * L * sizeof(num));
-		mu->zz = my_calloc(num_ij * L * sizeof(num));
-		mu->pair_sw = my_calloc(num_ij * L * sizeof(num));
-		if (p->meas_bond_corr) {
-			mu->pair_bb = my_calloc(num_bb * L * sizeof(num));
-			mu->jj = my_calloc(num_bb * L * sizeof(num));
-			mu->jsjs = my_calloc(num_bb * L * sizeof(num));
-			mu->kk = my_calloc(num_bb * L * sizeof(num));
-			mu->ksks = my_calloc(num_bb * L * sizeof(num));
-		}
-	}
+	struct mentry m[MEAS_MAX];
+	const int nm = meas_table(sim, m);
+	for (int i = 0; i < nm; i++)
+		if (m[i].on) *m[i].dst = my_calloc(m[i].n * sizeof(num));
 	const struct ientry iarrays[] = {
 		{"params/map_i", p->map_i, N}, {"params/map_ij", p->map_ij, N * N},
 		{"params/bonds", p->bonds, num_b * 2}, {"params/map_bb", p->map_bb, num_b * num_b},
@@ -207,40 +250,14 @@ int sim_data_read_alloc(struct sim_data *sim)
 	RD(dqsf_read_f64(fp, "params/exp_lambda", p->exp_lambda, N * 2));
 	RD(dqsf_read_f64(fp, "params/del", p->del, N * 2));
 	RD(dqsf_read_u64(fp, "state/rng", sim->s.rng, 17));
-	RD(dqsf_read_int(fp, "meas_eqlt/n_sample", &me->n_sample, 1));
-	const struct nentry eq[] = {
-		{"meas_eqlt/sign", &me->sign, 1}, {"meas_eqlt/density", me->density, num_i},
-		{"meas_eqlt/density_u", me->density_u, num_i}, {"meas_eqlt/density_d", me->density_d, num_i},
-		{"meas_eqlt/double_occ", me->double_occ, num_i}, {"meas_eqlt/g00", me->g00, num_ij},
-		{"meas_eqlt/g00_u", me->g00_u, num_ij}, {"meas_eqlt/g00_d", me->g00_d, num_ij},
-		{"meas_eqlt/nn", me->nn, num_ij}, {"meas_eqlt/xx", me->xx, num_ij},
-		{"meas_eqlt/zz", me->zz, num_ij}, {"meas_eqlt/pair_sw", me->pair_sw, num_ij},
-	};
-	for (size_t i = 0; i < sizeof(eq) / sizeof(eq[0]); i++)
-		RD(read_num(fp, eq[i].name, eq[i].dst, eq[i].n));
+	RD(dqsf_read_int(fp, "meas_eqlt/n_sample", &sim->m_eq.n_sample, 1));
+	RD(read_num(fp, "meas_eqlt/sign", &sim->m_eq.sign, 1));
 	if (p->period_uneqlt > 0) {
-		RD(dqsf_read_int(fp, "meas_uneqlt/n_sample", &mu->n_sample, 1));
-		const struct nentry ue[] = {
-			{"meas_uneqlt/sign", &mu->sign, 1}, {"meas_uneqlt/gt0", mu->gt0, num_ij * L},
-			{"meas_uneqlt/gt0_u", mu->gt0_u, num_ij * L},
-			{"meas_uneqlt/gt0_d", mu->gt0_d, num_ij * L}, {"meas_uneqlt/nn", mu->nn, num_ij * L},
-			{"meas_uneqlt/xx", mu->xx, num_ij * L}, {"meas_uneqlt/zz", mu->zz, num_ij * L},
-			{"meas_uneqlt/pair_sw", mu->pair_sw, num_ij * L},
-		};
-		for (size_t i = 0; i < sizeof(ue) / sizeof(ue[0]); i++)
-			RD(read_num(fp, ue[i].name, ue[i].dst, ue[i].n));
-		if (p->meas_bond_corr) {
-			const struct nentry bc[] = {
-				{"meas_uneqlt/pair_bb", mu->pair_bb, num_bb * L},
-				{"meas_uneqlt/jj", mu->jj, num_bb * L},
-				{"meas_uneqlt/jsjs", mu->jsjs, num_bb * L},
-				{"meas_uneqlt/kk", mu->kk, num_bb * L},
-				{"meas_uneqlt/ksks", mu->ksks, num_bb * L},
-			};
-			for (size_t i = 0; i < sizeof(bc) / sizeof(bc[0]); i++)
-				RD(read_num(fp, bc[i].name, bc[i].dst, bc[i].n));
-		}
+		RD(dqsf_read_int(fp, "meas_uneqlt/n_sample", &sim->m_ue.n_sample, 1));
+		RD(read_num(fp, "meas_uneqlt/sign", &sim->m_ue.sign, 1));
 	}
+	for (int i = 0; i < nm; i++)
+		if (m[i].on) RD(read_num(fp, m[i].name, *m[i].dst, m[i].n));
 	return dqsf_close(fp);
 }
 
@@ -261,47 +278,19 @@ int sim_data_save(const struct sim_data *sim)
 	WR(dqsf_write_int(fp, "state/partial_write", &partial_write, 1));
 	fflush(NULL);
 	const struct params *p = &sim->p;
-	const size_t N = p->N, L = p->L, num_i = p->num_i, num_ij = p->num_ij;
-	const size_t num_bb = p->num_bb;
 	WR(dqsf_write_u64(fp, "state/rng", sim->s.rng, 17));
 	WR(dqsf_write_int(fp, "state/sweep", &sim->s.sweep, 1));
-	WR(dqsf_write_int(fp, "state/hs", sim->s.hs, N * L));
-	const struct meas_eqlt *me = &sim->m_eq;
-	WR(dqsf_write_int(fp, "meas_eqlt/n_sample", &me->n_sample, 1));
-	const struct nentry eq[] = {
-		{"meas_eqlt/sign", (num *)&me->sign, 1}, {"meas_eqlt/density", me->density, num_i},
-		{"meas_eqlt/density_u", me->density_u, num_i}, {"meas_eqlt/density_d", me->density_d, num_i},
-		{"meas_eqlt/double_occ", me->double_occ, num_i}, {"meas_eqlt/g00", me->g00, num_ij},
-		{"meas_eqlt/g00_u", me->g00_u, num_ij}, {"meas_eqlt/g00_d", me->g00_d, num_ij},
-		{"meas_eqlt/nn", me->nn, num_ij}, {"meas_eqlt/xx", me->xx, num_ij},
-		{"meas_eqlt/zz", me->zz, num_ij}, {"meas_eqlt/pair_sw", me->pair_sw, num_ij},
-	};
-	for (size_t i = 0; i < sizeof(eq) / sizeof(eq[0]); i++)
-		WR(write_num(fp, eq[i].name, eq[i].dst, eq[i].n));
+	WR(dqsf_write_int(fp, "state/hs", sim->s.hs, (size_t)p->N * p->L));
+	WR(dqsf_write_int(fp, "meas_eqlt/n_sample", &sim->m_eq.n_sample, 1));
+	WR(write_num(fp, "meas_eqlt/sign", (num *)&sim->m_eq.sign, 1));
 	if (p->period_uneqlt > 0) {
-		const struct meas_uneqlt *mu = &sim->m_ue;
-		WR(dqsf_write_int(fp, "meas_uneqlt/n_sample", &mu->n_sample, 1));
-		const struct nentry ue[] = {
-			{"meas_uneqlt/sign", (num *)&mu->sign, 1}, {"meas_uneqlt/gt0", mu->gt0, num_ij * L},
-			{"meas_uneqlt/gt0_u", mu->gt0_u, num_ij * L},
-			{"meas_uneqlt/gt0_d", mu->gt0_d, num_ij * L}, {"meas_uneqlt/nn", mu->nn, num_ij * L},
-			{"meas_uneqlt/xx", mu->xx, num_ij * L}, {"meas_uneqlt/zz", mu->zz, num_ij * L},
-			{"meas_uneqlt/pair_sw", mu->pair_sw, num_ij * L},
-		};
-		for (size_t i = 0; i < sizeof(ue) / sizeof(ue[0]); i++)
-			WR(write_num(fp, ue[i].name, ue[i].dst, ue[i].n));
-		if (p->meas_bond_corr) {
-			const struct nentry bc[] = {
-				{"meas_uneqlt/pair_bb", mu->pair_bb, num_bb * L},
-				{"meas_uneqlt/jj", mu->jj, num_bb * L},
-				{"meas_uneqlt/jsjs", mu->jsjs, num_bb * L},
-				{"meas_uneqlt/kk", mu->kk, num_bb * L},
-				{"meas_uneqlt/ksks", mu->ksks, num_bb * L},
-			};
-			for (size_t i = 0; i < sizeof(bc) / sizeof(bc[0]); i++)
-				WR(write_num(fp, bc[i].name, bc[i].dst, bc[i].n));
-		}
+		WR(dqsf_write_int(fp, "meas_uneqlt/n_sample", &sim->m_ue.n_sample, 1));
+		WR(write_num(fp, "meas_uneqlt/sign", (num *)&sim->m_ue.sign, 1));
 	}
+	struct mentry m[MEAS_MAX];
+	const int nm = meas_table((struct sim_data *)sim, m);
+	for (int i = 0; i < nm; i++)
+		if (m[i].on) WR(write_num(fp, m[i].name, *m[i].dst, m[i].n));
 	fflush(NULL);
 	partial_write = 0;
 	WR(dqsf_write_int(fp, "state/partial_write", &partial_write, 1));
@@ -311,19 +300,10 @@ int sim_data_save(const struct sim_data *sim)
 void sim_data_free(const struct sim_data *sim)
 {
 	const struct params *p = &sim->p;
-	if (p->period_uneqlt > 0) {
-		if (p->meas_bond_corr) {
-			my_free(sim->m_ue.ksks); my_free(sim->m_ue.kk); my_free(sim->m_ue.jsjs);
-			my_free(sim->m_ue.jj); my_free(sim->m_ue.pair_bb);
-		}
-		my_free(sim->m_ue.pair_sw); my_free(sim->m_ue.zz); my_free(sim->m_ue.xx);
-		my_free(sim->m_ue.nn); my_free(sim->m_ue.gt0); my_free(sim->m_ue.gt0_u);
-		my_free(sim->m_ue.gt0_d);
-	}
-	my_free(sim->m_eq.pair_sw); my_free(sim->m_eq.zz); my_free(sim->m_eq.xx);
-	my_free(sim->m_eq.nn); my_free(sim->m_eq.g00); my_free(sim->m_eq.g00_u);
-	my_free(sim->m_eq.g00_d); my_free(sim->m_eq.double_occ); my_free(sim->m_eq.density);
-	my_free(sim->m_eq.density_u); my_free(sim->m_eq.density_d);
+	struct mentry m[MEAS_MAX];
+	const int nm = meas_table((struct sim_data *)sim, m);
+	for (int i = 0; i < nm; i++)
+		if (m[i].on) my_free(*m[i].dst);
 	my_free(sim->s.hs); my_free(p->del); my_free(p->exp_lambda);
 	my_free(p->inv_exp_halfKd); my_free(p->inv_exp_halfKu); my_free(p->exp_halfKd);
 	my_free(p->exp_halfKu); my_free(p->inv_exp_Kd); my_free(p->inv_exp_Ku);

@@ -17,7 +17,8 @@ unequal-time every 4 sweeps; 20 + 40 sweeps) for 4 chains:
   identical too, and the observables differ only by rounding (the summary
   reports the largest difference over sigma, which for observables whose
   spread across chains is itself at the rounding level is of order one,
-  and the largest relative difference).
+  and the largest difference relative to the largest entry of its
+  dataset).
 
 The summary goes to stdout and, when DQMC_PARITY_OUT names a file, there as
 JSON.
@@ -124,8 +125,10 @@ def _compare(sims, refs, first_div, groups, worst_rel):
             assert np.all(ok), f"{key}: engine and reference differ beyond 2 sigma"
             scale = np.where(err > 0, err, 1.0)
             worst = max(worst, float(np.max(diff / scale)))
+            # relative to the dataset's largest entry (entries near zero
+            # would make a per-entry ratio meaningless)
             worst_rel[0] = max(worst_rel[0],
-                               float(np.max(diff / np.maximum(np.abs(mu_r), 1e-300))))
+                               float(np.max(diff) / max(np.max(np.abs(mu_r)), 1e-300)))
     if first_div is None:
         for s, r in zip(sims, refs):
             assert np.array_equal(s.hs, r.hs)
