@@ -59,6 +59,24 @@ CASES = {
                        dt=0.1, L=20, n_matmul=5, n_delay=4, period_eqlt=5,
                        period_uneqlt=2, meas_bond_corr=1, n_sweep_warm=2,
                        n_sweep_meas=6),
+    # every measurement toggle (t' != 0 gives the square lattice's full
+    # bond and two-bond families)
+    "tog_sq": dict(geometry="square", seed=41, Nx=4, Ny=4, tp=-0.25, U=4.0, mu=-0.3,
+                   dt=0.1, L=16, n_matmul=4, n_delay=4, period_eqlt=4, period_uneqlt=2,
+                   meas_bond_corr=1, meas_energy_corr=1, meas_thermal=1, meas_2bond_corr=1,
+                   meas_nematic_corr=1, meas_chiral=1, meas_gen_suscept=1,
+                   n_sweep_warm=2, n_sweep_meas=4),
+    # the toggles with Peierls phases (the reference has no complex nematic)
+    "tog_cplx": dict(geometry="square", seed=42, Nx=4, Ny=4, nflux=1, tp=-0.25, U=4.0,
+                     mu=-0.3, dt=0.1, L=16, n_matmul=4, n_delay=4, period_eqlt=4,
+                     period_uneqlt=2, meas_bond_corr=1, meas_energy_corr=1, meas_thermal=1,
+                     meas_2bond_corr=1, meas_chiral=1, meas_gen_suscept=1,
+                     n_sweep_warm=2, n_sweep_meas=4),
+    # the toggles that need trans_sym = 0: local heat current, pair_bb only
+    "tog_local": dict(geometry="square", seed=43, Nx=4, Ny=4, tp=-0.25, U=4.0, mu=-0.3,
+                      dt=0.1, L=16, n_matmul=4, n_delay=4, period_eqlt=4, period_uneqlt=2,
+                      trans_sym=0, meas_local_JQ=1, meas_pair_bb_only=1,
+                      n_sweep_warm=2, n_sweep_meas=4),
     # a larger lattice, for kernels that tile N (N = 64)
     "sq8_small": dict(geometry="square", seed=21, Nx=8, Ny=8, tp=-0.25, U=6.0,
                       mu=-0.5, dt=0.1, L=16, n_matmul=8, n_delay=16, period_eqlt=8,
@@ -105,9 +123,17 @@ DROP = ("bond2s", "map_b2", "map_b2b", "map_bb2", "map_b2b2", "pp_u", "pp_d",
         "ppr_u", "ppr_d", "map_bs", "plaqs", "map_plaq")
 
 
+TOGGLES = ("meas_thermal", "meas_2bond_corr", "meas_energy_corr", "meas_nematic_corr",
+           "meas_chiral", "meas_local_JQ", "meas_gen_suscept", "meas_pair_bb_only")
+
+
 def compact(case_dir):
+    """drop the maps no engine path reads, unless a measurement toggle that
+    reads them is on"""
     path = os.path.join(case_dir, "sim.h5.params")
     d = simfile.read(path, resolve_links=False)
+    if any(int(np.asarray(d.get("params/" + t, 0)).reshape(-1)[0]) for t in TOGGLES):
+        return
     keep = {k: v for k, v in d.items() if k.split("/")[-1] not in DROP}
     simfile.write(path, keep)
 
