@@ -18,6 +18,7 @@ __host__ __device__ inline zd mkz(double a, double b) { return zd{a, b}; }
 __host__ __device__ inline zd operator+(zd a, zd b) { return zd{a.x + b.x, a.y + b.y}; }
 __host__ __device__ inline zd operator-(zd a, zd b) { return zd{a.x - b.x, a.y - b.y}; }
 __host__ __device__ inline zd operator-(zd a) { return zd{-a.x, -a.y}; }
+__host__ __device__ inline zd operator+(zd a) { return a; }
 __host__ __device__ inline zd operator*(zd a, zd b) {
 	return zd{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
 }

@@ -17,6 +17,7 @@
 #include "dqmc_b200.h"
 #include "launch.cuh"
 #include "meas.cuh"
+#include "meas_x.cuh"
 #include "update.cuh"
 #include "update_cl.cuh"
 #include "uneq.cuh"
@@ -310,16 +311,31 @@ struct DevBuf {
 	}
 };
 
-// inverse of a class map: CSR offsets over classes, entries in loop order
+// inverse of a class map: CSR offsets over classes, entries in loop order;
+// entries with keep(e) false are left out.  Returns false when an entry's
+// class is outside [0, n_class).
+template <typename K>
+static bool invert_map_if(const int *map, long long n_entries, int n_class, K keep,
+		std::vector<int> &off, std::vector<int> &idx)
+{
+	off.assign(n_class + 1, 0);
+	for (long long e = 0; e < n_entries; e++) {
+		if (!keep(e)) continue;
+		if (map[e] < 0 || map[e] >= n_class) return false;
+		off[map[e] + 1]++;
+	}
+	for (int r = 0; r < n_class; r++) off[r + 1] += off[r];
+	idx.resize(off[n_class]);
+	std::vector<int> fill(off.begin(), off.end() - 1);
+	for (long long e = 0; e < n_entries; e++)
+		if (keep(e)) idx[fill[map[e]]++] = (int)e;
+	return true;
+}
+
 static void invert_map(const int *map, int n_entries, int n_class, std::vector<int> &off,
 		std::vector<int> &idx)
 {
-	off.assign(n_class + 1, 0);
-	for (int e = 0; e < n_entries; e++) off[map[e] + 1]++;
-	for (int r = 0; r < n_class; r++) off[r + 1] += off[r];
-	idx.resize(n_entries);
-	std::vector<int> fill(off.begin(), off.end() - 1);
-	for (int e = 0; e < n_entries; e++) idx[fill[map[e]]++] = e;
+	invert_map_if(map, n_entries, n_class, [](long long) { return true; }, off, idx);
 }
 
 // S_b += diag(d_l) (I - G_b) diag(1/d_l): the slice-l term of the log-det
@@ -470,6 +486,8 @@ struct GroupBase {
 	virtual int profile(int meq, int mue, double *out, int ncls) = 0;
 	virtual int logdet_grad(double *logdet, void *S) = 0;
 	virtual int obs_grad(double *obs, void *Z) = 0;
+	// the eight hopping matrices exp(-+dt K), exp(-+dt K / 2) of both spins
+	virtual int set_hopping(const void *const *m) = 0;
 };
 
 template <typename T>
@@ -514,6 +532,11 @@ struct Group : GroupBase, ProfHook {
 	// parameters
 	DevBuf<T> expK, iexpK, ehK, iehK, peu, ped;
 	DevBuf<int> i_off, i_idx, ij_off, ij_idx, bb_off, bb_idx, bonds;
+	// the measurement toggles' maps (inverses) and two-hop bond phases
+	DevBuf<int> bs_off, bs_idx, bb2_off, bb2_idx, b2b_off, b2b_idx, b2b2_off, b2b2_idx;
+	DevBuf<int> nem_off, nem_idx, plq_off, plq_idx, b_off, b_idx, b2_off, b2_idx, plaqs, bond2s;
+	DevBuf<T> ppu, ppd, ppru, pprd, gs_eq, gs_ue;
+	AccLayout lay;
 	// chains
 	DevBuf<double> el, del, dv, dvi;
 	DevBuf<uint64_t> rng, rng_ckpt;
@@ -523,6 +546,16 @@ struct Group : GroupBase, ProfHook {
 	bool need_init = true;     // G must be recomputed from the fields before sweeping
 	DevBuf<T> phase, G, Cl, Qm, Tm, Tm2, Rs, X, W, Gh, acc_eq, acc_ue, phi, qdet;
 	DevBuf<T> Sg;                  // gradient sums, allocated by the first logdet_grad
+	struct ObsWork {               // observable-gradient work, allocated by the first obs_grad
+		DevBuf<T> O, Gr, Qh, Tw, Rw, Yh, Zb, dg;
+		DevBuf<double> wb;
+		void release()
+		{
+			DevBuf<T> *b[] = {&O, &Gr, &Qh, &Tw, &Rw, &Yh, &Zb, &dg};
+			for (auto *x : b) x->release();
+			wb.release();
+		}
+	} og;
 	DevBuf<T> Pr;                  // pair products C_{(m+1)%F} C_m, F >= 2
 	DevBuf<double> dR, ldet;       // UDT scales; log |det(I + B...B)| per item
 	DevBuf<int> pvt;
@@ -533,15 +566,99 @@ struct Group : GroupBase, ProfHook {
 	{
 		for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
 		DevBuf<T> *tb[] = {&expK, &iexpK, &ehK, &iehK, &peu, &ped, &phase, &G, &Cl, &Qm, &Tm,
-		                   &Tm2, &Rs, &X, &W, &Gh, &acc_eq, &acc_ue, &phi, &qdet, &Sg, &Pr};
+		                   &Tm2, &Rs, &X, &W, &Gh, &acc_eq, &acc_ue, &phi, &qdet, &Sg, &Pr,
+		                   &ppu, &ppd, &ppru, &pprd, &gs_eq, &gs_ue};
 		for (auto *b : tb) b->release();
 		DevBuf<int> *ib[] = {&i_off, &i_idx, &ij_off, &ij_idx, &bb_off, &bb_idx, &bonds, &hs,
-		                     &nacc, &n_eq, &n_ue, &pvt};
+		                     &nacc, &n_eq, &n_ue, &pvt, &bs_off, &bs_idx, &bb2_off, &bb2_idx,
+		                     &b2b_off, &b2b_idx, &b2b2_off, &b2b2_idx, &nem_off, &nem_idx,
+		                     &plq_off, &plq_idx, &b_off, &b_idx, &b2_off, &b2_idx, &plaqs,
+		                     &bond2s};
 		for (auto *b : ib) b->release();
+		og.release();
 		el.release(); del.release(); dv.release(); dvi.release(); dR.release(); ldet.release();
 		rng.release(); rng_ckpt.release(); order.release(); ubuf.release(); err.release();
 		ue.release();
 		if (st) cudaStreamDestroy(st);
+	}
+
+	// the maps and phases the measurement toggles read (struct params,
+	// data.h:7-38), as inverse maps per class; refuses a toggle whose maps
+	// are missing, and nematic correlators with complex hoppings (the
+	// reference stops there, meas.c:1363-1369)
+	template <typename U>
+	int toggle_maps(U &upv)
+	{
+		std::vector<int> off, idx;
+		const bool ue_on = p.period_uneqlt > 0;
+		const long long nb = p.num_b, nb2 = p.num_b2;
+		auto all = [](long long) { return true; };
+		auto inv = [&](const int *map, long long n, int ncls, DevBuf<int> &o, DevBuf<int> &x,
+		               auto keep) -> int {
+			if (!map || ncls < 1) return DQMC_E_ARG;
+			if (!invert_map_if(map, n, ncls, keep, off, idx)) return DQMC_E_ARG;
+			if (upv(o, off) || upv(x, idx)) return DQMC_E_NOMEM;
+			return 0;
+		};
+		auto up_num = [&](DevBuf<T> &dst, const void *src, long long n) -> int {
+			if (!src || n < 1) return DQMC_E_ARG;
+			if (dst.alloc((size_t)n)) return DQMC_E_NOMEM;
+			cudaMemcpy(dst.p, src, sizeof(T) * n, cudaMemcpyHostToDevice);
+			return 0;
+		};
+		int rc;
+		if (ue_on && p.meas_nematic_corr && is_cplx<T>::value) {
+			fprintf(stderr, "dqmc_b200: nematic correlators have no complex form\n");
+			return DQMC_E_ARG;
+		}
+		if (p.meas_energy_corr &&
+		    (rc = inv(p.map_bs, (long long)N * nb, p.num_bs, bs_off, bs_idx, all)) != 0)
+			return rc;
+		const bool two_hop = ue_on && (p.meas_thermal || p.meas_2bond_corr);
+		if (two_hop || p.meas_local_JQ) {
+			if (nb2 < 1 || !p.bond2s) return DQMC_E_ARG;
+			std::vector<int> b2(p.bond2s, p.bond2s + 2 * nb2);
+			if (upv(bond2s, b2)) return DQMC_E_NOMEM;
+			if ((rc = up_num(ppu, p.pp_u, nb2)) || (rc = up_num(ppd, p.pp_d, nb2)) ||
+			    (rc = up_num(ppru, p.ppr_u, nb2)) || (rc = up_num(pprd, p.ppr_d, nb2)))
+				return rc;
+		}
+		if (two_hop) {
+			if ((rc = inv(p.map_bb2, nb2 * nb, p.num_bb2, bb2_off, bb2_idx, all)) ||
+			    (rc = inv(p.map_b2b, nb * nb2, p.num_b2b, b2b_off, b2b_idx, all)))
+				return rc;
+			if (p.meas_2bond_corr &&
+			    (rc = inv(p.map_b2b2, nb2 * nb2, p.num_b2b2, b2b2_off, b2b2_idx, all)) != 0)
+				return rc;
+		}
+		if (ue_on && p.meas_nematic_corr) {
+			const long long nem = std::min<long long>(2LL * N, nb);   // NEM_BONDS N bonds
+			if ((rc = inv(p.map_bb, nb * nb, p.num_bb, nem_off, nem_idx,
+			              [&](long long e) { return e % nb < nem && e / nb < nem; })) != 0)
+				return rc;
+		}
+		if (p.meas_chiral) {
+			if (!p.plaqs || p.num_plaq < 1) return DQMC_E_ARG;
+			std::vector<int> pq(p.plaqs, p.plaqs + 3 * (size_t)p.num_plaq);
+			if (upv(plaqs, pq)) return DQMC_E_NOMEM;
+			if ((rc = inv(p.map_plaq, p.num_plaq, p.num_plaq_accum, plq_off, plq_idx, all)) != 0)
+				return rc;
+		}
+		if (p.meas_local_JQ &&
+		    ((rc = inv(p.map_b, nb, p.num_b_accum, b_off, b_idx, all)) ||
+		     (rc = inv(p.map_b2, nb2, p.num_b2_accum, b2_off, b2_idx, all))))
+			return rc;
+		if (p.meas_gen_suscept) {
+			if (p.Nx < 1 || p.Ny < 1) return DQMC_E_ARG;
+			if (gs_eq.alloc((size_t)C * 4 * p.num_ij)) return DQMC_E_NOMEM;
+			if (ue_on && gs_ue.alloc((size_t)C * L * 4 * p.num_ij)) return DQMC_E_NOMEM;
+		}
+		return 0;
+	}
+
+	bool eq_toggles() const
+	{
+		return p.meas_gen_suscept || p.meas_chiral || p.meas_energy_corr || p.meas_local_JQ;
 	}
 
 	int create(const dqmc_params &pp, int nchain)
@@ -574,8 +691,9 @@ struct Group : GroupBase, ProfHook {
 		rc |= ldet.alloc(NB);
 		if (F >= 2) rc |= Pr.alloc((size_t)NB * F * NN);
 		rc |= err.alloc(1);
-		eq_size = eq_acc_size(p.num_i, p.num_ij);
-		ue_size = p.period_uneqlt > 0 ? ue_acc_size(p.num_ij, p.num_bb, L, p.meas_bond_corr) : 0;
+		lay = acc_layout(p);
+		eq_size = (int)lay.eq_size;
+		ue_size = (int)lay.ue_size;
 		rc |= acc_eq.alloc((size_t)C * eq_size);
 		if (ue_size) rc |= acc_ue.alloc((size_t)C * ue_size);
 		if (rc) return DQMC_E_NOMEM;
@@ -601,12 +719,20 @@ struct Group : GroupBase, ProfHook {
 		if (upv(i_off, off) || upv(i_idx, idx)) return DQMC_E_NOMEM;
 		invert_map(p.map_ij, N * N, p.num_ij, off, idx);
 		if (upv(ij_off, off) || upv(ij_idx, idx)) return DQMC_E_NOMEM;
-		if (p.meas_bond_corr && p.num_b > 0) {
-			invert_map(p.map_bb, p.num_b * p.num_b, p.num_bb, off, idx);
-			if (upv(bb_off, off) || upv(bb_idx, idx)) return DQMC_E_NOMEM;
+		const bool ue_on = p.period_uneqlt > 0;
+		const bool need_bb = (ue_on && (p.meas_bond_corr || p.meas_pair_bb_only || p.meas_thermal ||
+		                                p.meas_nematic_corr)) || p.meas_energy_corr;
+		if ((need_bb || p.meas_local_JQ || (ue_on && p.meas_2bond_corr)) && p.num_b > 0) {
 			std::vector<int> bv(p.bonds, p.bonds + 2 * p.num_b);
 			if (upv(bonds, bv)) return DQMC_E_NOMEM;
 		}
+		if (need_bb && p.num_b > 0) {
+			if (!invert_map_if(p.map_bb, (long long)p.num_b * p.num_b, p.num_bb,
+			                   [](long long) { return true; }, off, idx))
+				return DQMC_E_ARG;
+			if (upv(bb_off, off) || upv(bb_idx, idx)) return DQMC_E_NOMEM;
+		}
+		if ((rc = toggle_maps(upv)) != 0) return rc;
 		// delayed-update panels: the file's n_delay unless shared memory is short
 		kd = p.n_delay < 1 ? 1 : p.n_delay;
 		ldp = (N + 15) / 16 * 16 + 4;
@@ -840,6 +966,23 @@ struct Group : GroupBase, ProfHook {
 		m.i_off = i_off.p; m.i_idx = i_idx.p; m.ij_off = ij_off.p; m.ij_idx = ij_idx.p;
 		m.bb_off = bb_off.p; m.bb_idx = bb_idx.p; m.bonds = bonds.p;
 		m.peu = peu.p; m.ped = ped.p;
+		m.energy = p.meas_energy_corr; m.thermal = p.meas_thermal; m.two_bond = p.meas_2bond_corr;
+		m.nematic = p.meas_nematic_corr; m.chiral = p.meas_chiral; m.local_jq = p.meas_local_JQ;
+		m.gen_suscept = p.meas_gen_suscept; m.pair_bb_only = p.meas_pair_bb_only;
+		m.Nx = p.Nx; m.Ny = p.Ny; m.num_bs = p.num_bs; m.num_b2 = p.num_b2;
+		m.num_b2b = p.num_b2b; m.num_bb2 = p.num_bb2; m.num_b2b2 = p.num_b2b2;
+		m.num_plaq = p.num_plaq; m.num_plaq_accum = p.num_plaq_accum;
+		m.num_b_accum = p.num_b_accum; m.num_b2_accum = p.num_b2_accum;
+		m.degen_bs = p.degen_bs; m.degen_b2b = p.degen_b2b; m.degen_bb2 = p.degen_bb2;
+		m.degen_b2b2 = p.degen_b2b2; m.degen_plaq = p.degen_plaq; m.degen_b = p.degen_b;
+		m.degen_b2 = p.degen_b2;
+		m.bs_off = bs_off.p; m.bs_idx = bs_idx.p; m.bb2_off = bb2_off.p; m.bb2_idx = bb2_idx.p;
+		m.b2b_off = b2b_off.p; m.b2b_idx = b2b_idx.p; m.b2b2_off = b2b2_off.p; m.b2b2_idx = b2b2_idx.p;
+		m.nem_off = nem_off.p; m.nem_idx = nem_idx.p; m.plaq_off = plq_off.p; m.plaq_idx = plq_idx.p;
+		m.b_off = b_off.p; m.b_idx = b_idx.p; m.b2_off = b2_off.p; m.b2_idx = b2_idx.p;
+		m.plaqs = plaqs.p; m.bond2s = bond2s.p;
+		m.pp_u = ppu.p; m.pp_d = ppd.p; m.ppr_u = ppru.p; m.ppr_d = pprd.p;
+		m.lay = lay;
 		return m;
 	}
 
@@ -852,8 +995,12 @@ struct Group : GroupBase, ProfHook {
 		m.acc = acc_eq.p; m.acc_stride = eq_size; m.n_sample = n_eq.p;
 		prof_begin(4);
 		k_meas_eqlt<T><<<C, 256, 2 * N * sizeof(T) + 64, st>>>(m);
-		prof_end(PC_MEAS, 0.0, 0.0);
 		launch_count++;
+		if (eq_toggles()) {
+			k_meas_eqlt_x<T><<<C, 256, 0, st>>>(m, gs_eq.p);
+			launch_count++;
+		}
+		prof_end(PC_MEAS, 0.0, 0.0);
 		watchdog("k_meas_eqlt");
 	}
 
@@ -1062,8 +1209,24 @@ struct Group : GroupBase, ProfHook {
 		m.bond = p.meas_bond_corr;
 		prof_begin(4);
 		k_meas_uneqlt<T><<<dim3(C, L), 256, 0, st>>>(m);
-		prof_end(PC_MEAS, 0.0, 0.0);
 		launch_count++;
+		if (p.meas_gen_suscept || p.meas_energy_corr) {
+			k_meas_uneqlt_xs<T><<<dim3(C, L), 256, 0, st>>>(m, gs_ue.p);
+			launch_count++;
+		}
+		if (p.meas_thermal) {
+			k_meas_uneqlt_xb<T><<<dim3(C, L), 128, 0, st>>>(m);
+			launch_count++;
+		}
+		if (p.meas_thermal || p.meas_2bond_corr) {
+			k_meas_uneqlt_x2<T><<<dim3(C, L), 128, 0, st>>>(m);
+			launch_count++;
+		}
+		if (p.meas_nematic_corr) {
+			k_meas_uneqlt_xn<T><<<dim3(C, L), 128, 0, st>>>(m);
+			launch_count++;
+		}
+		prof_end(PC_MEAS, 0.0, 0.0);
 		watchdog("k_meas_uneqlt");
 		return 0;
 	}
@@ -1262,22 +1425,23 @@ struct Group : GroupBase, ProfHook {
 			const int rc = init();
 			if (rc) return rc;
 		}
-		DevBuf<T> O, Gr, Qh, Tw, Rw, Yh, Zb, dg;
-		DevBuf<double> wb;
+		// the work buffers are allocated by the first call and kept, so that
+		// repeated evaluations (new hopping, same fields) allocate nothing
+		DevBuf<T> &O = og.O, &Gr = og.Gr, &Qh = og.Qh, &Tw = og.Tw, &Rw = og.Rw, &Yh = og.Yh,
+		          &Zb = og.Zb, &dg = og.dg;
+		DevBuf<double> &wb = og.wb;
 		int rc = 0;
-		rc |= O.alloc(NB * NL2); rc |= Gr.alloc(NB * NL2);
-		rc |= Qh.alloc((size_t)NB * std::max(L - 1, 1) * 4 * NN); rc |= Tw.alloc((size_t)NB * L * NN);
-		rc |= Rw.alloc((size_t)NB * NL * 2 * N); rc |= Yh.alloc(NB * NN); rc |= Zb.alloc(NB * NN);
-		rc |= dg.alloc(NB * NL); rc |= wb.alloc(NB * NL);
-		auto release = [&]() {
-			DevBuf<T> *b[] = {&O, &Gr, &Qh, &Tw, &Rw, &Yh, &Zb, &dg};
-			for (auto *x : b) x->release();
-			wb.release();
-		};
-		if (rc) { release(); return DQMC_E_NOMEM; }
-		// the buffers are zeroed on the legacy default stream, which the
-		// engine's non-blocking stream does not wait for
-		CK(cudaDeviceSynchronize());
+		if (!O.p) {
+			rc |= O.alloc(NB * NL2); rc |= Gr.alloc(NB * NL2);
+			rc |= Qh.alloc((size_t)NB * std::max(L - 1, 1) * 4 * NN); rc |= Tw.alloc((size_t)NB * L * NN);
+			rc |= Rw.alloc((size_t)NB * NL * 2 * N); rc |= Yh.alloc(NB * NN); rc |= Zb.alloc(NB * NN);
+			rc |= dg.alloc(NB * NL); rc |= wb.alloc(NB * NL);
+			if (rc) { og.release(); return DQMC_E_NOMEM; }
+			// zeroed on the legacy default stream, which the engine's
+			// non-blocking stream does not wait for
+			CK(cudaDeviceSynchronize());
+		}
+		auto release = [&]() {};
 		CK(cudaMemsetAsync(O.p, 0, sizeof(T) * NB * NL2, st));
 		k_add_diag<T><<<grid_for((long long)NL * NB), 256, 0, st>>>((int)NL, NB, O.p, (long long)NL2);
 		k_build_o<T><<<grid_for((long long)NN * L * NB), 256, 0, st>>>(N, L, NB, expK.p, dv.p, O.p);
@@ -1329,6 +1493,23 @@ struct Group : GroupBase, ProfHook {
 		CK(cudaGetLastError());
 		release();
 		return sync();
+	}
+
+	// replace the hopping matrices in place (stream-ordered after queued
+	// work); G and the clusters are recomputed before the next use
+	int set_hopping(const void *const *m) override
+	{
+		const size_t NN = (size_t)N * N;
+		DevBuf<T> *dst[4] = {&expK, &iexpK, &ehK, &iehK};
+		for (int k = 0; k < 4; k++)
+			for (int sp = 0; sp < 2; sp++) {
+				if (!m[2 * k + sp]) return DQMC_E_ARG;
+				CK(cudaMemcpyAsync(dst[k]->p + sp * NN, m[2 * k + sp], sizeof(T) * NN,
+				                   cudaMemcpyHostToDevice, st));
+			}
+		CK(cudaStreamSynchronize(st));
+		need_init = true;
+		return 0;
 	}
 
 	int sync() override
@@ -1437,10 +1618,9 @@ struct Lanes : GroupBase {
 		elem = p.cplx ? sizeof(zd) : sizeof(double);
 		n_site = (size_t)p.N;
 		hs_len = (size_t)p.L * p.N;
-		eq_bytes = elem * (size_t)eq_acc_size(p.num_i, p.num_ij);
-		ue_bytes = p.period_uneqlt > 0
-		                   ? elem * (size_t)ue_acc_size(p.num_ij, p.num_bb, p.L, p.meas_bond_corr)
-		                   : 0;
+		const AccLayout al = acc_layout(p);
+		eq_bytes = elem * (size_t)al.eq_size;
+		ue_bytes = elem * (size_t)al.ue_size;
 		CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
 		ev.assign(n_lane + 1, nullptr);
 		for (auto &e : ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -1643,6 +1823,16 @@ struct Lanes : GroupBase {
 		});
 	}
 
+	int set_hopping(const void *const *m) override
+	{
+		CK(cudaStreamSynchronize(st));
+		for (GroupBase *x : g) {
+			const int rc = x->set_hopping(m);
+			if (rc) return rc;
+		}
+		return 0;
+	}
+
 	int obs_grad(double *obs, void *Z) override
 	{
 		return per_lane([&](size_t k) {
@@ -1682,9 +1872,9 @@ extern "C" {
 int dqmc_acc_sizes(const dqmc_params *p, int *eq_size, int *ue_size)
 {
 	if (!p) return DQMC_E_ARG;
-	if (eq_size) *eq_size = eq_acc_size(p->num_i, p->num_ij);
-	if (ue_size)
-		*ue_size = p->period_uneqlt > 0 ? ue_acc_size(p->num_ij, p->num_bb, p->L, p->meas_bond_corr) : 0;
+	const AccLayout al = acc_layout(*p);
+	if (eq_size) *eq_size = (int)al.eq_size;
+	if (ue_size) *ue_size = (int)al.ue_size;
 	return 0;
 }
 
@@ -1794,6 +1984,16 @@ int dqmc_engine_logdet_grad(dqmc_engine *e, double *logdet, void *S)
 int dqmc_engine_obs_grad(dqmc_engine *e, double *obs, void *Z)
 {
 	return e ? e->g->obs_grad(obs, Z) : DQMC_E_ARG;
+}
+
+int dqmc_engine_set_hopping(dqmc_engine *e, const void *exp_Ku, const void *exp_Kd,
+		const void *inv_exp_Ku, const void *inv_exp_Kd, const void *exp_halfKu,
+		const void *exp_halfKd, const void *inv_exp_halfKu, const void *inv_exp_halfKd)
+{
+	if (!e) return DQMC_E_ARG;
+	const void *m[8] = {exp_Ku, exp_Kd, inv_exp_Ku, inv_exp_Kd, exp_halfKu, exp_halfKd,
+	                    inv_exp_halfKu, inv_exp_halfKd};
+	return e->g->set_hopping(m);
 }
 
 int dqmc_engine_profile_sweep(dqmc_engine *e, int meas_eq, int meas_ue, double *out, int n_class)

@@ -10,18 +10,54 @@
 #pragma once
 
 #include "common.cuh"
+#include "dqmc_b200.h"
 
 namespace dq {
 
-// accumulator layout, per chain
+// accumulator layout, per chain (each group only when its toggle is on)
 //   eqlt:   sign | density, density_u, density_d, double_occ [num_i]
 //           | g00, g00_u, g00_d, nn, xx, zz, pair_sw [num_ij]
+//           | uuuu, dddd, dduu, uudd [num_ij^2]                 (gen_suscept)
+//           | chi [num_plaq_accum]                              (chiral)
+//           | kk [num_bb], kv, kn [num_bs], vv, vn [num_ij]     (energy_corr)
+//           | j, jn [num_b_accum], j2 [num_b2_accum]            (local_JQ)
 //   uneqlt: sign | gt0, gt0_u, gt0_d, nn, xx, zz, pair_sw [L][num_ij]
-//           | pair_bb, jj, jsjs, kk, ksks [L][num_bb]       (meas_bond_corr)
-inline int eq_acc_size(int num_i, int num_ij) { return 1 + 4 * num_i + 7 * num_ij; }
-inline int ue_acc_size(int num_ij, int num_bb, int L, int bond)
+//           | uuuu, dddd, dduu, uudd [L][num_ij^2]              (gen_suscept)
+//           | pair_bb [L][num_bb]                   (bond_corr or pair_bb_only)
+//           | jj, jsjs, kk, ksks [L][num_bb]                    (bond_corr)
+//           | j2jn [L][num_b2b], jnj2 [L][num_bb2], jnjn, jnj, jjn [L][num_bb]
+//                                                               (thermal)
+//           | pair_b2b2, j2j2 [L][num_b2b2], j2j [L][num_b2b], jj2 [L][num_bb2],
+//             js2js2, k2k2, ks2ks2 [L][num_b2b2]                (2bond_corr)
+//           | kv, kn [L][num_bs], vv, vn [L][num_ij]            (energy_corr)
+//           | nem_nnnn, nem_ssss [L][num_bb]                    (nematic_corr)
+// The dataset names and sizes are those of the reference's data.c:441-522.
+struct AccLayout {
+	long long eq_size, ue_size;
+	long long gs, chi, energy, jq;                                   // eqlt groups
+	long long ue_gs, pair_bb, bond, thermal, two_bond, ue_energy, nem;  // uneqlt groups
+};
+
+inline AccLayout acc_layout(const dqmc_params &p)
 {
-	return 1 + 7 * num_ij * L + (bond ? 5 * num_bb * L : 0);
+	AccLayout a;
+	const long long L = p.L, ni = p.num_i, nij = p.num_ij, nbb = p.num_bb, nbs = p.num_bs;
+	long long o = 1 + 4 * ni + 7 * nij;
+	a.gs = o;     o += p.meas_gen_suscept ? 4 * nij * nij : 0;
+	a.chi = o;    o += p.meas_chiral ? p.num_plaq_accum : 0;
+	a.energy = o; o += p.meas_energy_corr ? nbb + 2 * nbs + 2 * nij : 0;
+	a.jq = o;     o += p.meas_local_JQ ? 2LL * p.num_b_accum + p.num_b2_accum : 0;
+	a.eq_size = o;
+	o = 1 + 7 * nij * L;
+	a.ue_gs = o;     o += p.meas_gen_suscept ? 4 * nij * nij * L : 0;
+	a.pair_bb = o;   o += (p.meas_bond_corr || p.meas_pair_bb_only) ? nbb * L : 0;
+	a.bond = o;      o += p.meas_bond_corr ? 4 * nbb * L : 0;
+	a.thermal = o;   o += p.meas_thermal ? ((long long)p.num_b2b + p.num_bb2 + 3 * nbb) * L : 0;
+	a.two_bond = o;  o += p.meas_2bond_corr ? (5LL * p.num_b2b2 + p.num_b2b + p.num_bb2) * L : 0;
+	a.ue_energy = o; o += p.meas_energy_corr ? (2 * nbs + 2 * nij) * L : 0;
+	a.nem = o;       o += p.meas_nematic_corr ? 2 * nbb * L : 0;
+	a.ue_size = p.period_uneqlt > 0 ? o : 0;
+	return a;
 }
 
 template <typename T>
@@ -40,6 +76,23 @@ struct MeasArgs {
 	long long acc_stride;
 	int *n_sample;         // [chain]
 	int bond;              // accumulate the bond correlators
+	// the measurement toggles (meas.c:125-714, 827-858, 966-1363) and the
+	// inverse maps of their classes; `lay` holds the group offsets
+	int energy, thermal, two_bond, nematic, chiral, local_jq, gen_suscept, pair_bb_only;
+	int Nx, Ny, num_bs, num_b2, num_b2b, num_bb2, num_b2b2, num_plaq;
+	int degen_bs, degen_b2b, degen_bb2, degen_b2b2, degen_plaq, degen_b, degen_b2;
+	int num_plaq_accum, num_b_accum, num_b2_accum;
+	const int *bs_off, *bs_idx;      // inverse of map_bs, entries b + num_b*j
+	const int *bb2_off, *bb2_idx;    // inverse of map_bb2, entries b + num_b2*c
+	const int *b2b_off, *b2b_idx;    // inverse of map_b2b, entries b + num_b*c
+	const int *b2b2_off, *b2b2_idx;  // inverse of map_b2b2, entries b + num_b2*c
+	const int *nem_off, *nem_idx;    // inverse of map_bb over b, c < 2N
+	const int *plaq_off, *plaq_idx;  // inverse of map_plaq
+	const int *b_off, *b_idx;        // inverse of map_b
+	const int *b2_off, *b2_idx;      // inverse of map_b2
+	const int *plaqs, *bond2s;       // [3][num_plaq], [2][num_b2]
+	const T *pp_u, *pp_d, *ppr_u, *ppr_d;  // two-hop phases [num_b2]
+	AccLayout lay;
 };
 
 template <typename T>
@@ -91,7 +144,7 @@ __global__ void k_meas_eqlt(MeasArgs<T> a)
 	T *a2 = acc + 1 + 4 * ni;
 	for (int r = threadIdx.x; r < nij; r += blockDim.x) {
 		T g00 = zero<T>(), g00u = zero<T>(), g00d = zero<T>(), nn = zero<T>();
-		T xx = zero<T>(), zz = zero<T>(), ps = zero<T>();
+		T xx = zero<T>(), zz = zero<T>(), ps = zero<T>(), vv = zero<T>(), vn = zero<T>();
 		for (int q = a.ij_off[r]; q < a.ij_off[r + 1]; q++) {
 			const int e = a.ij_idx[q];
 			const int i = e % N, j = e / N;
@@ -108,6 +161,18 @@ __global__ void k_meas_eqlt(MeasArgs<T> a)
 			xx += 0.25 * (delta * (guii + gdii) - (guji * gdij + gdji * guij));
 			zz += 0.25 * ((gdii - guii) * (gdjj - gujj) + x);
 			ps += guij * gdij;
+			if (a.energy) {
+				// meas.c:113-118
+				const T nun = (1.0 - guii) * (1.0 - gujj) + (delta - guji) * guij;
+				const T ndn = (1.0 - gdii) * (1.0 - gdjj) + (delta - gdji) * gdij;
+				vv += nun * ndn;
+				vn += nun * (1.0 - gdii) + (1.0 - guii) * ndn;
+			}
+		}
+		if (a.energy) {
+			T *ae = acc + a.lay.energy + a.num_bb + 2 * (size_t)a.num_bs;
+			ae[r] += pre * vv;
+			ae[nij + r] += pre * vn;
 		}
 		a2[r] += pre * g00;
 		a2[nij + r] += pre * g00u;
@@ -144,7 +209,7 @@ __global__ void k_meas_uneqlt(MeasArgs<T> a)
 	T *a2 = acc + 1;
 	for (int r = threadIdx.x; r < nij; r += blockDim.x) {
 		T g0 = zero<T>(), g0u = zero<T>(), g0d = zero<T>(), nn = zero<T>();
-		T xx = zero<T>(), zz = zero<T>(), ps = zero<T>();
+		T xx = zero<T>(), zz = zero<T>(), ps = zero<T>(), vv = zero<T>(), vn = zero<T>();
 		for (int q = a.ij_off[r]; q < a.ij_off[r + 1]; q++) {
 			const int e = a.ij_idx[q];
 			const int i = e % N, j = e / N;
@@ -162,8 +227,20 @@ __global__ void k_meas_uneqlt(MeasArgs<T> a)
 			xx += 0.25 * (dtij * (guii + gdii) - (guji * gdij + gdji * guij));
 			zz += 0.25 * ((gdii - guii) * (gdjj - gujj) + x);
 			ps += guij * gdij;
+			if (a.energy) {
+				// meas.c:791-798
+				const T nun = (1.0 - guii) * (1.0 - gujj) + (dtij - guji) * guij;
+				const T ndn = (1.0 - gdii) * (1.0 - gdjj) + (dtij - gdji) * gdij;
+				vv += nun * ndn;
+				vn += nun * (1.0 - gdii) + (1.0 - guii) * ndn;
+			}
 		}
 		const size_t o = (size_t)nij * t + r, st = (size_t)nij * L;
+		if (a.energy) {
+			T *ae = acc + a.lay.ue_energy + 2 * (size_t)a.num_bs * L;
+			ae[o] += pre * vv;
+			ae[st + o] += pre * vn;
+		}
 		a2[o] += pre * g0;
 		a2[st + o] += pre * g0u;
 		a2[2 * st + o] += pre * g0d;
@@ -172,9 +249,9 @@ __global__ void k_meas_uneqlt(MeasArgs<T> a)
 		a2[5 * st + o] += pre * zz;
 		a2[6 * st + o] += pre * ps;
 	}
-	if (!a.bond) return;
+	if (!a.bond && !a.pair_bb_only) return;
 	const int nb = a.num_b, nbb = a.num_bb;
-	T *a3 = acc + 1 + 7 * (size_t)nij * L;
+	T *a3 = acc + a.lay.pair_bb;
 	const T preb = phase / (double)a.degen_bb;
 	for (int bb = threadIdx.x; bb < nbb; bb += blockDim.x) {
 		T pbb = zero<T>(), jj = zero<T>(), jsjs = zero<T>(), kk = zero<T>(), ksks = zero<T>();
@@ -199,6 +276,8 @@ __global__ void k_meas_uneqlt(MeasArgs<T> a)
 			const T gdj0i0 = d0t[j0 + i0 * N], gdj1i0 = d0t[j1 + i0 * N];
 			const T gdj0i1 = d0t[j0 + i1 * N], gdj1i1 = d0t[j1 + i1 * N];
 			const T gdj1j0 = d00[j1 + j0 * N], gdj0j1 = d00[j0 + j1 * N];
+			pbb += 0.5 * (gui0j0 * gdi1j1 + gui1j0 * gdi0j1 + gui0j1 * gdi1j0 + gui1j1 * gdi0j0);
+			if (!a.bond) continue;   // pair_bb_only (meas.c:827-858)
 			const double e00 = (i0 == j0) ? dt : 0.0, e10 = (i1 == j0) ? dt : 0.0;
 			const double e01 = (i0 == j1) ? dt : 0.0, e11 = (i1 == j1) ? dt : 0.0;
 			// the eight exchange terms of meas.c:932-941, with their phases
@@ -206,7 +285,6 @@ __global__ void k_meas_uneqlt(MeasArgs<T> a)
 			          + pui0i1 * puj0j1 * ((e01 - guj1i0) * gui1j0) + pui1i0 * puj1j0 * ((e10 - guj0i1) * gui0j1);
 			const T y = pdi0i1 * pdj1j0 * ((e00 - gdj0i0) * gdi1j1) + pdi1i0 * pdj0j1 * ((e11 - gdj1i1) * gdi0j0)
 			          + pui0i1 * puj1j0 * ((e00 - guj0i0) * gui1j1) + pui1i0 * puj0j1 * ((e11 - guj1i1) * gui0j0);
-			pbb += 0.5 * (gui0j0 * gdi1j1 + gui1j0 * gdi0j1 + gui0j1 * gdi1j0 + gui1j1 * gdi0j0);
 			const T t0 = pui1i0 * gui0i1, t1 = pui0i1 * gui1i0, t2 = pdi1i0 * gdi0i1, t3 = pdi0i1 * gdi1i0;
 			const T t4 = puj1j0 * guj0j1, t5 = puj0j1 * guj1j0, t6 = pdj1j0 * gdj0j1, t7 = pdj0j1 * gdj1j0;
 			jj += (t0 - t1 + t2 - t3) * (t4 - t5 + t6 - t7) + x - y;
@@ -216,6 +294,7 @@ __global__ void k_meas_uneqlt(MeasArgs<T> a)
 		}
 		const size_t o = (size_t)nbb * t + bb, st = (size_t)nbb * L;
 		a3[o] += preb * pbb;
+		if (!a.bond) continue;
 		a3[st + o] += preb * jj;
 		a3[2 * st + o] += preb * jsjs;
 		a3[3 * st + o] += preb * kk;

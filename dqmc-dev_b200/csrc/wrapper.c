@@ -128,16 +128,75 @@ struct sim {
 	int eq_n, ue_n;
 	double *eq_acc, *ue_acc;      /* num arrays in the engine's layout */
 	int eq_size, ue_size;
+	int *tmap[9];                 /* the measurement toggles' maps, tmap_names order */
+	double *pp[4];                /* two-hop phases pp_u, pp_d, ppr_u, ppr_d (num) */
 };
+
+/* the measurement toggles and sizes appended to dqmc_params, with their
+ * dataset names (params/...) */
+static const char *toggle_int_names[] = {
+	"meas_energy_corr", "meas_thermal", "meas_2bond_corr", "meas_nematic_corr",
+	"meas_chiral", "meas_local_JQ", "meas_gen_suscept", "meas_pair_bb_only", "Nx", "Ny",
+	"num_plaq", "num_plaq_accum", "num_b_accum", "num_b2_accum", "num_bs", "num_b2",
+	"num_b2b", "num_bb2", "num_b2b2", "degen_plaq", "degen_b", "degen_b2", "degen_bs",
+	"degen_b2b", "degen_bb2", "degen_b2b2"};
+#define N_TOGGLE_INTS (int)(sizeof(toggle_int_names) / sizeof(toggle_int_names[0]))
+static const char *tmap_names[9] = {"plaqs", "map_plaq", "map_b", "map_bs", "bond2s", "map_b2",
+                                    "map_bb2", "map_b2b", "map_b2b2"};
+static const char *pp_names[4] = {"pp_u", "pp_d", "ppr_u", "ppr_d"};
+
+/* the accumulated datasets after `sign`, in the engine's accumulator order
+ * (csrc/meas.cuh), with the reference's names and sizes (data.c:441-522) */
+struct dset { const char *name; size_t n; };
+#define MAX_DSETS 48
+
+static int acc_sets(const dqmc_params *p, int uneqlt, struct dset *d)
+{
+	const size_t L = p->L, ni = p->num_i, nij = p->num_ij, nbb = p->num_bb, nbs = p->num_bs;
+	int k = 0;
+#define D(nm, cnt) d[k++] = (struct dset){nm, (cnt)}
+	if (!uneqlt) {
+		D("density", ni); D("density_u", ni); D("density_d", ni); D("double_occ", ni);
+		D("g00", nij); D("g00_u", nij); D("g00_d", nij); D("nn", nij); D("xx", nij);
+		D("zz", nij); D("pair_sw", nij);
+		if (p->meas_gen_suscept) {
+			D("uuuu", nij * nij); D("dddd", nij * nij); D("dduu", nij * nij); D("uudd", nij * nij);
+		}
+		if (p->meas_chiral) D("chi", (size_t)p->num_plaq_accum);
+		if (p->meas_energy_corr) { D("kk", nbb); D("kv", nbs); D("kn", nbs); D("vv", nij); D("vn", nij); }
+		if (p->meas_local_JQ) {
+			D("j", (size_t)p->num_b_accum); D("jn", (size_t)p->num_b_accum);
+			D("j2", (size_t)p->num_b2_accum);
+		}
+		return k;
+	}
+	D("gt0", nij * L); D("gt0_u", nij * L); D("gt0_d", nij * L); D("nn", nij * L);
+	D("xx", nij * L); D("zz", nij * L); D("pair_sw", nij * L);
+	if (p->meas_gen_suscept) {
+		D("uuuu", nij * nij * L); D("dddd", nij * nij * L);
+		D("dduu", nij * nij * L); D("uudd", nij * nij * L);
+	}
+	if (p->meas_bond_corr || p->meas_pair_bb_only) D("pair_bb", nbb * L);
+	if (p->meas_bond_corr) { D("jj", nbb * L); D("jsjs", nbb * L); D("kk", nbb * L); D("ksks", nbb * L); }
+	if (p->meas_thermal) {
+		D("j2jn", (size_t)p->num_b2b * L); D("jnj2", (size_t)p->num_bb2 * L);
+		D("jnjn", nbb * L); D("jnj", nbb * L); D("jjn", nbb * L);
+	}
+	if (p->meas_2bond_corr) {
+		const size_t n4 = (size_t)p->num_b2b2 * L;
+		D("pair_b2b2", n4); D("j2j2", n4); D("j2j", (size_t)p->num_b2b * L);
+		D("jj2", (size_t)p->num_bb2 * L); D("js2js2", n4); D("k2k2", n4); D("ks2ks2", n4);
+	}
+	if (p->meas_energy_corr) { D("kv", nbs * L); D("kn", nbs * L); D("vv", nij * L); D("vn", nij * L); }
+	if (p->meas_nematic_corr) { D("nem_nnnn", nbb * L); D("nem_ssss", nbb * L); }
+#undef D
+	return k;
+}
 
 static const char *mat_names[8] = {
 	"params/exp_Ku", "params/exp_Kd", "params/inv_exp_Ku", "params/inv_exp_Kd",
 	"params/exp_halfKu", "params/exp_halfKd", "params/inv_exp_halfKu", "params/inv_exp_halfKd"};
 
-static const char *eq_i_names[4] = {"density", "density_u", "density_d", "double_occ"};
-static const char *eq_ij_names[7] = {"g00", "g00_u", "g00_d", "nn", "xx", "zz", "pair_sw"};
-static const char *ue_ij_names[7] = {"gt0", "gt0_u", "gt0_d", "nn", "xx", "zz", "pair_sw"};
-static const char *ue_bb_names[5] = {"pair_bb", "jj", "jsjs", "kk", "ksks"};
 
 static void sim_free(struct sim *s)
 {
@@ -146,6 +205,8 @@ static void sim_free(struct sim *s)
 	for (int i = 0; i < 8; i++) free(s->mats[i]);
 	free(s->exp_lambda); free(s->del); free(s->hs);
 	free(s->eq_acc); free(s->ue_acc);
+	for (int i = 0; i < 9; i++) free(s->tmap[i]);
+	for (int i = 0; i < 4; i++) free(s->pp[i]);
 	memset(s, 0, sizeof(*s));
 }
 
@@ -188,21 +249,21 @@ static int sim_read(struct sim *s)
 		{"state/sweep", &s->sweep},
 	};
 	for (size_t i = 0; i < sizeof(sc) / sizeof(sc[0]); i++) TRY(dqsf_read_int(f, sc[i].n, sc[i].d, 1));
-	/* toggles this engine does not carry are refused, as a reference build
-	 * without them would mis-read the file */
-	const char *unsupported[] = {"params/meas_thermal", "params/meas_2bond_corr",
-		"params/meas_energy_corr", "params/meas_nematic_corr", "params/meas_chiral",
-		"params/meas_local_JQ", "params/meas_gen_suscept", "params/meas_pair_bb_only"};
-	for (size_t i = 0; i < sizeof(unsupported) / sizeof(unsupported[0]); i++) {
-		int v = 0;
-		if (dqsf_has(f, unsupported[i])) TRY(dqsf_read_int(f, unsupported[i], &v, 1));
-		if (v) {
-			fprintf(stderr, "%s = %d is not supported by this engine\n", unsupported[i], v);
-			dqsf_close(f);
-			sim_free(s);
-			return DQSF_RW_FAIL;
-		}
+	/* the measurement toggles and the sizes of their maps (absent: 0) */
+	int *tf[N_TOGGLE_INTS] = {&p->meas_energy_corr, &p->meas_thermal, &p->meas_2bond_corr,
+		&p->meas_nematic_corr, &p->meas_chiral, &p->meas_local_JQ, &p->meas_gen_suscept,
+		&p->meas_pair_bb_only, &p->Nx, &p->Ny, &p->num_plaq, &p->num_plaq_accum,
+		&p->num_b_accum, &p->num_b2_accum, &p->num_bs, &p->num_b2, &p->num_b2b, &p->num_bb2,
+		&p->num_b2b2, &p->degen_plaq, &p->degen_b, &p->degen_b2, &p->degen_bs, &p->degen_b2b,
+		&p->degen_bb2, &p->degen_b2b2};
+	for (int i = 0; i < N_TOGGLE_INTS; i++) {
+		char nm[64];
+		snprintf(nm, sizeof(nm), "params/%s", toggle_int_names[i]);
+		*tf[i] = 0;
+		if (dqsf_has(f, nm)) TRY(dqsf_read_int(f, nm, tf[i], 1));
 	}
+	/* files written without the two-hop bond family run with num_b2 = 0 */
+	if (!dqsf_has(f, "params/bond2s") || !dqsf_has(f, "params/map_b2b2")) p->num_b2 = 0;
 	int dt;
 	size_t cnt;
 	TRY(dqsf_info(f, "params/exp_Ku", &dt, &cnt));
@@ -215,10 +276,12 @@ static int sim_read(struct sim *s)
 	s->num_b_alloc = p->num_b > 0 ? p->num_b : 1;
 	s->bonds = calloc(2 * (size_t)s->num_b_alloc, sizeof(int));
 	s->map_bb = calloc((size_t)s->num_b_alloc * s->num_b_alloc, sizeof(int));
-	if (p->meas_bond_corr && p->num_b > 0) {
+	/* the bonds and bond-pair map feed the bond correlators and most
+	 * toggles: read them whenever the file has them */
+	if (p->num_b > 0 && dqsf_has(f, "params/bonds"))
 		TRY(dqsf_read_int(f, "params/bonds", s->bonds, 2 * (size_t)p->num_b));
+	if (p->num_b > 0 && dqsf_has(f, "params/map_bb"))
 		TRY(dqsf_read_int(f, "params/map_bb", s->map_bb, (size_t)p->num_b * p->num_b));
-	}
 	s->peierlsu = calloc(NN * w, sizeof(double));
 	s->peierlsd = calloc(NN * w, sizeof(double));
 	TRY(rd_num(f, "params/peierlsu", s->peierlsu, NN, s->cplx));
@@ -239,33 +302,47 @@ static int sim_read(struct sim *s)
 	p->exp_Ku = s->mats[0]; p->exp_Kd = s->mats[1]; p->inv_exp_Ku = s->mats[2];
 	p->inv_exp_Kd = s->mats[3]; p->exp_halfKu = s->mats[4]; p->exp_halfKd = s->mats[5];
 	p->inv_exp_halfKu = s->mats[6]; p->inv_exp_halfKd = s->mats[7];
+	/* the measurement toggles' maps and two-hop phases, where present */
+	const size_t nb = p->num_b, nb2 = p->num_b2, npl = p->num_plaq;
+	const size_t tmap_n[9] = {3 * npl, npl, nb, N * nb, 2 * nb2, nb2, nb * nb2, nb2 * nb, nb2 * nb2};
+	for (int i = 0; i < 9; i++) {
+		char nm[64];
+		snprintf(nm, sizeof(nm), "params/%s", tmap_names[i]);
+		if (tmap_n[i] == 0 || !dqsf_has(f, nm)) continue;
+		s->tmap[i] = calloc(tmap_n[i], sizeof(int));
+		TRY(dqsf_read_int(f, nm, s->tmap[i], tmap_n[i]));
+	}
+	for (int i = 0; i < 4; i++) {
+		char nm[64];
+		snprintf(nm, sizeof(nm), "params/%s", pp_names[i]);
+		if (nb2 == 0 || !dqsf_has(f, nm)) continue;
+		s->pp[i] = calloc(nb2 * w, sizeof(double));
+		TRY(rd_num(f, nm, s->pp[i], nb2, s->cplx));
+	}
+	p->plaqs = s->tmap[0]; p->map_plaq = s->tmap[1]; p->map_b = s->tmap[2];
+	p->map_bs = s->tmap[3]; p->bond2s = s->tmap[4]; p->map_b2 = s->tmap[5];
+	p->map_bb2 = s->tmap[6]; p->map_b2b = s->tmap[7]; p->map_b2b2 = s->tmap[8];
+	p->pp_u = s->pp[0]; p->pp_d = s->pp[1]; p->ppr_u = s->pp[2]; p->ppr_d = s->pp[3];
 	dqmc_acc_sizes(p, &s->eq_size, &s->ue_size);
 	s->eq_acc = calloc((size_t)s->eq_size * w, sizeof(double));
 	s->ue_acc = calloc((size_t)(s->ue_size ? s->ue_size : 1) * w, sizeof(double));
 	char name[128];
-	const size_t ni = p->num_i, nij = p->num_ij, nbb = p->num_bb;
+	struct dset ds[MAX_DSETS];
 	TRY(dqsf_read_int(f, "meas_eqlt/n_sample", &s->eq_n, 1));
 	TRY(rd_num(f, "meas_eqlt/sign", s->eq_acc, 1, s->cplx));
-	for (int k = 0; k < 4; k++) {
-		snprintf(name, sizeof(name), "meas_eqlt/%s", eq_i_names[k]);
-		TRY(rd_num(f, name, s->eq_acc + w * (1 + k * ni), ni, s->cplx));
-	}
-	for (int k = 0; k < 7; k++) {
-		snprintf(name, sizeof(name), "meas_eqlt/%s", eq_ij_names[k]);
-		TRY(rd_num(f, name, s->eq_acc + w * (1 + 4 * ni + k * nij), nij, s->cplx));
+	size_t o = 1;
+	for (int k = 0, n = acc_sets(p, 0, ds); k < n; o += ds[k].n, k++) {
+		snprintf(name, sizeof(name), "meas_eqlt/%s", ds[k].name);
+		TRY(rd_num(f, name, s->eq_acc + w * o, ds[k].n, s->cplx));
 	}
 	if (p->period_uneqlt > 0) {
 		TRY(dqsf_read_int(f, "meas_uneqlt/n_sample", &s->ue_n, 1));
 		TRY(rd_num(f, "meas_uneqlt/sign", s->ue_acc, 1, s->cplx));
-		for (int k = 0; k < 7; k++) {
-			snprintf(name, sizeof(name), "meas_uneqlt/%s", ue_ij_names[k]);
-			TRY(rd_num(f, name, s->ue_acc + w * (1 + k * nij * L), nij * L, s->cplx));
+		o = 1;
+		for (int k = 0, n = acc_sets(p, 1, ds); k < n; o += ds[k].n, k++) {
+			snprintf(name, sizeof(name), "meas_uneqlt/%s", ds[k].name);
+			TRY(rd_num(f, name, s->ue_acc + w * o, ds[k].n, s->cplx));
 		}
-		if (p->meas_bond_corr)
-			for (int k = 0; k < 5; k++) {
-				snprintf(name, sizeof(name), "meas_uneqlt/%s", ue_bb_names[k]);
-				TRY(rd_num(f, name, s->ue_acc + w * (1 + 7 * nij * L + k * nbb * L), nbb * L, s->cplx));
-			}
 	}
 	return dqsf_close(f);
 }
@@ -290,33 +367,26 @@ static int sim_save(const struct sim *s)
 	fflush(NULL);
 	const dqmc_params *p = &s->p;
 	const size_t L = p->L, w = s->cplx ? 2 : 1;
-	const size_t ni = p->num_i, nij = p->num_ij, nbb = p->num_bb;
 	char name[128];
+	struct dset ds[MAX_DSETS];
 	TRYW(dqsf_write_u64(f, "state/rng", s->rng, 17));
 	TRYW(dqsf_write_int(f, "state/sweep", &s->sweep, 1));
 	TRYW(dqsf_write_int(f, "state/hs", s->hs, (size_t)p->N * L));
 	TRYW(dqsf_write_int(f, "meas_eqlt/n_sample", &s->eq_n, 1));
 	TRYW(wr_num(f, "meas_eqlt/sign", s->eq_acc, 1, s->cplx));
-	for (int k = 0; k < 4; k++) {
-		snprintf(name, sizeof(name), "meas_eqlt/%s", eq_i_names[k]);
-		TRYW(wr_num(f, name, s->eq_acc + w * (1 + k * ni), ni, s->cplx));
-	}
-	for (int k = 0; k < 7; k++) {
-		snprintf(name, sizeof(name), "meas_eqlt/%s", eq_ij_names[k]);
-		TRYW(wr_num(f, name, s->eq_acc + w * (1 + 4 * ni + k * nij), nij, s->cplx));
+	size_t o = 1;
+	for (int k = 0, n = acc_sets(p, 0, ds); k < n; o += ds[k].n, k++) {
+		snprintf(name, sizeof(name), "meas_eqlt/%s", ds[k].name);
+		TRYW(wr_num(f, name, s->eq_acc + w * o, ds[k].n, s->cplx));
 	}
 	if (p->period_uneqlt > 0) {
 		TRYW(dqsf_write_int(f, "meas_uneqlt/n_sample", &s->ue_n, 1));
 		TRYW(wr_num(f, "meas_uneqlt/sign", s->ue_acc, 1, s->cplx));
-		for (int k = 0; k < 7; k++) {
-			snprintf(name, sizeof(name), "meas_uneqlt/%s", ue_ij_names[k]);
-			TRYW(wr_num(f, name, s->ue_acc + w * (1 + k * nij * L), nij * L, s->cplx));
+		o = 1;
+		for (int k = 0, n = acc_sets(p, 1, ds); k < n; o += ds[k].n, k++) {
+			snprintf(name, sizeof(name), "meas_uneqlt/%s", ds[k].name);
+			TRYW(wr_num(f, name, s->ue_acc + w * o, ds[k].n, s->cplx));
 		}
-		if (p->meas_bond_corr)
-			for (int k = 0; k < 5; k++) {
-				snprintf(name, sizeof(name), "meas_uneqlt/%s", ue_bb_names[k]);
-				TRYW(wr_num(f, name, s->ue_acc + w * (1 + 7 * nij * L + k * nbb * L), nbb * L, s->cplx));
-			}
 	}
 	fflush(NULL);
 	pw = 0;
@@ -538,7 +608,9 @@ cleanup:
 static int same_group(const struct sim *a, const struct sim *b)
 {
 	const dqmc_params *p = &a->p, *q = &b->p;
-	if (memcmp(&p->N, &q->N, sizeof(int) * 18) != 0 || a->sweep != b->sweep ||
+	if (memcmp(&p->N, &q->N, sizeof(int) * 18) != 0 ||
+	    memcmp(&p->meas_energy_corr, &q->meas_energy_corr, sizeof(int) * N_TOGGLE_INTS) != 0 ||
+	    a->sweep != b->sweep ||
 	    a->checkpoint_every != b->checkpoint_every)
 		return 0;
 	const size_t NN = (size_t)p->N * p->N, w = a->cplx ? 2 : 1;

@@ -29,6 +29,47 @@ def _scalar(v) -> int:
     return int(np.asarray(v).reshape(-1)[0])
 
 
+def acc_datasets(p: dict):
+    """The accumulated datasets after `sign`, in the engine's accumulator
+    order (dqmc-dev_b200/csrc/meas.cuh), as (name, size) lists for the
+    equal-time and unequal-time groups; the names and sizes are the
+    reference's (data.c:441-522)."""
+    L, ni, nij, nbb = p["L"], p["num_i"], p["num_ij"], p["num_bb"]
+    g = lambda k: p.get(k, 0)  # noqa: E731
+    eq = [(k, ni) for k in EQ_I] + [(k, nij) for k in EQ_IJ]
+    if g("meas_gen_suscept"):
+        eq += [(k, nij * nij) for k in ("uuuu", "dddd", "dduu", "uudd")]
+    if g("meas_chiral"):
+        eq += [("chi", g("num_plaq_accum"))]
+    if g("meas_energy_corr"):
+        eq += [("kk", nbb), ("kv", g("num_bs")), ("kn", g("num_bs")), ("vv", nij), ("vn", nij)]
+    if g("meas_local_JQ"):
+        eq += [("j", g("num_b_accum")), ("jn", g("num_b_accum")), ("j2", g("num_b2_accum"))]
+    ue = []
+    if p["period_uneqlt"] > 0:
+        ue = [(k, nij * L) for k in UE_IJ]
+        if g("meas_gen_suscept"):
+            ue += [(k, nij * nij * L) for k in ("uuuu", "dddd", "dduu", "uudd")]
+        if p["meas_bond_corr"] or g("meas_pair_bb_only"):
+            ue += [("pair_bb", nbb * L)]
+        if p["meas_bond_corr"]:
+            ue += [(k, nbb * L) for k in UE_BB[1:]]
+        if g("meas_thermal"):
+            ue += [("j2jn", g("num_b2b") * L), ("jnj2", g("num_bb2") * L)]
+            ue += [(k, nbb * L) for k in ("jnjn", "jnj", "jjn")]
+        if g("meas_2bond_corr"):
+            nb2b2 = g("num_b2b2") * L
+            ue += [("pair_b2b2", nb2b2), ("j2j2", nb2b2), ("j2j", g("num_b2b") * L),
+                   ("jj2", g("num_bb2") * L), ("js2js2", nb2b2), ("k2k2", nb2b2),
+                   ("ks2ks2", nb2b2)]
+        if g("meas_energy_corr"):
+            ue += [("kv", g("num_bs") * L), ("kn", g("num_bs") * L), ("vv", nij * L),
+                   ("vn", nij * L)]
+        if g("meas_nematic_corr"):
+            ue += [("nem_nnnn", nbb * L), ("nem_ssss", nbb * L)]
+    return eq, ue
+
+
 class SimData:
     """Parameters, state and accumulators of one sim file, as numpy arrays."""
 
@@ -38,6 +79,8 @@ class SimData:
         nt = np.complex128 if self.cplx else np.float64
         self.nt = nt
         self.p = {k: _scalar(d["params/" + k]) for k in INT_PARAMS}
+        self.p.update({k: _scalar(d["params/" + k]) if "params/" + k in d else 0
+                       for k in _lib.TOGGLE_INTS})
         N, L = self.p["N"], self.p["L"]
         self.N, self.L = N, L
         a = lambda k, t: np.ascontiguousarray(np.asarray(d[k], dtype=t).reshape(-1))  # noqa: E731
@@ -49,24 +92,27 @@ class SimData:
         self.peierlsu = a("params/peierlsu", nt)
         self.peierlsd = a("params/peierlsd", nt)
         self.mats = {k: a("params/" + k, nt) for k in MATS}
+        # the measurement toggles' maps and two-hop phases (absent: empty)
+        self.tmaps = {}
+        for k in _lib.TOGGLE_PTRS:
+            t = nt if k.startswith("pp") else np.int32
+            self.tmaps[k] = a("params/" + k, t) if "params/" + k in d else np.zeros(1, t)
         self.exp_lambda = a("params/exp_lambda", np.float64)
         self.del_ = a("params/del", np.float64)
         self.rng = a("state/rng", np.uint64).copy()
         self.sweep = _scalar(d["state/sweep"])
         self.hs = a("state/hs", np.int32).copy()
-        ni, nij, nbb = self.p["num_i"], self.p["num_ij"], self.p["num_bb"]
+        self._eq_sets, self._ue_sets = acc_datasets(self.p)
         self.eq_n = _scalar(d["meas_eqlt/n_sample"])
-        parts = [a("meas_eqlt/sign", nt)] + [a("meas_eqlt/" + k, nt) for k in EQ_I + EQ_IJ]
+        parts = [a("meas_eqlt/sign", nt)] + [a("meas_eqlt/" + k, nt) for k, _ in self._eq_sets]
         self.eq_acc = np.concatenate(parts).astype(nt)
         self.ue_n = 0
         self.ue_acc = np.zeros(1, nt)
         if self.p["period_uneqlt"] > 0:
             self.ue_n = _scalar(d["meas_uneqlt/n_sample"])
-            parts = [a("meas_uneqlt/sign", nt)] + [a("meas_uneqlt/" + k, nt) for k in UE_IJ]
-            if self.p["meas_bond_corr"]:
-                parts += [a("meas_uneqlt/" + k, nt) for k in UE_BB]
+            parts = [a("meas_uneqlt/sign", nt)] + [a("meas_uneqlt/" + k, nt)
+                                                    for k, _ in self._ue_sets]
             self.ue_acc = np.concatenate(parts).astype(nt)
-        self._sizes = (ni, nij, nbb)
 
     def clone(self) -> "SimData":
         """An independent copy (state and accumulators included)."""
@@ -92,31 +138,25 @@ class SimData:
         for k, v in self.mats.items():
             setattr(p, k, v.ctypes.data)
             keep.append(v)
+        for k, v in self.tmaps.items():
+            setattr(p, k, v.ctypes.data)
+            keep.append(v)
         return p, keep
 
     def measurements(self) -> dict:
         """Accumulators as the datasets the reference writes (data.c:687-789)."""
-        ni, nij, nbb = self._sizes
-        L = self.L
         out = {"meas_eqlt/n_sample": self.eq_n, "meas_eqlt/sign": self.eq_acc[0]}
         o = 1
-        for k in EQ_I:
-            out["meas_eqlt/" + k] = self.eq_acc[o:o + ni]
-            o += ni
-        for k in EQ_IJ:
-            out["meas_eqlt/" + k] = self.eq_acc[o:o + nij]
-            o += nij
+        for k, n in self._eq_sets:
+            out["meas_eqlt/" + k] = self.eq_acc[o:o + n]
+            o += n
         if self.p["period_uneqlt"] > 0:
             out["meas_uneqlt/n_sample"] = self.ue_n
             out["meas_uneqlt/sign"] = self.ue_acc[0]
             o = 1
-            for k in UE_IJ:
-                out["meas_uneqlt/" + k] = self.ue_acc[o:o + nij * L]
-                o += nij * L
-            if self.p["meas_bond_corr"]:
-                for k in UE_BB:
-                    out["meas_uneqlt/" + k] = self.ue_acc[o:o + nbb * L]
-                    o += nbb * L
+            for k, n in self._ue_sets:
+                out["meas_uneqlt/" + k] = self.ue_acc[o:o + n]
+                o += n
         return out
 
     def save(self, path: str | None = None):
@@ -204,6 +244,15 @@ class Engine:
         _lib.check(self.lib.dqmc_engine_obs_grad(self.h, obs.ctypes.data, Z.ctypes.data),
                    "dqmc_engine_obs_grad")
         return obs.reshape(n, 2), Z.reshape(n, 2, 2, N, N).transpose(0, 1, 2, 4, 3)
+
+    def set_hopping(self, mats: dict):
+        """Replace the eight hopping matrices (names as MATS, N x N arrays of
+        the engine's scalar type) of every chain in place
+        (dqmc_engine_set_hopping); G follows before the next use."""
+        nt = self.sims[0].nt
+        col = [np.ascontiguousarray(np.asarray(mats[k], dtype=nt).T).reshape(-1) for k in MATS]
+        _lib.check(self.lib.dqmc_engine_set_hopping(self.h, *[c.ctypes.data for c in col]),
+                   "dqmc_engine_set_hopping")
 
     def stream(self) -> int:
         return int(self.lib.dqmc_engine_stream(self.h) or 0)

@@ -27,8 +27,12 @@ function, d <X> = sum_l tr[W_l dGst(l, l)] and dGst = -Gst dO Gst collapse to
 tr[Z D_theta] with Z = sum_m s_m exp(V_m) Y_m exp(-dt K) and
 Y_m = sum_l Gst(m, l) W_l Gst(l, m+1) (W_l the observable's weights).
 
-LogDet wraps the log-determinant in a torch.autograd.Function: the forward
-runs the sweep and keeps the per-configuration gradients for the backward.
+LogDet and Observables wrap the log-determinant and (<n>, <docc>) in
+torch.autograd.Functions: the forward runs the engine and keeps the
+per-configuration gradients for the backward.  A model keeps one engine for
+all its evaluations: a new theta only replaces the hopping matrices
+(dqmc_engine_set_hopping), so repeated evaluations allocate no device
+memory, and the parameter contraction runs on the device.
 """
 from __future__ import annotations
 
@@ -77,6 +81,8 @@ class SquareModel:
             dK[1, j, i] -= 1.0
         dK[2] -= np.eye(N)
         self.dK = dK
+        self._eng = None
+        self._dK_dev = None
 
     def K(self, theta: np.ndarray) -> np.ndarray:
         t, tp, mu, h = theta[0], theta[1], theta[2], theta[3:]
@@ -91,16 +97,20 @@ class SquareModel:
         K -= mu * np.eye(N)
         return K
 
-    def _sims(self, K: np.ndarray) -> list[SimData]:
+    def _hopping(self, K: np.ndarray) -> dict:
+        """the eight matrices exp(-+dt K), exp(-+dt K / 2), both spins"""
         from scipy.linalg import expm
         dt = self.dt
-        d0 = gen.make_sim(Nx=self.Nx, Ny=self.Ny, U=self.U, dt=dt, L=self.L,
-                          n_matmul=self.n_matmul, period_eqlt=self.n_matmul, n_sweep_warm=0,
-                          n_sweep_meas=1)
         mats = {"exp_Ku": expm(-dt * K), "inv_exp_Ku": expm(dt * K),
                 "exp_halfKu": expm(-dt / 2 * K), "inv_exp_halfKu": expm(dt / 2 * K)}
         for k in list(mats):
-            mats[k.replace("u", "d") if k.endswith("u") else k] = mats[k]
+            mats[k[:-1] + "d"] = mats[k]
+        return mats
+
+    def _sims(self, K: np.ndarray, mats: dict) -> list[SimData]:
+        d0 = gen.make_sim(Nx=self.Nx, Ny=self.Ny, U=self.U, dt=self.dt, L=self.L,
+                          n_matmul=self.n_matmul, period_eqlt=self.n_matmul, n_sweep_warm=0,
+                          n_sweep_meas=1)
         for k, v in mats.items():
             d0["params/" + k] = v
         d0["params/Ku"], d0["params/Kd"] = K, K.copy()
@@ -110,6 +120,56 @@ class SquareModel:
             d["state/hs"] = self.fields[c]
             out.append(SimData(d))
         return out
+
+    def engine(self, K: np.ndarray) -> Engine:
+        """The model's engine with hopping K: created (and its device buffers
+        allocated) by the first evaluation, then only its hopping matrices
+        change (dqmc_engine_set_hopping)."""
+        mats = self._hopping(K)
+        if self._eng is None:
+            self._eng = Engine(self._sims(K, mats), device=self.device)
+        else:
+            self._eng.set_hopping(mats)
+        return self._eng
+
+    def close(self):
+        if self._eng is not None:
+            self._eng.close()
+            self._eng = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _contract(self, V, w, X):
+        """sum_ij (V^T X_c V)_ji w_ij (V^T dK_k V)_ij for every leading
+        index c of X (shape [..., 2 spins, N, N], summed over the spins) and
+        parameter k, on the device when one is present: two batched products
+        and one (c, ij) x (ij, k) product"""
+        try:
+            import torch
+        except ImportError:  # pragma: no cover - torch is part of the environment
+            torch = None
+        lead = X.shape[:-3]
+        N = self.N
+        if torch is not None and torch.cuda.is_available() and self.device >= 0:
+            dev = torch.device("cuda", self.device)
+            Vt = torch.from_numpy(V).to(dev)
+            if self._dK_dev is None:
+                self._dK_dev = torch.from_numpy(self.dK).to(dev)
+            E = Vt.T @ self._dK_dev @ Vt                                   # [k, i, j]
+            Xs = torch.from_numpy(np.ascontiguousarray(X)).to(dev).sum(-3)  # [..., a, b]
+            Xp = Vt.T @ Xs.reshape(-1, N, N) @ Vt                          # [c, i, j]
+            W = torch.from_numpy(w).to(dev)
+            A = (Xp.transpose(-1, -2) * W).reshape(-1, N * N)             # [c, ij]
+            out = (A @ E.reshape(-1, N * N).T).cpu().numpy()
+        else:
+            E = np.einsum("ai,kab,bj->kij", V, self.dK, V, optimize=True)
+            Xp = np.einsum("ai,...sab,bj->...ij", V, X, V, optimize=True).reshape(-1, N, N)
+            out = np.einsum("cji,ij,kij->ck", Xp, w, E, optimize=True)
+        return out.reshape(lead + (self.n_params,))
 
     def d_theta(self, K: np.ndarray):
         """(V, weights) with D_theta = V [(V^T dK_theta V) * weights] V^T:
@@ -129,18 +189,10 @@ class SquareModel:
         (n_cfg x n_params) at the parameters theta."""
         theta = np.asarray(theta, dtype=np.float64)
         K = self.K(theta)
-        sims = self._sims(K)
-        e = Engine(sims, device=self.device)
-        try:
-            ld, S = e.logdet_grad()
-        finally:
-            e.close()
+        ld, S = self.engine(K).logdet_grad()
         V, w = self.d_theta(K)
-        E = np.einsum("ai,kab,bj->kij", V, self.dK, V, optimize=True)    # V^T dK V
-        Sp = np.einsum("ai,csab,bj->cij", V, S, V, optimize=True)        # V^T (S_up + S_dn) V
-        # tr[S D] = sum_ij (V^T S V)_ji w_ij E_ij
-        grad = np.einsum("cji,ij,kij->ck", Sp, w, E, optimize=True)
-        return ld, grad
+        # tr[S D_k] = sum_ij (V^T (S_up + S_dn) V)_ji w_ij (V^T dK_k V)_ij
+        return ld, self._contract(V, w, S)
 
 
     def evaluate_obs(self, theta) -> tuple[np.ndarray, np.ndarray]:
@@ -149,16 +201,9 @@ class SquareModel:
         space-time Green's function (dqmc_engine_obs_grad)."""
         theta = np.asarray(theta, dtype=np.float64)
         K = self.K(theta)
-        sims = self._sims(K)
-        e = Engine(sims, device=self.device)
-        try:
-            obs, Z = e.obs_grad()
-        finally:
-            e.close()
+        obs, Z = self.engine(K).obs_grad()
         V, w = self.d_theta(K)
-        E = np.einsum("ai,kab,bj->kij", V, self.dK, V, optimize=True)
-        Zp = np.einsum("ai,cosab,bj->coij", V, Z, V, optimize=True)
-        return obs, np.einsum("coji,ij,kij->cok", Zp, w, E, optimize=True)
+        return obs, self._contract(V, w, Z)
 
 
 try:
@@ -179,5 +224,22 @@ try:
         def backward(ctx, g):
             (grad,) = ctx.saved_tensors
             return (g[:, None].to(grad.dtype) * grad).sum(0), None
+
+    class Observables(torch.autograd.Function):
+        """y_c = (<n>, <docc>) of configuration c at fixed fields as a
+        function of theta; the backward contracts the incoming gradient
+        with the per-configuration gradients of the forward
+        (SquareModel.evaluate_obs)."""
+
+        @staticmethod
+        def forward(ctx, theta, model: SquareModel):
+            obs, grad = model.evaluate_obs(theta.detach().cpu().numpy())
+            ctx.save_for_backward(torch.from_numpy(grad).to(theta.device))
+            return torch.from_numpy(obs).to(theta.device)
+
+        @staticmethod
+        def backward(ctx, g):
+            (grad,) = ctx.saved_tensors
+            return (g[:, :, None].to(grad.dtype) * grad).sum((0, 1)), None
 except ImportError:  # pragma: no cover - torch is part of the environment
-    LogDet = None
+    LogDet = Observables = None

@@ -29,9 +29,21 @@ EXPORTS = [
     "dqmc_engine_accepts", "dqmc_engine_stream", "dqmc_engine_lanes",
     "dqmc_engine_set_chains", "dqmc_engine_get_chains", "dqmc_engine_launches_per_sweep",
     "dqmc_engine_profile_sweep", "dqmc_engine_logdet_grad", "dqmc_engine_obs_grad",
+    "dqmc_engine_set_hopping",
     "dqmc_gpu_gemm", "dqmc_gpu_calc_eq_g", "dqmc_gpu_update_delayed", "dqmc_gpu_mul_seq",
     "dqmc_gpu_calc_eq_g_noalloc",
 ]
+
+
+# the measurement toggles and their maps, appended to dqmc_params
+TOGGLES = ("meas_energy_corr", "meas_thermal", "meas_2bond_corr", "meas_nematic_corr",
+           "meas_chiral", "meas_local_JQ", "meas_gen_suscept", "meas_pair_bb_only")
+TOGGLE_INTS = TOGGLES + (
+    "Nx", "Ny", "num_plaq", "num_plaq_accum", "num_b_accum", "num_b2_accum",
+    "num_bs", "num_b2", "num_b2b", "num_bb2", "num_b2b2",
+    "degen_plaq", "degen_b", "degen_b2", "degen_bs", "degen_b2b", "degen_bb2", "degen_b2b2")
+TOGGLE_PTRS = ("plaqs", "map_plaq", "map_b", "map_bs", "bond2s", "map_b2", "map_bb2",
+               "map_b2b", "map_b2b2", "pp_u", "pp_d", "ppr_u", "ppr_d")
 
 
 class Params(C.Structure):
@@ -45,6 +57,8 @@ class Params(C.Structure):
             "map_i", "map_ij", "bonds", "map_bb", "peierlsu", "peierlsd",
             "exp_Ku", "exp_Kd", "inv_exp_Ku", "inv_exp_Kd",
             "exp_halfKu", "exp_halfKd", "inv_exp_halfKu", "inv_exp_halfKd")]
+        + [(n, C.c_int) for n in TOGGLE_INTS]
+        + [(n, C.c_void_p) for n in TOGGLE_PTRS]
     )
 
 
@@ -88,6 +102,7 @@ def load(path: str | None = None):
         "dqmc_engine_profile_sweep": (i, [vp, i, i, C.POINTER(C.c_double), i]),
         "dqmc_engine_logdet_grad": (i, [vp, vp, vp]),
         "dqmc_engine_obs_grad": (i, [vp, vp, vp]),
+        "dqmc_engine_set_hopping": (i, [vp] * 9),
         "dqmc_gpu_gemm": (i, [i, i, i, i, i, vp, vp, i, C.c_longlong, vp, i, C.c_longlong, vp,
                               vp, i, C.c_longlong, vp]),
         "dqmc_gpu_calc_eq_g": (i, [i, i, i, i, i, vp, vp, vp, vp]),

@@ -71,10 +71,25 @@ typedef struct {
 	const void *peierlsu, *peierlsd;  /* num[N*N] */
 	const void *exp_Ku, *exp_Kd, *inv_exp_Ku, *inv_exp_Kd;
 	const void *exp_halfKu, *exp_halfKd, *inv_exp_halfKu, *inv_exp_halfKd;
+	/* The measurement toggles beyond meas_bond_corr (struct params,
+	 * src/data.h:21-26; 0 = off) and the maps they read, as the sim file's
+	 * params group holds them.  All zero / NULL when no toggle is on. */
+	int meas_energy_corr, meas_thermal, meas_2bond_corr, meas_nematic_corr;
+	int meas_chiral, meas_local_JQ, meas_gen_suscept, meas_pair_bb_only;
+	int Nx, Ny;
+	int num_plaq, num_plaq_accum, num_b_accum, num_b2_accum;
+	int num_bs, num_b2, num_b2b, num_bb2, num_b2b2;
+	int degen_plaq, degen_b, degen_b2, degen_bs, degen_b2b, degen_bb2, degen_b2b2;
+	const int *plaqs, *map_plaq;             /* [3*num_plaq], [num_plaq] */
+	const int *map_b, *map_bs;               /* [num_b], [N*num_b] */
+	const int *bond2s, *map_b2;              /* [2*num_b2], [num_b2] */
+	const int *map_bb2, *map_b2b, *map_b2b2; /* [num_b*num_b2] x 2, [num_b2^2] */
+	const void *pp_u, *pp_d, *ppr_u, *ppr_d; /* num[num_b2] */
 } dqmc_params;
 
 /* Accumulator sizes in num elements per chain (layout documented in
- * dqmc-dev_b200/csrc/meas.cuh: sign, then the datasets in data.h order). */
+ * dqmc-dev_b200/csrc/meas.cuh: sign, the always-on datasets, then those of
+ * each enabled toggle). */
 int dqmc_acc_sizes(const dqmc_params *p, int *eq_size, int *ue_size);
 
 /* An engine advances n_chain chains of one parameter set (the batched form
@@ -177,6 +192,16 @@ int dqmc_engine_logdet_grad(dqmc_engine *e, double *logdet, void *S);
  * corner block m = L-1 and +1 otherwise.  Needs 2 (N L)^2 nums of device
  * memory per chain and spin for the duration of the call. */
 int dqmc_engine_obs_grad(dqmc_engine *e, double *obs, void *Z);
+
+/* Replaces the hopping matrices of every chain (the eight exp(-+dt K) and
+ * exp(-+dt K / 2) of dqmc_params, both spins) in place, without any device
+ * allocation; G and the cluster products are recomputed from the chains'
+ * fields before their next use.  No counterpart in the reference, which
+ * fixes the hopping per sim file: it serves the fixed-field gradient
+ * evaluations, which visit many hoppings for the same fields. */
+int dqmc_engine_set_hopping(dqmc_engine *e, const void *exp_Ku, const void *exp_Kd,
+		const void *inv_exp_Ku, const void *inv_exp_Kd, const void *exp_halfKu,
+		const void *exp_halfKd, const void *inv_exp_halfKu, const void *inv_exp_halfKd);
 
 /* ---------------------------------------------------------------------------
  * Kernel-level seams on device pointers, batched over `batch` independent

@@ -101,3 +101,22 @@ def test_engine_reports_missing_device(lib, golden, tmp_path):
     assert open(sim, "rb").read() == before
     assert np.array_equal(np.frombuffer(before, np.uint8), np.frombuffer(open(sim, "rb").read(),
                                                                          np.uint8))
+
+
+@pytest.mark.parametrize("case", ["tog_sq", "tog_cplx", "tog_local"])
+def test_toggle_layout_matches_the_library(lib, golden, case):
+    """With measurement toggles on, the accumulator layout the Python side
+    builds (dataset by dataset, data.c:441-522 sizes) has the size the
+    library computes."""
+    from dqmc_b200 import engine
+    s = engine.SimData.read(os.path.join(golden, case, "sim_0.h5"))
+    p, _keep = s.params()
+    eq, ue = C.c_int(), C.c_int()
+    assert lib.load().dqmc_acc_sizes(C.byref(p), C.byref(eq), C.byref(ue)) == 0
+    assert eq.value == s.eq_acc.size
+    assert ue.value == s.ue_acc.size
+    ref = np.load(os.path.join(golden, case, "ref_out.npz"))
+    for k, v in s.measurements().items():
+        key = k.replace("/", "__")
+        assert key in ref.files, k
+        assert np.asarray(v).size == ref[key].size, k

@@ -121,3 +121,38 @@ def test_observable_gradients_match_central_differences(grad):
         tm[k] -= h
         fd = (m.evaluate_obs(tp)[0] - m.evaluate_obs(tm)[0]) / (2 * h)
         np.testing.assert_allclose(g[:, :, k], fd, rtol=FD_RTOL, atol=FD_RTOL * np.abs(g).max())
+
+
+def test_reused_engine_matches_fresh_models(grad):
+    """One model evaluated at theta_1, theta_2, theta_1 (the hopping replaced
+    in place each time) gives what fresh models give at each theta."""
+    fields = _fields(3, 8, 16, 11)
+    rng = np.random.default_rng(3)
+    t1 = np.concatenate([[1.0, -0.2, -0.3], 0.05 * rng.standard_normal(32)])
+    t2 = np.concatenate([[0.9, -0.1, 0.2], 0.05 * rng.standard_normal(32)])
+    m = grad.SquareModel(4, 4, U=4.0, dt=0.1, L=8, fields=fields, n_matmul=4)
+    seq = [m.evaluate(t) + m.evaluate_obs(t) for t in (t1, t2, t1)]
+    m.close()
+    for t, got in zip((t1, t2), seq[:2]):
+        f = grad.SquareModel(4, 4, U=4.0, dt=0.1, L=8, fields=fields, n_matmul=4)
+        want = f.evaluate(t) + f.evaluate_obs(t)
+        f.close()
+        for a, b in zip(got, want):
+            np.testing.assert_allclose(a, b, rtol=1e-12, atol=1e-12)
+    for a, b in zip(seq[0], seq[2]):
+        np.testing.assert_allclose(a, b, rtol=1e-12, atol=1e-12)
+
+
+def test_observables_autograd(grad):
+    import torch
+    fields = _fields(2, 8, 16, 13)
+    m = grad.SquareModel(4, 4, U=4.0, dt=0.1, L=8, fields=fields, n_matmul=4)
+    theta = torch.tensor(np.concatenate([[1.0, -0.2, -0.3], np.zeros(32)]), requires_grad=True)
+    y = grad.Observables.apply(theta, m)
+    wts = torch.tensor([[1.0, 2.0], [-0.5, 3.0]], dtype=torch.float64)
+    (y * wts).sum().backward()
+    obs, g = m.evaluate_obs(theta.detach().numpy())
+    np.testing.assert_allclose(y.detach().numpy(), obs, rtol=1e-13)
+    want = (wts.numpy()[:, :, None] * g).sum((0, 1))
+    np.testing.assert_allclose(theta.grad.numpy(), want, rtol=1e-12, atol=1e-14)
+    m.close()
