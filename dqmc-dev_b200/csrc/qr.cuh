@@ -62,7 +62,7 @@ template <typename T, int NBK>
 size_t qrb_smem_bytes(int N, bool gm = false)
 {
 	const int np = (N + NBK - 1) / NBK, ld = gm ? N : qrb_ld(N);
-	return sizeof(T) * ((gm ? 0 : (size_t)ld * N) + (size_t)ld * NBK + N + (size_t)np * NBK * NBK)
+	return sizeof(T) * ((gm ? 0 : (size_t)ld * N) + 2 * (size_t)ld * NBK + N + (size_t)np * NBK * NBK)
 	       + sizeof(double) * 3 * (size_t)N + sizeof(int) * (size_t)N + 64;
 }
 
@@ -253,30 +253,44 @@ __device__ inline void qrb_block_t(const T *A, int ld, const T *tau, T *Tp, int 
 // acts on rows and columns >= j0 of the partial product, whose panel
 // columns are still e_c there and whose rows j0..j1-1 are zero), then Q to
 // global memory and the phase of det Q.  All warps of the CTA.
+//
+// Block p's reflectors are moved out of A into Vb2[p & 1] ("prep") while
+// block p+1 is applied: prep(p) touches columns j0..j1-1 and rows j0..j1-1
+// of the columns right of them, the apply of block p+1 only rows and
+// columns >= j1, so one barrier per block suffices.
 template <typename T, int NW, int NBK, int RPL>
-__device__ inline void qrb_form_q(const QrArgs<T> &a, int item, T *A, int ld, T *Vb, const T *Ts,
+__device__ inline void qrb_form_q(const QrArgs<T> &a, int item, T *A, int ld, T *Vb2, const T *Ts,
 		const T *tau, const double *vv, int N)
 {
 	const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
 	const int np = (N + NBK - 1) / NBK;
-	for (int p = np - 1; p >= 0; p--) {
+	auto prep = [&](int p) {
 		const int j0 = p * NBK, nb = min(NBK, N - j0), j1 = j0 + nb, mr = N - j0;
-		(void)mr;
-		if (w < nb)
-			for (int r = j0 + lane; r < N; r += 32) Vb[r + (size_t)ld * w] = A[r + (size_t)ld * (j0 + w)];
-		__syncthreads();
-		if (w < nb)
-			for (int r = j0 + lane; r < N; r += 32)
-				A[r + (size_t)ld * (j0 + w)] = (r == j0 + w) ? one<T>() : zero<T>();
-		for (int c = j1 + tid / nb; c < N; c += blockDim.x / nb)
-			A[j0 + tid % nb + (size_t)ld * c] = zero<T>();
-		__syncthreads();
-		qrb_apply_cols<T, NBK, RPL, false>(A, ld, j0, Vb, Ts + (size_t)p * NBK * NBK, N, j0, nb, w, NW,
-		                                   lane);
+		T *Vb = Vb2 + (size_t)(p & 1) * ld * NBK;
+		// element (j0 + q % mr, j0 + q / mr) of the panel, copied then reset
+		for (int q = tid; q < nb * mr; q += blockDim.x) {
+			const int k = q / mr, r = j0 + q - k * mr;
+			T *e = A + r + (size_t)ld * (j0 + k);
+			Vb[r + (size_t)ld * k] = *e;
+			*e = (r == j0 + k) ? one<T>() : zero<T>();
+		}
+		for (int q = tid; q < nb * (N - j1); q += blockDim.x) {
+			const int c = q / nb;
+			A[j0 + q - c * nb + (size_t)ld * (j1 + c)] = zero<T>();
+		}
+	};
+	prep(np - 1);
+	__syncthreads();
+	for (int p = np - 1; p >= 0; p--) {
+		const int j0 = p * NBK, nb = min(NBK, N - j0);
+		qrb_apply_cols<T, NBK, RPL, false>(A, ld, j0, Vb2 + (size_t)(p & 1) * ld * NBK,
+		                                   Ts + (size_t)p * NBK * NBK, N, j0, nb, w, NW, lane);
+		if (p > 0) prep(p - 1);
 		__syncthreads();
 	}
 	T *Q = a.Q + (size_t)item * a.q_stride;
-	for (int q = tid; q < N * N; q += blockDim.x) Q[q] = A[(q % N) + (size_t)ld * (q / N)];
+	for (int c = w; c < N; c += NW)
+		for (int r = lane; r < N; r += 32) Q[r + (size_t)N * c] = A[r + (size_t)ld * c];
 	if (tid == 0 && a.qdet) {
 		T ph = one<T>();
 		for (int j = 0; j < N; j++) ph = ph * phase_of(one<T>() - tau[j] * vv[j]);
@@ -296,7 +310,7 @@ __global__ void __launch_bounds__(NW * 32) k_qrb(QrArgs<T> a)
 	// N columns, leading dimension ld, position order
 	T *A = GM ? a.work + (size_t)item * a.w_stride : (T *)smraw;
 	T *Vb = GM ? (T *)smraw : A + (size_t)ld * N;   // copy of one panel's V (ld x NBK)
-	T *tau = Vb + (size_t)ld * NBK;             // N
+	T *tau = Vb + 2 * (size_t)ld * NBK;         // N (Vb: two panel buffers)
 	T *Ts = tau + N;                            // np blocks of NBK x NBK
 	double *dsh = (double *)(Ts + (size_t)np * NBK * NBK);
 	double *vv = dsh + N;                       // v^H v
@@ -491,15 +505,144 @@ __global__ void __launch_bounds__(NW * 32) k_qrb(QrArgs<T> a)
 // LAPACK dlaqp2 does and recomputed when cancellation makes the downdate
 // unreliable), with the matrix in shared memory and columns swapped in
 // place so that column j holds pivot position j.  Step j: warp 0 picks
-// the pivot (first largest norm in position order, as idamax), swaps and
-// forms the reflector; all warps then update the remaining columns and
-// their norms.  Q is formed from blocks of NBK reflectors as in k_qrb.
+// the pivot (first largest norm in position order, as idamax) from the
+// per-warp first largest norms of the last update, exchanges the two
+// columns with the pivot column kept in registers and forms the reflector
+// there; all warps then update the remaining columns and their norms
+// (qrp_update) and leave their own first largest norm for the next step.
+// Q is formed from blocks of NBK reflectors as in k_qrb.
 // Outputs: Q, T = D^-1 R P^T, diag(R) and the pivot order.
 
 template <typename T, int NBK>
 size_t qrp_smem_bytes(int N, bool gm = false)
 {
 	return qrb_smem_bytes<T, NBK>(N, gm) + sizeof(double) * (size_t)N + 16;
+}
+
+// Householder step j of the pivoted QR on the columns j+1 .. N-1: one column
+// per 8 lanes, 4 columns per warp at a time (lane = 4 g + s: column slot s,
+// rows j + g + 8 i), so that a column's products need three exchange levels;
+// then each column's partial norm is downdated from its updated row j as
+// LAPACK dlaqp2 does, or recomputed below row j when the downdate has lost
+// too much.  The downdate n1 sqrt(1 - (|a_j| / n1)^2) is taken as
+// sqrt((n1 - |a_j|)(n1 + |a_j|)) and its test tt (n1 / n2)^2 <= tol3z as
+// (n1 - |a_j|)(n1 + |a_j|) <= tol3z n2^2: the same quantities without a
+// division.  The loops over a lane's rows stop at the last row (a
+// warp-uniform test), so late steps issue only the rows that remain.
+// Returns this warp's first largest new norm among its columns (NaN ranks
+// below every number, as -0.5) and its position, in every lane.
+// MAXI >= ceil(N / 8); the real shared-memory forms keep v and the column
+// in registers.
+template <typename T, int NW, int MAXI>
+__device__ inline void qrp_update(T *A, int ld, int N, int j, T ct, double *vn1, double *vn2,
+		double tol3z, double &best, int &bi, bool &nan_seen)
+{
+	constexpr bool CACHE = !is_cplx<T>::value && MAXI <= 20;
+	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, s = lane & 3, g = lane >> 2;
+	const T *vj = A + (size_t)ld * j;
+	auto vrow = [&](int r) { return (r < N) ? ((r == j) ? one<T>() : vj[r]) : zero<T>(); };
+	T v[CACHE ? MAXI : 1];
+	if constexpr (CACHE) {
+#pragma unroll
+		for (int i = 0; i < MAXI; i++) {
+			if (j + 8 * i >= N) break;
+			v[i] = vrow(j + g + 8 * i);
+		}
+	}
+	best = -1.0;
+	bi = N;
+	const int nc = N - j - 1;
+	for (int q0 = 4 * w; q0 < nc; q0 += 4 * NW) {
+		const int q = q0 + s, c = j + 1 + q;
+		const bool act = q < nc;
+		// an idle slot reads column j+1 and writes nothing
+		T *col = A + (size_t)ld * (act ? c : j + 1);
+		T d0 = zero<T>(), d1 = zero<T>(), aj;
+		double s2a = 0.0, s2b = 0.0;
+		if constexpr (CACHE) {
+			T x[MAXI];
+#pragma unroll
+			for (int i = 0; i < MAXI; i++) {
+				if (j + 8 * i >= N) break;
+				const int r = j + g + 8 * i;
+				x[i] = (r < N) ? col[r] : zero<T>();
+				if (i & 1) d1 += conjv(v[i]) * x[i];
+				else d0 += conjv(v[i]) * x[i];
+			}
+			T d = d0 + d1;
+			d += shfl_xor(d, 4);
+			d += shfl_xor(d, 8);
+			d += shfl_xor(d, 16);
+			const T f = ct * d;
+#pragma unroll
+			for (int i = 0; i < MAXI; i++) {
+				if (j + 8 * i >= N) break;
+				const int r = j + g + 8 * i;
+				x[i] -= v[i] * f;
+				if (r < N) {
+					if (act) col[r] = x[i];
+					if (r > j) {
+						if (i & 1) s2b += abs2(x[i]);
+						else s2a += abs2(x[i]);
+					}
+				}
+			}
+			aj = shfl(x[0], s);
+		} else {
+			for (int r = j + g; r < N; r += 8) d0 += conjv(vrow(r)) * col[r];
+			T d = d0;
+			d += shfl_xor(d, 4);
+			d += shfl_xor(d, 8);
+			d += shfl_xor(d, 16);
+			const T f = ct * d;
+			T x0 = zero<T>();
+			for (int r = j + g; r < N; r += 8) {
+				const T y = col[r] - vrow(r) * f;
+				if (act) col[r] = y;
+				if (r > j) s2a += abs2(y);
+				else x0 = y;
+			}
+			aj = shfl(x0, s);
+		}
+		double s2 = s2a + s2b;
+		s2 += __shfl_xor_sync(0xffffffffu, s2, 4);
+		s2 += __shfl_xor_sync(0xffffffffu, s2, 8);
+		s2 += __shfl_xor_sync(0xffffffffu, s2, 16);
+		if (act) {
+			// every lane of the column computes the new norm; lane g = 0 stores it
+			const double n1 = vn1[c], n2 = vn2[c];
+			double nv = n1;
+			if (n1 != 0.0) {
+				const double aa = absv(aj);
+				const double d2 = fmax(0.0, (n1 - aa) * (n1 + aa));
+				if (d2 <= tol3z * n2 * n2) {
+					nv = sqrt(s2);
+					if (g == 0) vn2[c] = nv;
+				} else {
+					nv = sqrt(d2);
+				}
+				if (g == 0) vn1[c] = nv;
+			}
+			if (!(nv >= 0.0)) {
+				nv = -0.5;
+				nan_seen = true;
+			}
+			if (nv > best) {
+				best = nv;
+				bi = c;
+			}
+		}
+	}
+	// first largest over the warp's four column slots
+#pragma unroll
+	for (int o = 1; o <= 2; o <<= 1) {
+		const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+		const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+		if (ob > best || (ob == best && oi < bi)) {
+			best = ob;
+			bi = oi;
+		}
+	}
 }
 
 template <typename T, int NW, int NBK, int RPL, bool GM>
@@ -513,7 +656,7 @@ __global__ void __launch_bounds__(NW * 32) k_qrp(QrArgs<T> a)
 	extern __shared__ __align__(16) unsigned char smraw[];
 	T *A = GM ? a.work + (size_t)item * a.w_stride : (T *)smraw;
 	T *Vb = GM ? (T *)smraw : A + (size_t)ld * N;
-	T *tau = Vb + (size_t)ld * NBK;
+	T *tau = Vb + 2 * (size_t)ld * NBK;
 	T *Ts = tau + N;
 	double *dsh = (double *)(Ts + (size_t)np * NBK * NBK);
 	double *vv = dsh + N;
@@ -525,38 +668,50 @@ __global__ void __launch_bounds__(NW * 32) k_qrp(QrArgs<T> a)
 		if (tid == 0 && a.err) atomicOr(a.err, DQ_ERR_SIZE);
 		return;
 	}
+	// per warp: first largest candidate norm of its columns and its position
+	__shared__ double s_best[NW];
+	__shared__ int s_bi[NW];
+	bool nan_seen = false;
 	const T *X = a.X + (size_t)item * a.x_stride;
-	for (int c = w; c < N; c += NW) {
-		double s = 0.0;
-		for (int r = lane; r < N; r += 32) {
-			const T v = X[r + (size_t)N * c];
-			A[r + (size_t)ld * c] = v;
-			s += abs2(v);
+	{
+		double best = -1.0;
+		int bi = N;
+		for (int c = w; c < N; c += NW) {
+			double s = 0.0;
+			for (int r = lane; r < N; r += 32) {
+				const T v = X[r + (size_t)N * c];
+				A[r + (size_t)ld * c] = v;
+				s += abs2(v);
+			}
+			s = sqrt(warp_sum(s));
+			if (lane == 0) {
+				vn1[c] = s;
+				vn2[c] = s;
+				pvt[c] = c;
+			}
+			if (!(s >= 0.0)) {
+				s = -0.5;
+				nan_seen = true;
+			}
+			if (s > best) {
+				best = s;
+				bi = c;
+			}
 		}
-		s = warp_sum(s);
 		if (lane == 0) {
-			vn1[c] = sqrt(s);
-			vn2[c] = vn1[c];
-			pvt[c] = c;
+			s_best[w] = best;
+			s_bi[w] = bi;
 		}
 	}
 	__syncthreads();
 	const double tol3z = sqrt(2.220446049250313e-16);
-	bool nan_seen = false;
 	for (int j = 0; j < N; j++) {
 		if (w == 0) {
-			// first largest partial norm among positions j..N-1; a NaN norm
-			// ranks below every number but stays a candidate
-			double best = -1.0;
-			int bi = N;
-			for (int c = j + lane; c < N; c += 32) {
-				double v = vn1[c];
-				if (!(v >= 0.0)) {
-					v = -0.5;
-					nan_seen = true;
-				}
-				if (v > best) { best = v; bi = c; }
-			}
+			// pivot: the first largest partial norm among positions j..N-1 (a
+			// NaN norm ranks below every number but stays a candidate), from
+			// the warps' partial results of the last update
+			double best = lane < NW ? s_best[lane] : -1.0;
+			int bi = lane < NW ? s_bi[lane] : N;
 #pragma unroll
 			for (int o = 16; o > 0; o >>= 1) {
 				const double ob = __shfl_xor_sync(0xffffffffu, best, o);
@@ -564,11 +719,20 @@ __global__ void __launch_bounds__(NW * 32) k_qrp(QrArgs<T> a)
 				if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
 			}
 			const int pj = bi;
+			// columns pj and j exchange places; the pivot column stays in
+			// registers and becomes the reflector (dlarfg convention)
+			T xp[RPL], xj[RPL];
+#pragma unroll
+			for (int t = 0; t < RPL; t++) {
+				const int r = lane + 32 * t;
+				xp[t] = (r < N) ? A[r + (size_t)ld * pj] : zero<T>();
+				xj[t] = (r < N) ? A[r + (size_t)ld * j] : zero<T>();
+			}
 			if (pj != j) {
-				for (int r = lane; r < N; r += 32) {
-					const T t0 = A[r + (size_t)ld * j];
-					A[r + (size_t)ld * j] = A[r + (size_t)ld * pj];
-					A[r + (size_t)ld * pj] = t0;
+#pragma unroll
+				for (int t = 0; t < RPL; t++) {
+					const int r = lane + 32 * t;
+					if (r < N) A[r + (size_t)ld * pj] = xj[t];
 				}
 				if (lane == 0) {
 					const double t1 = vn1[j]; vn1[j] = vn1[pj]; vn1[pj] = t1;
@@ -576,12 +740,16 @@ __global__ void __launch_bounds__(NW * 32) k_qrp(QrArgs<T> a)
 					const int t3 = pvt[j]; pvt[j] = pvt[pj]; pvt[pj] = t3;
 				}
 			}
-			__syncwarp();
-			T *vj = A + (size_t)ld * j;
 			double sig = 0.0;
-			for (int r = j + 1 + lane; r < N; r += 32) sig += abs2(vj[r]);
+			T al = zero<T>();
+#pragma unroll
+			for (int t = 0; t < RPL; t++) {
+				const int r = lane + 32 * t;
+				if (r > j && r < N) sig += abs2(xp[t]);
+				if (t == (j >> 5)) al = xp[t];
+			}
 			sig = warp_sum(sig);
-			const T alpha = vj[j];
+			const T alpha = shfl(al, j & 31);
 			T tj, scal;
 			double beta;
 			if (sig == 0.0 && im(alpha) == 0.0) {
@@ -593,10 +761,13 @@ __global__ void __launch_bounds__(NW * 32) k_qrp(QrArgs<T> a)
 				tj = (from_re<T>(beta) - alpha) / beta;
 				scal = one<T>() / (alpha - beta);
 			}
-			__syncwarp();
-			for (int r = j + 1 + lane; r < N; r += 32) vj[r] *= scal;
+			T *vj = A + (size_t)ld * j;
+#pragma unroll
+			for (int t = 0; t < RPL; t++) {
+				const int r = lane + 32 * t;
+				if (r < N) vj[r] = (r > j) ? xp[t] * scal : ((r == j) ? from_re<T>(beta) : xp[t]);
+			}
 			if (lane == 0) {
-				vj[j] = from_re<T>(beta);
 				tau[j] = tj;
 				dsh[j] = beta;
 				vv[j] = 1.0 + sig * abs2(scal);
@@ -605,58 +776,16 @@ __global__ void __launch_bounds__(NW * 32) k_qrp(QrArgs<T> a)
 		__syncthreads();
 		// H_j^H = I - conj(tau) v v^H on every remaining column, then the
 		// norm downdate from the updated row j
-		const T *vj = A + (size_t)ld * j;
-		T vr[RPL];
-#pragma unroll
-		for (int t = 0; t < RPL; t++) {
-			const int r = j + lane + 32 * t;
-			vr[t] = (r < N) ? ((r == j) ? one<T>() : vj[r]) : zero<T>();
-		}
-		const T ct = conjv(tau[j]);
-		for (int c = j + 1 + w; c < N; c += NW) {
-			T *col = A + (size_t)ld * c;
-			T x[RPL];
-			T d = zero<T>();
-#pragma unroll
-			for (int t = 0; t < RPL; t++) {
-				const int r = j + lane + 32 * t;
-				x[t] = (r < N) ? col[r] : zero<T>();
-				d += conjv(vr[t]) * x[t];
-			}
-			d = warp_sum(d);
-			const T f = ct * d;
-#pragma unroll
-			for (int t = 0; t < RPL; t++) {
-				const int r = j + lane + 32 * t;
-				x[t] -= vr[t] * f;
-				if (r < N) col[r] = x[t];
-			}
-			const double n1 = vn1[c], n2 = vn2[c];
-			if (n1 != 0.0) {
-				const T aj = shfl(x[0], 0);
-				double tt = absv(aj) / n1;
-				tt = fmax(0.0, 1.0 - tt * tt);
-				const double t2 = tt * (n1 / n2) * (n1 / n2);
-				if (t2 <= tol3z) {
-					double s2 = 0.0;
-#pragma unroll
-					for (int t = 0; t < RPL; t++) {
-						const int r = j + lane + 32 * t;
-						if (r > j && r < N) s2 += abs2(x[t]);
-					}
-					s2 = warp_sum(s2);
-					if (lane == 0) {
-						vn1[c] = sqrt(s2);
-						vn2[c] = vn1[c];
-					}
-				} else if (lane == 0) {
-					vn1[c] = n1 * sqrt(tt);
-				}
-			}
+		double best;
+		int bi;
+		qrp_update<T, NW, 4 * RPL>(A, ld, N, j, conjv(tau[j]), vn1, vn2, tol3z, best, bi, nan_seen);
+		if (lane == 0) {
+			s_best[w] = best;
+			s_bi[w] = bi;
 		}
 		__syncthreads();
 	}
-	if (nan_seen && lane == 0 && a.err) atomicOr(a.err, DQ_ERR_NAN);
+	if (nan_seen && a.err) atomicOr(a.err, DQ_ERR_NAN);
 	// T = D^-1 R P^T: position j is original column pvt[j]
 	for (int j = w; j < N; j += NW) {
 		const int c = pvt[j];
