@@ -168,10 +168,13 @@ static double dense_flops(int N, int batch)
 }
 
 template <typename T>
-static int eq_gemm(const GemmArgs<T> &g, cudaStream_t st, int *count, ProfHook *ph = nullptr)
+static int eq_gemm(const GemmArgs<T> &g, cudaStream_t st, int *count, ProfHook *ph = nullptr,
+		unsigned *err = nullptr)
 {
 	if (ph) ph->begin();
-	const int rc = launch_gemm<T>(g, st);
+	GemmArgs<T> ge = g;
+	if (!ge.err) ge.err = err;
+	const int rc = launch_gemm<T>(ge, st);
 	if (ph) ph->end(PC_GEMM, gemm_flops(g), gemm_bytes(g));
 	if (count) (*count)++;
 	return rc;
@@ -200,7 +203,7 @@ static int run_calc_eq_g(const EqWork<T> &w, int l0, cudaStream_t st, int *count
 	if (first == 2 && w.Pr) {
 		q.X = w.Pr + (size_t)l0 * NN; q.x_stride = w.pr_stride;
 	} else if (first == 2) {
-		eq_gemm(gargs<T>(N, N, N, NB, clu(l0 + 1), aCl, N, clu(l0), aCl, N, w.X, aI, N), st, count, ph);
+		eq_gemm(gargs<T>(N, N, N, NB, clu(l0 + 1), aCl, N, clu(l0), aCl, N, w.X, aI, N), st, count, ph, w.err);
 		q.X = w.X; q.x_stride = NN;
 	} else {
 		q.X = clu(l0); q.x_stride = w.cl_stride;
@@ -217,10 +220,10 @@ static int run_calc_eq_g(const EqWork<T> &w, int l0, cudaStream_t st, int *count
 		const int next = (m + 2) % F;
 		if (w.Pr) {
 			eq_gemm(gargs<T>(N, N, N, NB, w.Pr + (size_t)m * NN, Addr{w.pr_stride, 0, 1}, N, w.Qm, aI, N,
-			                 w.X, aI, N), st, count, ph);
+			                 w.X, aI, N), st, count, ph, w.err);
 		} else {
-			eq_gemm(gargs<T>(N, N, N, NB, clu(m + 1), aCl, N, clu(m), aCl, N, w.W, aI, N), st, count, ph);
-			eq_gemm(gargs<T>(N, N, N, NB, w.W, aI, N, w.Qm, aI, N, w.X, aI, N), st, count, ph);
+			eq_gemm(gargs<T>(N, N, N, NB, clu(m + 1), aCl, N, clu(m), aCl, N, w.W, aI, N), st, count, ph, w.err);
+			eq_gemm(gargs<T>(N, N, N, NB, w.W, aI, N, w.Qm, aI, N, w.X, aI, N), st, count, ph, w.err);
 		}
 		m = next;
 		QrArgs<T> r = q;
@@ -237,7 +240,7 @@ static int run_calc_eq_g(const EqWork<T> &w, int l0, cudaStream_t st, int *count
 		                         zero<T>(), GM_A_UPPER | GM_B_GATHER);
 		g.gidx = w.pvt;
 		g.aG = Addr{(long long)N, 0, 1};
-		eq_gemm(g, st, count, ph);
+		eq_gemm(g, st, count, ph, w.err);
 		T *t = Tc; Tc = Tn; Tn = t;
 	}
 	RecArgs<T> ra;
@@ -264,7 +267,8 @@ static int run_calc_eq_g(const EqWork<T> &w, int l0, cudaStream_t st, int *count
 // l*N; exp_K per spin (item parity); X, W: NB x N*N scratch.
 template <typename T>
 static void run_mul_seq(int N, int n, int NB, const T *expK, Addr aK, const double *d,
-		long long d_stride, T *out, Addr aout, T *X, T *W, cudaStream_t st, int *count)
+		long long d_stride, T *out, Addr aout, T *X, T *W, cudaStream_t st, int *count,
+		unsigned *err = nullptr)
 {
 	const size_t NN = (size_t)N * N;
 	const Addr aI = Addr{(long long)NN, 0, 1};
@@ -281,7 +285,7 @@ static void run_mul_seq(int N, int n, int NB, const T *expK, Addr aK, const doub
 		                         zero<T>(), GM_B_ROWD);
 		g.d = d + (size_t)m * N;
 		g.aD = Addr{d_stride, 0, 1};
-		eq_gemm(g, st, count);
+		eq_gemm(g, st, count, nullptr, err);
 		src = dst;
 		as = ad;
 	}
@@ -817,7 +821,7 @@ struct Group : GroupBase, ProfHook {
 	void gemm(const GemmArgs<T> &g)
 	{
 		prof_begin(0);
-		eq_gemm<T>(g, st, &launch_count);
+		eq_gemm<T>(g, st, &launch_count, nullptr, err.p);
 		watchdog("k_gemm");
 		double fl = 2.0 * g.M * g.N * g.K * g.batch * (is_cplx<T>::value ? 4.0 : 1.0);
 		if (g.mode & GM_A_UPPER) fl *= 0.5;
@@ -860,7 +864,8 @@ struct Group : GroupBase, ProfHook {
 		const size_t NN = (size_t)N * N;
 		prof_begin(0);
 		run_mul_seq<T>(N, nmul, NB, expK.p, per_spin(NN), dv.p + (size_t)f * nmul * N, (long long)L * N,
-		               Cl.p + (size_t)f * NN, per_item((long long)F * NN), X.p, W.p, st, &launch_count);
+		               Cl.p + (size_t)f * NN, per_item((long long)F * NN), X.p, W.p, st, &launch_count,
+		               err.p);
 		watchdog("mul_seq");
 		const double fl = 2.0 * N * NN * NB * (nmul - 1) * (is_cplx<T>::value ? 4.0 : 1.0);
 		prof_end(0, fl, 3.0 * sizeof(T) * NN * NB * (nmul - 1));

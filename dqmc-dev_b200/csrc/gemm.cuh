@@ -18,12 +18,19 @@
 //                                        k-tiles left of the diagonal skipped)
 //   B_GATHER   B[k,c] = B[idx[k],c]     (row permutation P^T T)
 //   B_IDENT    B = I                    (C = alpha A + beta C)
-// Tiles move global -> shared with cp.async (zero-filled outside the matrix)
-// through a STAGES-deep ring; scale vectors are staged once per CTA and
-// applied when fragments are read, so every mode keeps the same pipeline.
+// Tiles move global -> shared through a STAGES-deep ring, zero-filled
+// outside the matrix: in the TMA form one thread loads each stage's A and B
+// boxes with cp.async.bulk.tensor onto the stage's mbarrier (tensor maps over
+// this GPU's memory, no multicast); otherwise (row gathers, operands whose
+// address or strides a tensor map cannot take) every thread copies elements
+// with cp.async.  Scale vectors are staged once per CTA and applied when
+// fragments are read, so every mode keeps the same pipeline.
 #pragma once
 
+#include <cuda.h>
+
 #include "common.cuh"
+#include "mbar.cuh"
 
 namespace dq {
 
@@ -61,6 +68,11 @@ struct GemmArgs {
 	const double *d; const double *dinv; Addr aD;   // scaling vectors (length K or M)
 	const int *gidx; Addr aG;                       // row gather for B
 	int b0;                                         // first item of this launch
+	unsigned *err;                                  // error word (TMA wait timeouts), may be null
+	// TMA form: 4-d tensor maps (rows, columns, b % div, b / div) of A and B;
+	// tz / tw: whether the third / fourth coordinate is used (else 0)
+	CUtensorMap tmA, tmB;
+	int tzA, twA, tzB, twB;
 };
 
 __device__ inline void cp_async8(void *smem, const void *gmem, bool valid)
@@ -104,17 +116,23 @@ struct GemmCfg {
 	static constexpr int STAGE = TILE_A + TILE_B;     // elements of T
 	static constexpr int KMAX = 512;                  // largest K of the scale vectors
 	static constexpr int RING_BYTES = STAGES * STAGE * (int)sizeof(T);
-	// the ring, then (modes with scale vectors or a gather only) per-k
-	// scales, per-k inverse scales, per-row and per-column scales and the
-	// gather rows, sized for this launch's K so that the CTAs of the plain
-	// modes hold only the ring
-	static constexpr int smem_bytes(int mode, int K)
+	// TMA form: one mbarrier per stage and the CTA's abort flag
+	static constexpr int MBAR_BYTES = (8 * STAGES + 8 + 15) / 16 * 16;
+	// boxes land at 128-byte boundaries: every stage and tile is a multiple
+	static_assert((TILE_A * (int)sizeof(T)) % 128 == 0 && (TILE_B * (int)sizeof(T)) % 128 == 0,
+	              "tiles of 128-byte multiples");
+	// the ring, the mbarriers (TMA form), then (modes with scale vectors or
+	// a gather only) per-k scales, per-k inverse scales, per-row and
+	// per-column scales and the gather rows, sized for this launch's K so
+	// that the CTAs of the plain modes hold only the ring
+	static constexpr int smem_bytes(int mode, int K, bool tma)
 	{
-		return RING_BYTES + ((mode & (GM_A_DD | GM_B_ROWD | GM_B_COLD | GM_B_GATHER))
-		                         ? (2 * K + BM + BN) * (int)sizeof(double) + K * 4
-		                         : 0);
+		return RING_BYTES + (tma ? MBAR_BYTES : 0)
+		       + ((mode & (GM_A_DD | GM_B_ROWD | GM_B_COLD | GM_B_GATHER))
+		              ? (2 * K + BM + BN) * (int)sizeof(double) + K * 4
+		              : 0);
 	}
-	static constexpr int SMEM_MAX = RING_BYTES + (2 * KMAX + BM + BN) * (int)sizeof(double) + KMAX * 4;
+	static constexpr int SMEM_MAX = RING_BYTES + MBAR_BYTES + (2 * KMAX + BM + BN) * (int)sizeof(double) + KMAX * 4;
 	static constexpr int WTM = BM / WM, WTN = BN / WN;
 	static constexpr int MT = WTM / 8, NT = WTN / 8;
 	static constexpr int A_PER_T = (BM * BK + THREADS - 1) / THREADS;
@@ -123,15 +141,18 @@ struct GemmCfg {
 	static_assert(BK % 4 == 0, "BK multiple of 4");
 };
 
-template <typename T, int BM, int BN, int BK, int WM, int WN, int STAGES, int MODE>
+template <typename T, int BM, int BN, int BK, int WM, int WN, int STAGES, int MODE, bool TMA>
 __global__ void __launch_bounds__(WM *WN * 32)
-k_gemm(GemmArgs<T> g)
+k_gemm(const __grid_constant__ GemmArgs<T> g)
 {
 	using Cfg = GemmCfg<T, BM, BN, BK, WM, WN, STAGES>;
 	constexpr bool CX = Cfg::CX;
-	extern __shared__ __align__(16) unsigned char smraw[];
-	T *sm = (T *)smraw;
-	double *sdk = (double *)(smraw + Cfg::RING_BYTES);                    // per-k scale
+	static_assert(!(TMA && (MODE & GM_B_GATHER)), "the row gather loads element by element");
+	extern __shared__ __align__(128) unsigned char gsm_raw[];
+	T *sm = (T *)gsm_raw;
+	uint64_t *mbar = (uint64_t *)(gsm_raw + Cfg::RING_BYTES);             // TMA: one per stage
+	volatile int *abortp = (volatile int *)(mbar + STAGES);             // TMA: a wait timed out
+	double *sdk = (double *)(gsm_raw + Cfg::RING_BYTES + (TMA ? Cfg::MBAR_BYTES : 0)); // per-k scale
 	double *sdk2 = sdk + g.K;                                             // per-k 1/d (A_DD)
 	double *sdr = sdk2 + g.K;                                             // per-row (A_DD)
 	double *sdc = sdr + BM;                                               // per-column (B_COLD)
@@ -168,6 +189,29 @@ k_gemm(GemmArgs<T> g)
 	int kt0 = 0;
 	if (MODE & GM_A_UPPER) kt0 = m0 / BK;
 	const int nkt = (K + BK - 1) / BK;
+
+	// TMA form: the boxes of k-tile kt into ring stage `stage`, issued by one
+	// thread; the stage's mbarrier completes when both boxes have landed
+	constexpr int E = CX ? 2 : 1;   // doubles per element: tensor maps count doubles
+	constexpr uint32_t TX = (uint32_t)((Cfg::TILE_A + ((MODE & GM_B_IDENT) ? 0 : Cfg::TILE_B)) * sizeof(T));
+	const int zA = g.tzA ? b % g.aA.div : 0, wA = g.twA ? b / g.aA.div : 0;
+	const int zB = g.tzB ? b % g.aB.div : 0, wB = g.twB ? b / g.aB.div : 0;
+	auto issue_tma = [&](int kt, int stage) {
+		T *As = sm + stage * Cfg::STAGE;
+		T *Bs = As + Cfg::TILE_A;
+		const uint32_t mb = smem_u32(mbar + stage);
+		mbar_arrive_tx(mb, TX);
+		tma_load_4d(smem_u32(As), &g.tmA, E * m0, kt * BK, zA, wA, mb);
+		if (!(MODE & GM_B_IDENT)) tma_load_4d(smem_u32(Bs), &g.tmB, E * kt * BK, n0, zB, wB, mb);
+	};
+	if constexpr (TMA) {
+		if (tid == 0) {
+			for (int s = 0; s < STAGES; s++) mbar_init(smem_u32(mbar + s), 1);
+			*abortp = 0;
+			asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+		}
+		__syncthreads();
+	}
 
 	auto issue = [&](int kt, int stage) {
 		T *As = sm + stage * Cfg::STAGE;
@@ -210,21 +254,34 @@ k_gemm(GemmArgs<T> g)
 		}
 
 	// prologue
+	if constexpr (TMA) {
+		if (tid == 0)
+			for (int sidx = 0; sidx < STAGES - 1; sidx++)
+				if (kt0 + sidx < nkt) issue_tma(kt0 + sidx, sidx);
+	} else {
 #pragma unroll
-	for (int sidx = 0; sidx < STAGES - 1; sidx++) {
-		if (kt0 + sidx < nkt) issue(kt0 + sidx, sidx);
-		cp_commit();
+		for (int sidx = 0; sidx < STAGES - 1; sidx++) {
+			if (kt0 + sidx < nkt) issue(kt0 + sidx, sidx);
+			cp_commit();
+		}
 	}
 	const int gq = lane >> 2, tq = lane & 3;
 	for (int kt = kt0; kt < nkt; kt++) {
-		cp_wait<STAGES - 2>();
-		__syncthreads();
-		{
+		const int it = kt - kt0;
+		// the stage written next is the one every warp finished at kt - 1
+		if constexpr (TMA) {
+			mbar_wait_bounded(smem_u32(mbar + it % STAGES), (it / STAGES) & 1, abortp, g.err);
+			__syncthreads();
+			const int nk = kt + STAGES - 1;
+			if (tid == 0 && nk < nkt) issue_tma(nk, (nk - kt0) % STAGES);
+		} else {
+			cp_wait<STAGES - 2>();
+			__syncthreads();
 			const int nk = kt + STAGES - 1;
 			if (nk < nkt) issue(nk, (nk - kt0) % STAGES);
 			cp_commit();
 		}
-		const int stage = (kt - kt0) % STAGES;
+		const int stage = it % STAGES;
 		const T *As = sm + stage * Cfg::STAGE;
 		const T *Bs = As + Cfg::TILE_A;
 		const int k0 = kt * BK;
@@ -276,7 +333,7 @@ k_gemm(GemmArgs<T> g)
 				}
 		}
 	}
-	cp_wait<0>();
+	if constexpr (!TMA) cp_wait<0>();
 
 	// epilogue: lane holds C[gq][2 tq + {0,1}] of each 8x8 tile
 	const bool use_beta = !(re(g.beta) == 0.0 && im(g.beta) == 0.0);

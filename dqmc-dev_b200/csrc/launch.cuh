@@ -24,6 +24,14 @@ inline cudaError_t raise_smem(K kern, size_t bytes)
 	return raise_smem_ptr((const void *)kern, bytes);
 }
 
+// Tensor map of one batched GEMM operand (column-major rows x cols, leading
+// dimension ld, item b at base + (b / div) * hi + (b % div) * lo) for boxes
+// of box_rows x box_cols elements; elem_doubles = 2 for complex128.  False
+// when a tensor map cannot describe it (alignment, strides, a slice table),
+// and the caller then loads element by element.
+bool tma_map_operand(CUtensorMap *map, int *tz, int *tw, const void *base, int elem_doubles, int rows,
+		int cols, long long ld, const Addr &ad, int batch, int box_rows, int box_cols);
+
 // largest N the per-matrix factorisations (QR, recombine) support: the
 // shared-memory form while N x N fits there, the global-memory form (working
 // matrix in the caller's per-item workspace, L2-resident) up to 256

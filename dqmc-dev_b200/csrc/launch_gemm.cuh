@@ -2,25 +2,51 @@
 // choice.  Included by launch_gemm_r.cu and launch_gemm_c.cu only.
 #pragma once
 
+#include <cstdlib>
+
 #include "dqmc_b200.h"
 #include "launch.cuh"
 
 namespace dq {
 
-template <typename T, int BM, int BN, int BK, int WM, int WN, int ST, int MODE>
-static int launch_gemm_mode(const GemmArgs<T> &g, cudaStream_t st)
+template <typename T, int BM, int BN, int BK, int WM, int WN, int ST, int MODE, bool TMA>
+static int launch_gemm_form(const GemmArgs<T> &g, cudaStream_t st)
 {
 	using Cfg = GemmCfg<T, BM, BN, BK, WM, WN, ST>;
-	if (raise_smem(k_gemm<T, BM, BN, BK, WM, WN, ST, MODE>, Cfg::SMEM_MAX) != cudaSuccess)
+	if (raise_smem(k_gemm<T, BM, BN, BK, WM, WN, ST, MODE, TMA>, Cfg::SMEM_MAX) != cudaSuccess)
 		return DQMC_E_ARG;
 	// the grid's z extent is at most 65535: larger batches take several launches
 	for (int b0 = 0; b0 < g.batch; b0 += 65535) {
 		GemmArgs<T> gc = g;
 		gc.b0 = b0;
 		dim3 grid((g.M + BM - 1) / BM, (g.N + BN - 1) / BN, min(65535, g.batch - b0));
-		k_gemm<T, BM, BN, BK, WM, WN, ST, MODE><<<grid, Cfg::THREADS, Cfg::smem_bytes(MODE, g.K), st>>>(gc);
+		k_gemm<T, BM, BN, BK, WM, WN, ST, MODE, TMA>
+			<<<grid, Cfg::THREADS, Cfg::smem_bytes(MODE, g.K, TMA), st>>>(gc);
 	}
 	return 0;
+}
+
+// the TMA form wherever tensor maps describe both operands (not the row
+// gather, whose rows come from a table); the element-wise form otherwise.
+// DQMC_GEMM_TMA=0 in the environment selects the element-wise form always.
+template <typename T, int BM, int BN, int BK, int WM, int WN, int ST, int MODE>
+static int launch_gemm_mode(const GemmArgs<T> &g, cudaStream_t st)
+{
+	using Cfg = GemmCfg<T, BM, BN, BK, WM, WN, ST>;
+	if constexpr (!(MODE & GM_B_GATHER)) {
+		static const bool off = [] {
+			const char *e = getenv("DQMC_GEMM_TMA");
+			return e && e[0] == '0';
+		}();
+		constexpr int ED = is_cplx<T>::value ? 2 : 1;
+		GemmArgs<T> gt = g;
+		if (!off &&
+		    tma_map_operand(&gt.tmA, &gt.tzA, &gt.twA, g.A, ED, g.M, g.K, g.lda, g.aA, g.batch, Cfg::SA, BK) &&
+		    ((MODE & GM_B_IDENT) ||
+		     tma_map_operand(&gt.tmB, &gt.tzB, &gt.twB, g.B, ED, g.K, g.N, g.ldb, g.aB, g.batch, Cfg::SB, BN)))
+			return launch_gemm_form<T, BM, BN, BK, WM, WN, ST, MODE, true>(gt, st);
+	}
+	return launch_gemm_form<T, BM, BN, BK, WM, WN, ST, MODE, false>(g, st);
 }
 
 template <typename T, int BM, int BN, int BK, int WM, int WN, int ST>
