@@ -266,6 +266,13 @@ k_gemm(const __grid_constant__ GemmArgs<T> g)
 		}
 	}
 	const int gq = lane >> 2, tq = lane & 3;
+	// this lane's row scales (A_DD) and column scales (B_COLD) do not change
+	// along k: read once instead of at every fragment
+	double srow[Cfg::MT], scol[Cfg::NT];
+#pragma unroll
+	for (int i = 0; i < Cfg::MT; i++) srow[i] = (MODE & GM_A_DD) ? sdr[wm * Cfg::WTM + i * 8 + gq] : 1.0;
+#pragma unroll
+	for (int j = 0; j < Cfg::NT; j++) scol[j] = (MODE & GM_B_COLD) ? sdc[wn * Cfg::WTN + j * 8 + gq] : 1.0;
 	for (int kt = kt0; kt < nkt; kt++) {
 		const int it = kt - kt0;
 		// the stage written next is the one every warp finished at kt - 1
@@ -299,7 +306,7 @@ k_gemm(const __grid_constant__ GemmArgs<T> g)
 				double xr, xi;
 				split(v, xr, xi);
 				double sc = ka;
-				if (MODE & GM_A_DD) sc *= sdr[r];
+				if (MODE & GM_A_DD) sc *= srow[i];
 				if ((MODE & GM_A_UPPER) && (m0 + r > gk)) sc = 0.0;
 				fa[i] = xr * sc;
 				if constexpr (CX) fai[i] = xi * sc;
@@ -316,7 +323,7 @@ k_gemm(const __grid_constant__ GemmArgs<T> g)
 					split(v, xr, xi);
 				}
 				double sc = kb;
-				if (MODE & GM_B_COLD) sc *= sdc[c];
+				if (MODE & GM_B_COLD) sc *= scol[j];
 				fb[j] = xr * sc;
 				if constexpr (CX) fbi[j] = xi * sc;
 			}
