@@ -89,7 +89,7 @@ ROOFLINE_KERNELS = {
 # DRAM bytes (read + write) per chain-spin item of one launch, from ncu
 # captures of these kernels on the 12x12 model (profiles/), scaled by the
 # items of a launch; other workloads report null
-TRAFFIC_PER_ITEM = {"batch256": {"gemm": 172848, "qr_presort": 168068, "qr_pivot": 166916,
+TRAFFIC_PER_ITEM = {"batch256": {"gemm": 172580, "qr_presort": 168068, "qr_pivot": 166916,
                                  "recombine": 333636, "update": 170852}}
 
 T0 = time.time()
