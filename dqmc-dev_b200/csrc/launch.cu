@@ -57,7 +57,7 @@ bool tma_map_operand(CUtensorMap *map, int *tz, int *tw, const void *base, int e
 	return true;
 }
 
-cudaError_t raise_smem_ptr(const void *kern, size_t bytes)
+cudaError_t raise_smem_ptr(const void *kern, size_t bytes, bool carve)
 {
 	static std::mutex mu;
 	static std::map<std::pair<int, const void *>, size_t> cur;
@@ -65,7 +65,13 @@ cudaError_t raise_smem_ptr(const void *kern, size_t bytes)
 	const cudaError_t ge = cudaGetDevice(&dev);
 	if (ge != cudaSuccess) return ge;
 	std::lock_guard<std::mutex> lk(mu);
-	size_t &c = cur[std::make_pair(dev, kern)];
+	const auto key = std::make_pair(dev, kern);
+	if (carve && !cur.count(key)) {
+		const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+		                                           (int)cudaSharedmemCarveoutMaxShared);
+		if (e != cudaSuccess) return e;
+	}
+	size_t &c = cur[key];
 	if (bytes <= c) return cudaSuccess;
 	const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 	if (e == cudaSuccess) c = bytes;

@@ -16,12 +16,16 @@ namespace dq {
 // shrink it below what an earlier group's launches (and captured graphs)
 // rely on.  Keyed by (device, kernel) under one lock: engines on other
 // devices and the gradient paths' host threads launch concurrently.
-cudaError_t raise_smem_ptr(const void *kern, size_t bytes);
+// With carve, the kernel also prefers the largest shared-memory carveout,
+// so that an SM configured for one such kernel (a QR CTA of one lane) can
+// take CTAs of another (a GEMM of the next lane); the delayed update keeps
+// the default, which leaves it the L1 cache its reads of G go through.
+cudaError_t raise_smem_ptr(const void *kern, size_t bytes, bool carve);
 
 template <typename K>
-inline cudaError_t raise_smem(K kern, size_t bytes)
+inline cudaError_t raise_smem(K kern, size_t bytes, bool carve = false)
 {
-	return raise_smem_ptr((const void *)kern, bytes);
+	return raise_smem_ptr((const void *)kern, bytes, carve);
 }
 
 // Tensor map of one batched GEMM operand (column-major rows x cols, leading

@@ -13,7 +13,7 @@ template <typename T, int BM, int BN, int BK, int WM, int WN, int ST, int MODE, 
 static int launch_gemm_form(const GemmArgs<T> &g, cudaStream_t st)
 {
 	using Cfg = GemmCfg<T, BM, BN, BK, WM, WN, ST>;
-	if (raise_smem(k_gemm<T, BM, BN, BK, WM, WN, ST, MODE, TMA>, Cfg::SMEM_MAX) != cudaSuccess)
+	if (raise_smem(k_gemm<T, BM, BN, BK, WM, WN, ST, MODE, TMA>, Cfg::SMEM_MAX, true) != cudaSuccess)
 		return DQMC_E_ARG;
 	// the grid's z extent is at most 65535: larger batches take several launches
 	for (int b0 = 0; b0 < g.batch; b0 += 65535) {

@@ -17,7 +17,7 @@ static const size_t SMEM_FIT = 226 * 1024;
 template <typename K, typename Args>
 static int launch_dense(K kern, const Args &a, size_t sm, cudaStream_t st)
 {
-	if (raise_smem(kern, sm) != cudaSuccess) return DQMC_E_ARG;
+	if (raise_smem(kern, sm, true) != cudaSuccess) return DQMC_E_ARG;
 	kern<<<a.batch, 512, sm, st>>>(a);
 	return 0;
 }

@@ -62,7 +62,7 @@ template <typename T, int NBK>
 size_t qrb_smem_bytes(int N, bool gm = false)
 {
 	const int np = (N + NBK - 1) / NBK, ld = gm ? N : qrb_ld(N);
-	return sizeof(T) * ((gm ? 0 : (size_t)ld * N) + 2 * (size_t)ld * NBK + N + (size_t)np * NBK * NBK)
+	return sizeof(T) * ((gm ? 0 : (size_t)ld * N) + (size_t)ld * NBK + N + (size_t)np * NBK * NBK)
 	       + sizeof(double) * 3 * (size_t)N + sizeof(int) * (size_t)N + 64;
 }
 
@@ -252,21 +252,20 @@ __device__ inline void qrb_block_t(const T *A, int ld, const T *tau, T *Tp, int 
 // block factors Ts, accumulated backwards by blocks in place of A (block p
 // acts on rows and columns >= j0 of the partial product, whose panel
 // columns are still e_c there and whose rows j0..j1-1 are zero), then Q to
-// global memory and the phase of det Q.  All warps of the CTA.
-//
-// Block p's reflectors are moved out of A into Vb2[p & 1] ("prep") while
-// block p+1 is applied: prep(p) touches columns j0..j1-1 and rows j0..j1-1
-// of the columns right of them, the apply of block p+1 only rows and
-// columns >= j1, so one barrier per block suffices.
+// global memory and the phase of det Q.  All warps of the CTA.  Per block:
+// each thread moves its elements of the block's reflectors into Vb and
+// resets them to e_c in the same pass; one barrier; the apply; one barrier.
+// (A second buffer, filled while the previous block is applied, saves the
+// first barrier but takes 9.5 KB more shared memory, which keeps a GEMM CTA
+// of another lane from sharing the SM.)
 template <typename T, int NW, int NBK, int RPL>
-__device__ inline void qrb_form_q(const QrArgs<T> &a, int item, T *A, int ld, T *Vb2, const T *Ts,
+__device__ inline void qrb_form_q(const QrArgs<T> &a, int item, T *A, int ld, T *Vb, const T *Ts,
 		const T *tau, const double *vv, int N)
 {
 	const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
 	const int np = (N + NBK - 1) / NBK;
-	auto prep = [&](int p) {
+	for (int p = np - 1; p >= 0; p--) {
 		const int j0 = p * NBK, nb = min(NBK, N - j0), j1 = j0 + nb, mr = N - j0;
-		T *Vb = Vb2 + (size_t)(p & 1) * ld * NBK;
 		// element (j0 + q % mr, j0 + q / mr) of the panel, copied then reset
 		for (int q = tid; q < nb * mr; q += blockDim.x) {
 			const int k = q / mr, r = j0 + q - k * mr;
@@ -278,14 +277,9 @@ __device__ inline void qrb_form_q(const QrArgs<T> &a, int item, T *A, int ld, T 
 			const int c = q / nb;
 			A[j0 + q - c * nb + (size_t)ld * (j1 + c)] = zero<T>();
 		}
-	};
-	prep(np - 1);
-	__syncthreads();
-	for (int p = np - 1; p >= 0; p--) {
-		const int j0 = p * NBK, nb = min(NBK, N - j0);
-		qrb_apply_cols<T, NBK, RPL, false>(A, ld, j0, Vb2 + (size_t)(p & 1) * ld * NBK,
-		                                   Ts + (size_t)p * NBK * NBK, N, j0, nb, w, NW, lane);
-		if (p > 0) prep(p - 1);
+		__syncthreads();
+		qrb_apply_cols<T, NBK, RPL, false>(A, ld, j0, Vb, Ts + (size_t)p * NBK * NBK, N, j0, nb, w, NW,
+		                                   lane);
 		__syncthreads();
 	}
 	T *Q = a.Q + (size_t)item * a.q_stride;
@@ -310,7 +304,7 @@ __global__ void __launch_bounds__(NW * 32) k_qrb(QrArgs<T> a)
 	// N columns, leading dimension ld, position order
 	T *A = GM ? a.work + (size_t)item * a.w_stride : (T *)smraw;
 	T *Vb = GM ? (T *)smraw : A + (size_t)ld * N;   // copy of one panel's V (ld x NBK)
-	T *tau = Vb + 2 * (size_t)ld * NBK;         // N (Vb: two panel buffers)
+	T *tau = Vb + (size_t)ld * NBK;             // N
 	T *Ts = tau + N;                            // np blocks of NBK x NBK
 	double *dsh = (double *)(Ts + (size_t)np * NBK * NBK);
 	double *vv = dsh + N;                       // v^H v
@@ -531,8 +525,9 @@ size_t qrp_smem_bytes(int N, bool gm = false)
 // warp-uniform test), so late steps issue only the rows that remain.
 // Returns this warp's first largest new norm among its columns (NaN ranks
 // below every number, as -0.5) and its position, in every lane.
-// MAXI >= ceil(N / 8); the real shared-memory forms keep v and the column
-// in registers.
+// MAXI >= ceil(N / 8); the real shared-memory forms keep the column in
+// registers between the two passes (v is read again: its loads are shared by
+// the four column slots of a warp).
 template <typename T, int NW, int MAXI>
 __device__ inline void qrp_update(T *A, int ld, int N, int j, T ct, double *vn1, double *vn2,
 		double tol3z, double &best, int &bi, bool &nan_seen)
@@ -541,14 +536,6 @@ __device__ inline void qrp_update(T *A, int ld, int N, int j, T ct, double *vn1,
 	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, s = lane & 3, g = lane >> 2;
 	const T *vj = A + (size_t)ld * j;
 	auto vrow = [&](int r) { return (r < N) ? ((r == j) ? one<T>() : vj[r]) : zero<T>(); };
-	T v[CACHE ? MAXI : 1];
-	if constexpr (CACHE) {
-#pragma unroll
-		for (int i = 0; i < MAXI; i++) {
-			if (j + 8 * i >= N) break;
-			v[i] = vrow(j + g + 8 * i);
-		}
-	}
 	best = -1.0;
 	bi = N;
 	const int nc = N - j - 1;
@@ -566,8 +553,8 @@ __device__ inline void qrp_update(T *A, int ld, int N, int j, T ct, double *vn1,
 				if (j + 8 * i >= N) break;
 				const int r = j + g + 8 * i;
 				x[i] = (r < N) ? col[r] : zero<T>();
-				if (i & 1) d1 += conjv(v[i]) * x[i];
-				else d0 += conjv(v[i]) * x[i];
+				if (i & 1) d1 += conjv(vrow(r)) * x[i];
+				else d0 += conjv(vrow(r)) * x[i];
 			}
 			T d = d0 + d1;
 			d += shfl_xor(d, 4);
@@ -578,7 +565,7 @@ __device__ inline void qrp_update(T *A, int ld, int N, int j, T ct, double *vn1,
 			for (int i = 0; i < MAXI; i++) {
 				if (j + 8 * i >= N) break;
 				const int r = j + g + 8 * i;
-				x[i] -= v[i] * f;
+				x[i] -= vrow(r) * f;
 				if (r < N) {
 					if (act) col[r] = x[i];
 					if (r > j) {
@@ -645,8 +632,10 @@ __device__ inline void qrp_update(T *A, int ld, int N, int j, T ct, double *vn1,
 	}
 }
 
+// at most 96 registers a thread (48 K of the SM's 64 K for 512 threads), so
+// that a GEMM CTA of another lane can share the SM with this one
 template <typename T, int NW, int NBK, int RPL, bool GM>
-__global__ void __launch_bounds__(NW * 32) k_qrp(QrArgs<T> a)
+__global__ void __maxnreg__(96) k_qrp(QrArgs<T> a)
 {
 	const int item = blockIdx.x;
 	if (item >= a.batch) return;
@@ -656,7 +645,7 @@ __global__ void __launch_bounds__(NW * 32) k_qrp(QrArgs<T> a)
 	extern __shared__ __align__(16) unsigned char smraw[];
 	T *A = GM ? a.work + (size_t)item * a.w_stride : (T *)smraw;
 	T *Vb = GM ? (T *)smraw : A + (size_t)ld * N;
-	T *tau = Vb + 2 * (size_t)ld * NBK;
+	T *tau = Vb + (size_t)ld * NBK;
 	T *Ts = tau + N;
 	double *dsh = (double *)(Ts + (size_t)np * NBK * NBK);
 	double *vv = dsh + N;
