@@ -349,6 +349,29 @@ def plain_chain_rate(sim, device, warm=2, timed=3):
         e.close()
 
 
+def profile_one_lane(sims, device, period_uneqlt):
+    """profile_mix of a copy of the same chains in a one-lane engine, so
+    that every launch covers all chain-spin items of the workload (the
+    timed engine splits them into lanes whose launches overlap; profiled
+    one lane at a time, each launch would cover a fraction and underfill
+    the GPU).  Returns the profile and the items of one launch."""
+    from dqmc_b200 import engine
+    old = os.environ.get("DQMC_LANES")
+    os.environ["DQMC_LANES"] = "1"
+    try:
+        e1 = engine.Engine([s.clone() for s in sims], device=device)
+    finally:
+        if old is None:
+            del os.environ["DQMC_LANES"]
+        else:
+            os.environ["DQMC_LANES"] = old
+    try:
+        e1.init()
+        return profile_mix(e1, period_uneqlt), 2 * len(sims)
+    finally:
+        e1.close()
+
+
 def profile_mix(eng, period_uneqlt):
     """Per-class (ms, launches, flops, bytes) of an average sweep: one eager
     equal-time sweep, and with unequal-time measurements every p sweeps one
@@ -474,10 +497,9 @@ def run_engine_workload(args, rank, world, local):
 
     e2e = e2e_rate(eng, sims, e2e_steps, world)
     log("e2e done")
-    prof = profile_mix(eng, pu)
+    prof, items = profile_one_lane(sims, local, pu)
     log("profile sweep done")
     peak = fp64_peak()
-    items = 2 * nch / eng.lanes()      # chain-spin items of one launch (lane)
     rl = roofline(prof, items, args.workload, peak, 1e3 * t_max / args.steps)
 
     plain = None
@@ -501,9 +523,10 @@ def run_engine_workload(args, rank, world, local):
         cfg = {"workload": wl["desc"], "chains_per_gpu": nch, "lanes": eng.lanes(),
                "l2": "inputs larger than L2" if nch * 2 * 20 * sims[0].N ** 2 * 8 > 126e6
                      else "inputs fit L2 (one small chain): L2 is not flushed",
-               "sweep_profile_note": "kernel ms per class over one eager sweep with each lane "
-                                     "profiled alone, lanes one after another; the timed sweeps "
-                                     "overlap the lanes, so the sum can exceed ms_per_step"}
+               "sweep_profile_note": "kernel ms per class over one eager sweep of a copy of "
+                                     "the same chains in one lane (every launch covers all "
+                                     "chain-spin items), CUDA events around each launch; the "
+                                     "timed sweeps run the chains in overlapping lanes"}
         if plain is not None:
             cfg["plain_1chain_gpu"] = {"value": plain, "unit": METRIC,
                                        "batched_over_plain": value / world / plain}

@@ -478,6 +478,8 @@ struct GroupBase {
 	virtual int get_chains(int c0, int n, uint64_t *rng, int *hs, int *sweep, int *eqn, void *eq,
 	                       int *uen, void *ue) = 0;
 	virtual int init() = 0;
+	// init without waiting for it on the host
+	virtual int init_async() = 0;
 	virtual int sweeps(int n, int sync) = 0;
 	virtual int get_chain(int c, uint64_t *rng, int *hs, int *sweep) = 0;
 	virtual int get_acc(int c, int *eqn, void *eq, int *uen, void *ue) = 0;
@@ -1236,7 +1238,9 @@ struct Group : GroupBase, ProfHook {
 		return 0;
 	}
 
-	int init() override
+	// G, clusters and draws from the current fields, queued on the group's
+	// stream (the lanes of an engine queue theirs side by side)
+	int enqueue_init()
 	{
 		const long long tot = (long long)C * 2 * L * N;
 		k_diag_all<<<grid_for(tot), 256, 0, st>>>(N, L, C, el.p, hs.p, dv.p, dvi.p);
@@ -1247,9 +1251,16 @@ struct Group : GroupBase, ProfHook {
 		draws(0);
 		need_draws = false;
 		need_init = false;
+		return 0;
+	}
+	int init() override
+	{
+		const int rc = enqueue_init();
+		if (rc) return rc;
 		CK(cudaStreamSynchronize(st));
 		return 0;
 	}
+	int init_async() override { return enqueue_init(); }
 
 	// queue one sweep of the given kind
 	int enqueue_sweep(bool meq, bool mue)
@@ -1278,7 +1289,7 @@ struct Group : GroupBase, ProfHook {
 	{
 		if (need_init) {
 			// fields were replaced: G, clusters and draws follow them again
-			const int rc = init();
+			const int rc = enqueue_init();
 			if (rc) return rc;
 		}
 		if (need_draws) {
@@ -1725,14 +1736,17 @@ struct Lanes : GroupBase {
 
 	int init() override
 	{
-		// after work the caller queued on the engine's stream
+		// after work the caller queued on the engine's stream; the lanes
+		// recompute side by side, each on its own stream
 		CK(cudaStreamSynchronize(st));
 		for (GroupBase *x : g) {
-			const int rc = x->init();
+			const int rc = x->init_async();
 			if (rc) return rc;
 		}
+		for (GroupBase *x : g) CK(cudaStreamSynchronize(x->stream()));
 		return 0;
 	}
+	int init_async() override { return init(); }
 
 	int sweeps(int n, int sync_after) override
 	{
@@ -1848,19 +1862,22 @@ struct Lanes : GroupBase {
 	}
 };
 
-// lanes of an engine of n_chain chains: DQMC_LANES when set, else one lane
-// per 64 real or 32 complex chains, at most 4 (at 256 chains of 12 x 12,
-// two lanes run 9% and four 11% more chain-sweeps per second than one,
-// eight no more than four; 64 complex 10 x 10 chains run 3% faster in two
-// lanes than in one; the real gradients of 128 configurations of 8 x 8 run
-// 182 evaluations/s in two lanes, 173 in one and 72 in four)
+// lanes of an engine of n_chain chains: DQMC_LANES when set, else for real
+// chains one lane per 32 from 256 chains up (at most 8) and one per 64 below
+// (at most 4), for complex chains one per 32 (at most 4).  Measured: 256
+// chains of 12 x 12 run 1235 / 1268 / 1288 / 1297 chain-sweeps/s in 2 / 4 /
+// 6 / 8 lanes (end to end 1136 in 4, 1156 in 8); the real gradients of 128
+// configurations of 8 x 8 run 719 evaluations/s in two lanes and 628 in
+// four; 64 complex 10 x 10 chains 507 in two lanes and 518 in four.
 static int lane_count(int n_chain, bool cplx)
 {
 	if (const char *v = getenv("DQMC_LANES")) {
 		const int n = atoi(v);
 		if (n >= 1) return std::min(n, n_chain);
 	}
-	return std::max(1, std::min(4, n_chain / (cplx ? 32 : 64)));
+	if (cplx) return std::max(1, std::min(4, n_chain / 32));
+	if (n_chain >= 256) return std::min(8, n_chain / 32);
+	return std::max(1, std::min(4, n_chain / 64));
 }
 
 }  // namespace dq

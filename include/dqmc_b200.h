@@ -95,8 +95,9 @@ int dqmc_acc_sizes(const dqmc_params *p, int *eq_size, int *ue_size);
 /* An engine advances n_chain chains of one parameter set (the batched form
  * of the reference's one chain per process, main_1.c:27-60 and dqmc.c).
  * It splits them into lanes, contiguous sub-batches with their own streams
- * whose kernels overlap on the GPU: one lane per 64 real or 32 complex
- * chains, at most 4, or
+ * whose kernels overlap on the GPU: one lane per 32 real chains from 256
+ * chains up (at most 8), one per 64 real chains below (at most 4), one per
+ * 32 complex chains (at most 4), or
  * the value of the environment variable DQMC_LANES at creation.  Results do
  * not depend on the split. */
 int dqmc_engine_create(const dqmc_params *p, int n_chain, int device,
