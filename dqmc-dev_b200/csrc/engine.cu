@@ -58,6 +58,47 @@ static GemmArgs<T> gargs(int M, int N, int K, int batch, const T *A, Addr aA, in
 
 // ------------------------------------------------------- small helper kernels
 
+// G drift of one recalculation, one block per item: the largest and the
+// mean |G - G_wrapped| over the N x N entries (the reference's matdiff,
+// dqmc.c:61-71), folded into the item's running maximum (non-negative
+// doubles order as their bit patterns) and running sum of means; block 0
+// counts the recalculations
+template <typename T>
+__global__ void k_gdrift(int N, const T *G, const T *Gw, unsigned long long *dmax, double *dsum,
+		int *count)
+{
+	const int b = blockIdx.x;
+	const long long NN = (long long)N * N;
+	const T *g = G + b * NN, *w = Gw + b * NN;
+	double mx = 0.0, sm = 0.0;
+	for (long long q = threadIdx.x; q < NN; q += blockDim.x) {
+		const double d = absv(g[q] - w[q]);
+		mx = (mx != mx) ? mx : ((d != d) ? d : fmax(mx, d));   // a NaN stays
+		sm += d;
+	}
+	__shared__ double smx[8], ssm[8];
+	for (int o = 16; o > 0; o >>= 1) {
+		const double om = __shfl_xor_sync(0xffffffffu, mx, o);
+		mx = (mx != mx) ? mx : ((om != om) ? om : fmax(mx, om));
+		sm += __shfl_xor_sync(0xffffffffu, sm, o);
+	}
+	const int lane = threadIdx.x & 31, w8 = threadIdx.x >> 5;
+	if (lane == 0) {
+		smx[w8] = mx;
+		ssm[w8] = sm;
+	}
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		for (int k = 1; k < (int)(blockDim.x >> 5); k++) {
+			mx = (mx != mx) ? mx : ((smx[k] != smx[k]) ? smx[k] : fmax(mx, smx[k]));
+			sm += ssm[k];
+		}
+		atomicMax(dmax + b, (unsigned long long)__double_as_longlong(mx));
+		dsum[b] += sm / (double)NN;
+		if (b == 0) count[0] += 1;
+	}
+}
+
 // d_l and 1/d_l of every slice from the fields: spin s uses exp_lambda[i + N*(h^s)]
 __global__ void k_diag_all(int N, int L, int nchain, const double *el, const int *hs,
 		double *dv, double *dvi)
@@ -494,6 +535,11 @@ struct GroupBase {
 	virtual int obs_grad(double *obs, void *Z) = 0;
 	// the eight hopping matrices exp(-+dt K), exp(-+dt K / 2) of both spins
 	virtual int set_hopping(const void *const *m) = 0;
+	// G drift self-check: on / off (resets the counters when turned on), and
+	// per chain c0 .. c0+n-1 the largest and the mean |G - G_wrapped| over
+	// the checked recalculations and both spins
+	virtual int set_check_g(int on) = 0;
+	virtual int g_drift(int c0, int n, double *mx, double *mean, int *count) = 0;
 };
 
 template <typename T>
@@ -567,6 +613,14 @@ struct Group : GroupBase, ProfHook {
 	DevBuf<int> pvt;
 	DevBuf<unsigned> err;
 	UneqState<T> ue;
+	// G drift self-check (off unless enabled): at every recalculation the G
+	// of the previous slice wrapped once more, against the recalculated G
+	// (the reference's CHECK_G_WRP, dqmc.c:15-16, 277-287, 339-343)
+	bool check_g = false;
+	DevBuf<T> Gw;                      // wrapped G of the recalculation slice
+	DevBuf<unsigned long long> dmax;   // [item] running max |G - G_wrapped| (bits)
+	DevBuf<double> dsum;               // [item] running sum of mean |G - G_wrapped|
+	DevBuf<int> dcount;                // recalculations checked
 
 	~Group() override
 	{
@@ -582,6 +636,7 @@ struct Group : GroupBase, ProfHook {
 		                     &bond2s};
 		for (auto *b : ib) b->release();
 		og.release();
+		Gw.release(); dmax.release(); dsum.release(); dcount.release();
 		el.release(); del.release(); dv.release(); dvi.release(); dR.release(); ldet.release();
 		rng.release(); rng_ckpt.release(); order.release(); ubuf.release(); err.release();
 		ue.release();
@@ -818,6 +873,58 @@ struct Group : GroupBase, ProfHook {
 		return 0;
 	}
 
+	int set_check_g(int on) override
+	{
+		CK(cudaStreamSynchronize(st));
+		if (on && !Gw.p) {
+			CK(cudaDeviceSynchronize());   // the allocations' zeroing runs on the default stream
+			int rc = Gw.alloc((size_t)NB * N * N);
+			rc |= dmax.alloc(NB);
+			rc |= dsum.alloc(NB);
+			rc |= dcount.alloc(1);
+			CK(cudaDeviceSynchronize());
+			if (rc) return rc;
+		}
+		if (on) {
+			CK(cudaMemsetAsync(dmax.p, 0, sizeof(unsigned long long) * NB, st));
+			CK(cudaMemsetAsync(dsum.p, 0, sizeof(double) * NB, st));
+			CK(cudaMemsetAsync(dcount.p, 0, sizeof(int), st));
+		}
+		if ((on != 0) != check_g) {
+			// the captured sweeps follow the setting from the next sweep on
+			for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
+			graphs.clear();
+			graph_launches.clear();
+			check_g = on != 0;
+		}
+		CK(cudaStreamSynchronize(st));
+		return 0;
+	}
+
+	int g_drift(int c0, int n, double *mx, double *mean, int *count) override
+	{
+		if (c0 < 0 || n < 0 || c0 + n > C) return DQMC_E_ARG;
+		if (!check_g || !dmax.p) return DQMC_E_ARG;
+		std::vector<unsigned long long> hm((size_t)2 * n);
+		std::vector<double> hs((size_t)2 * n);
+		int cnt = 0;
+		CK(cudaMemcpyAsync(hm.data(), dmax.p + (size_t)2 * c0, sizeof(unsigned long long) * 2 * n,
+		                   cudaMemcpyDeviceToHost, st));
+		CK(cudaMemcpyAsync(hs.data(), dsum.p + (size_t)2 * c0, sizeof(double) * 2 * n,
+		                   cudaMemcpyDeviceToHost, st));
+		CK(cudaMemcpyAsync(&cnt, dcount.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+		CK(cudaStreamSynchronize(st));
+		for (int q = 0; q < n; q++) {
+			double a, b;
+			memcpy(&a, &hm[2 * q], sizeof(double));
+			memcpy(&b, &hm[2 * q + 1], sizeof(double));
+			if (mx) mx[q] = (a != a || b != b) ? (a != a ? a : b) : fmax(a, b);
+			if (mean) mean[q] = cnt > 0 ? (hs[2 * q] + hs[2 * q + 1]) / (2.0 * cnt) : 0.0;
+		}
+		if (count) *count = cnt;
+		return 0;
+	}
+
 	// ------------------------------------------------------------ steps
 
 	void gemm(const GemmArgs<T> &g)
@@ -941,7 +1048,8 @@ struct Group : GroupBase, ProfHook {
 	}
 
 	// G <- B_l G B_l^-1 = exp_K (D G D^-1) inv_exp_K
-	void wrap(int l)
+	// dst = B_l G B_l^-1 (dst = G: the wrap of dqmc.c:293-296, 331-334)
+	void wrap_into(int l, T *dst)
 	{
 		const size_t NN = (size_t)N * N;
 		const Addr aI = per_item(NN);
@@ -951,8 +1059,9 @@ struct Group : GroupBase, ProfHook {
 		g.dinv = dvi.p + (size_t)l * N;
 		g.aD = per_item((long long)L * N);
 		gemm(g);
-		gemm(gargs<T>(N, N, N, NB, expK.p, per_spin(NN), N, W.p, aI, N, G.p, aI, N));
+		gemm(gargs<T>(N, N, N, NB, expK.p, per_spin(NN), N, W.p, aI, N, dst, aI, N));
 	}
+	void wrap(int l) { wrap_into(l, G.p); }
 
 	// Gh = inv_exp_halfK (G exp_halfK)  (dqmc.c:366-380)
 	void half_wrap(const T *src, Addr as, T *dst, Addr ad, int batch_items)
@@ -1270,9 +1379,14 @@ struct Group : GroupBase, ProfHook {
 			const int f = l / nmul;
 			const bool recalc = ((l + 1) % nmul) == 0;
 			if (recalc) {
+				if (check_g) wrap_into(l, Gw.p);
 				build_cluster(f);
 				int rc = calc_eq_g((f + 1) % F);
 				if (rc) return rc;
+				if (check_g) {
+					k_gdrift<T><<<NB, 256, 0, st>>>(N, G.p, Gw.p, dmax.p, dsum.p, dcount.p);
+					launch_count++;
+				}
 			} else {
 				wrap(l);
 			}
@@ -1852,6 +1966,29 @@ struct Lanes : GroupBase {
 		return 0;
 	}
 
+	int set_check_g(int on) override
+	{
+		CK(cudaStreamSynchronize(st));
+		for (GroupBase *x : g) {
+			const int rc = x->set_check_g(on);
+			if (rc) return rc;
+		}
+		return 0;
+	}
+
+	int g_drift(int first, int n, double *mx, double *mean, int *count) override
+	{
+		if (first != 0 || n != c0s()) return DQMC_E_ARG;
+		CK(cudaStreamSynchronize(st));
+		for (size_t k = 0; k < g.size(); k++) {
+			const size_t a = c0[k], m = c0[k + 1] - c0[k];
+			const int rc = g[k]->g_drift(0, (int)m, mx ? mx + a : nullptr, mean ? mean + a : nullptr,
+			                             count);
+			if (rc) return rc;
+		}
+		return 0;
+	}
+
 	int obs_grad(double *obs, void *Z) override
 	{
 		return per_lane([&](size_t k) {
@@ -2016,6 +2153,18 @@ int dqmc_engine_set_hopping(dqmc_engine *e, const void *exp_Ku, const void *exp_
 	const void *m[8] = {exp_Ku, exp_Kd, inv_exp_Ku, inv_exp_Kd, exp_halfKu, exp_halfKd,
 	                    inv_exp_halfKu, inv_exp_halfKd};
 	return e->g->set_hopping(m);
+}
+
+int dqmc_engine_check_g(dqmc_engine *e, int on)
+{
+	return e ? e->g->set_check_g(on) : DQMC_E_ARG;
+}
+
+int dqmc_engine_g_drift(dqmc_engine *e, double *max_abs, double *mean_abs, int *n_recalc)
+{
+	if (!e) return DQMC_E_ARG;
+	const int n = ((Lanes *)e->g)->c0s();
+	return e->g->g_drift(0, n, max_abs, mean_abs, n_recalc);
 }
 
 int dqmc_engine_profile_sweep(dqmc_engine *e, int meas_eq, int meas_ue, double *out, int n_class)

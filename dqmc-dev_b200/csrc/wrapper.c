@@ -435,6 +435,11 @@ static int engine_from(struct sim **sims, int n, dqmc_engine **out)
 {
 	int rc = dqmc_engine_create(&sims[0]->p, n, 0, out);
 	if (rc) return rc;
+	/* the runtime form of the reference's CHECK_G_WRP (dqmc.c:15-16) */
+	if (getenv("DQMC_CHECK_G")) {
+		rc = dqmc_engine_check_g(*out, 1);
+		if (rc) return rc;
+	}
 	for (int c = 0; c < n; c++) {
 		struct sim *s = sims[c];
 		rc = dqmc_engine_set_chain(*out, c, s->exp_lambda, s->del, s->rng, s->hs, s->sweep);
@@ -442,6 +447,21 @@ static int engine_from(struct sim **sims, int n, dqmc_engine **out)
 		if (rc) return rc;
 	}
 	return dqmc_engine_init(*out);
+}
+
+/* the G drift of the check (DQMC_CHECK_G), per chain, in the wording of the
+ * reference's matdiff lines (dqmc.c:61-71) */
+static void log_drift(FILE *log, dqmc_engine *e, int n)
+{
+	if (!getenv("DQMC_CHECK_G") || n < 1) return;
+	double *mx = malloc(sizeof(double) * 2 * (size_t)n);
+	if (!mx) return;
+	int cnt = 0;
+	if (dqmc_engine_g_drift(e, mx, mx + n, &cnt) == 0)
+		for (int c = 0; c < n; c++)
+			fprintf(log, "chain %d: g - gwrp over %d recalculations:\tmax %.3e\tavg %.3e\n", c, cnt,
+			        mx[c], mx[n + c]);
+	free(mx);
 }
 
 static int engine_pull(dqmc_engine *e, struct sim **sims, int n)
@@ -562,6 +582,7 @@ int dqmc_wrapper(const char *sim_file, const char *log_file, const int64_t max_t
 		goto cleanup;
 	}
 	rc = run_group(e, one, 1, &stp, &pr);
+	log_drift(log, e, 1);
 	if (rc == 5) {
 		fprintf(log, "dqmc() interrupted\n");
 		ret = WRAP_INCOMPLETE;

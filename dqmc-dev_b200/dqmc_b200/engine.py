@@ -254,6 +254,23 @@ class Engine:
         _lib.check(self.lib.dqmc_engine_set_hopping(self.h, *[c.ctypes.data for c in col]),
                    "dqmc_engine_set_hopping")
 
+    def check_g(self, on: bool = True):
+        """G drift self-check on or off (dqmc_engine_check_g; the runtime form
+        of the reference's CHECK_G_WRP): every recalculation also compares
+        the recalculated G with the previous slice's G wrapped once more."""
+        _lib.check(self.lib.dqmc_engine_check_g(self.h, int(on)), "dqmc_engine_check_g")
+
+    def g_drift(self):
+        """(max, mean, n_recalc): per chain the largest |G - G_wrapped| and its
+        mean over the entries, over the recalculations checked and both spins
+        (dqmc_engine_g_drift)."""
+        n = len(self.sims)
+        mx, mean = np.zeros(n), np.zeros(n)
+        cnt = C.c_int(0)
+        _lib.check(self.lib.dqmc_engine_g_drift(self.h, mx.ctypes.data, mean.ctypes.data,
+                                                C.addressof(cnt)), "dqmc_engine_g_drift")
+        return mx, mean, int(cnt.value)
+
     def stream(self) -> int:
         return int(self.lib.dqmc_engine_stream(self.h) or 0)
 

@@ -29,7 +29,7 @@ EXPORTS = [
     "dqmc_engine_accepts", "dqmc_engine_stream", "dqmc_engine_lanes",
     "dqmc_engine_set_chains", "dqmc_engine_get_chains", "dqmc_engine_launches_per_sweep",
     "dqmc_engine_profile_sweep", "dqmc_engine_logdet_grad", "dqmc_engine_obs_grad",
-    "dqmc_engine_set_hopping",
+    "dqmc_engine_set_hopping", "dqmc_engine_check_g", "dqmc_engine_g_drift",
     "dqmc_gpu_gemm", "dqmc_gpu_calc_eq_g", "dqmc_gpu_update_delayed", "dqmc_gpu_mul_seq",
     "dqmc_gpu_calc_eq_g_noalloc",
 ]
@@ -103,6 +103,8 @@ def load(path: str | None = None):
         "dqmc_engine_logdet_grad": (i, [vp, vp, vp]),
         "dqmc_engine_obs_grad": (i, [vp, vp, vp]),
         "dqmc_engine_set_hopping": (i, [vp] * 9),
+        "dqmc_engine_check_g": (i, [vp, i]),
+        "dqmc_engine_g_drift": (i, [vp, vp, vp, vp]),
         "dqmc_gpu_gemm": (i, [i, i, i, i, i, vp, vp, i, C.c_longlong, vp, i, C.c_longlong, vp,
                               vp, i, C.c_longlong, vp]),
         "dqmc_gpu_calc_eq_g": (i, [i, i, i, i, i, vp, vp, vp, vp]),

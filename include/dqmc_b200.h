@@ -194,6 +194,23 @@ int dqmc_engine_logdet_grad(dqmc_engine *e, double *logdet, void *S);
  * memory per chain and spin for the duration of the call. */
 int dqmc_engine_obs_grad(dqmc_engine *e, double *obs, void *Z);
 
+/* G drift self-check, the runtime form of the reference's compile-time
+ * CHECK_G_WRP (src/dqmc.c:15-16, 277-287, 339-343): with it on, at every
+ * recalculation of G the engine also wraps the previous slice's G once more
+ * (B_l G B_l^-1, as at the other slices) and compares it with the
+ * recalculated G, entry by entry as the reference's matdiff (dqmc.c:61-71).
+ * dqmc_engine_check_g turns it on (and clears the counters) or off; it costs
+ * one wrap and one N x N comparison per recalculation and N x N nums of
+ * device memory per chain and spin.  The results leave the sweep unchanged.
+ * dqmc_engine_g_drift gives per chain (arrays of n_chain) the largest
+ * |G - G_wrapped| over the checked recalculations and both spins, and its
+ * mean over the entries averaged over the recalculations and spins, and the
+ * number of recalculations checked; DQMC_E_ARG while the check is off.
+ * dqmc_wrapper turns it on when the environment variable DQMC_CHECK_G is
+ * set and writes the drift to its log. */
+int dqmc_engine_check_g(dqmc_engine *e, int on);
+int dqmc_engine_g_drift(dqmc_engine *e, double *max_abs, double *mean_abs, int *n_recalc);
+
 /* Replaces the hopping matrices of every chain (the eight exp(-+dt K) and
  * exp(-+dt K / 2) of dqmc_params, both spins) in place, without any device
  * allocation; G and the cluster products are recomputed from the chains'
