@@ -9,6 +9,7 @@
 #include <unistd.h>
 #include <cstring>
 #include <map>
+#include <new>
 #include <memory>
 #include <mutex>
 #include <thread>
@@ -540,6 +541,20 @@ struct GroupBase {
 	// the checked recalculations and both spins
 	virtual int set_check_g(int on) = 0;
 	virtual int g_drift(int c0, int n, double *mx, double *mean, int *count) = 0;
+	// one sweep of a batch graph (dqmc_batch_sweeps): the kind of the next
+	// sweep (bit 0 equal-time, bit 1 unequal-time measurements; -1 when the
+	// run is complete), the pending re-initialisation queued outside any
+	// capture, the sweep's kernels queued eagerly on the group's streams
+	// (captured by the caller) and the sweep counter advanced, or the counter
+	// advanced alone when a captured graph replays the sweep
+	virtual int sweep_kind() = 0;
+	virtual int prepare() = 0;
+	virtual int enqueue_one() = 0;
+	virtual void advance() = 0;
+	// make stream s wait for the work queued so far on every stream of the
+	// group, and every stream of the group wait for event ev
+	virtual int join_into(cudaStream_t s) = 0;
+	virtual int wait_on(cudaEvent_t ev) = 0;
 };
 
 template <typename T>
@@ -625,6 +640,7 @@ struct Group : GroupBase, ProfHook {
 	~Group() override
 	{
 		for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
+		if (jev) cudaEventDestroy(jev);
 		DevBuf<T> *tb[] = {&expK, &iexpK, &ehK, &iehK, &peu, &ped, &phase, &G, &Cl, &Qm, &Tm,
 		                   &Tm2, &Rs, &X, &W, &Gh, &acc_eq, &acc_ue, &phi, &qdet, &Sg, &Pr,
 		                   &ppu, &ppd, &ppru, &pprd, &gs_eq, &gs_ue};
@@ -1399,6 +1415,54 @@ struct Group : GroupBase, ProfHook {
 		return 0;
 	}
 
+	int sweep_kind() override
+	{
+		if (sweep >= p.n_sweep) return -1;
+		const bool meq = sweep >= p.n_sweep_warm;
+		const bool mue = meq && p.period_uneqlt > 0 && sweep % p.period_uneqlt == 0;
+		return (meq ? 1 : 0) | (mue ? 2 : 0);
+	}
+	int prepare() override
+	{
+		if (need_init) {
+			const int rc = enqueue_init();
+			if (rc) return rc;
+		}
+		if (need_draws) {
+			draws(0);
+			need_draws = false;
+		}
+		return 0;
+	}
+	int enqueue_one() override
+	{
+		const int kind = sweep_kind();
+		if (kind < 0) return 0;
+		launch_count = 0;
+		const int rc = enqueue_sweep((kind & 1) != 0, (kind & 2) != 0);
+		if (rc) return rc;
+		if (!graph_launches.count(kind)) graph_launches[kind] = launch_count;
+		sweep++;
+		return 0;
+	}
+	void advance() override
+	{
+		if (sweep < p.n_sweep) sweep++;
+	}
+	cudaEvent_t jev = nullptr;
+	int join_into(cudaStream_t s) override
+	{
+		if (!jev) CK(cudaEventCreateWithFlags(&jev, cudaEventDisableTiming));
+		CK(cudaEventRecord(jev, st));
+		CK(cudaStreamWaitEvent(s, jev, 0));
+		return 0;
+	}
+	int wait_on(cudaEvent_t ev) override
+	{
+		CK(cudaStreamWaitEvent(st, ev, 0));
+		return 0;
+	}
+
 	int sweeps(int n, int sync_after) override
 	{
 		if (need_init) {
@@ -1976,6 +2040,54 @@ struct Lanes : GroupBase {
 		return 0;
 	}
 
+	int sweep_kind() override { return g[0]->sweep_kind(); }
+	int prepare() override
+	{
+		// after work the caller queued on the engine's stream
+		CK(cudaEventRecord(ev[0], st));
+		for (GroupBase *x : g) {
+			CK(cudaStreamWaitEvent(x->stream(), ev[0], 0));
+			const int rc = x->prepare();
+			if (rc) return rc;
+		}
+		return 0;
+	}
+	int enqueue_one() override
+	{
+		CK(cudaEventRecord(ev[0], st));
+		for (size_t k = 0; k < g.size(); k++) {
+			CK(cudaStreamWaitEvent(g[k]->stream(), ev[0], 0));
+			const int rc = g[k]->enqueue_one();
+			CK(cudaEventRecord(ev[1 + k], g[k]->stream()));
+			CK(cudaStreamWaitEvent(st, ev[1 + k], 0));
+			if (rc) return rc;
+		}
+		return 0;
+	}
+	void advance() override
+	{
+		for (GroupBase *x : g) x->advance();
+	}
+	int join_into(cudaStream_t s) override
+	{
+		for (GroupBase *x : g) {
+			const int rc = x->join_into(s);
+			if (rc) return rc;
+		}
+		CK(cudaEventRecord(ev[0], st));
+		CK(cudaStreamWaitEvent(s, ev[0], 0));
+		return 0;
+	}
+	int wait_on(cudaEvent_t e) override
+	{
+		CK(cudaStreamWaitEvent(st, e, 0));
+		for (GroupBase *x : g) {
+			const int rc = x->wait_on(e);
+			if (rc) return rc;
+		}
+		return 0;
+	}
+
 	int g_drift(int first, int n, double *mx, double *mean, int *count) override
 	{
 		if (first != 0 || n != c0s()) return DQMC_E_ARG;
@@ -2025,6 +2137,83 @@ struct dqmc_engine {
 	GroupBase *g;
 	int cplx;
 };
+
+// engines advanced together, one CUDA graph launch per sweep for all of them
+struct dqmc_batch {
+	std::vector<dqmc_engine *> es;
+	cudaStream_t st = nullptr;
+	cudaEvent_t fork = nullptr, done = nullptr;
+	std::vector<cudaEvent_t> join;
+	std::map<std::vector<int>, cudaGraphExec_t> graphs;   // by the engines' sweep kinds
+	~dqmc_batch()
+	{
+		for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
+		for (cudaEvent_t e : join) cudaEventDestroy(e);
+		if (fork) cudaEventDestroy(fork);
+		if (done) cudaEventDestroy(done);
+		if (st) cudaStreamDestroy(st);
+	}
+};
+
+// One sweep of every engine of b that has sweeps left, as one graph launch
+// on b's stream: the graph for this combination of sweep kinds is captured
+// on first use (a fork from b's stream into every engine and its lanes, each
+// engine's sweep kernels queued eagerly there, and the joins back), and
+// replayed afterwards.  Pending re-initialisations run first, outside the
+// graph.  Returns 1 when no engine had a sweep left.
+static int batch_sweep(dqmc_batch *b)
+{
+	std::vector<int> key(b->es.size());
+	bool any = false;
+	for (size_t i = 0; i < b->es.size(); i++) {
+		key[i] = b->es[i]->g->sweep_kind();
+		any |= key[i] >= 0;
+	}
+	if (!any) return 1;
+	for (size_t i = 0; i < b->es.size(); i++) {
+		if (key[i] < 0) continue;
+		int rc = b->es[i]->g->prepare();
+		if (!rc) rc = b->es[i]->g->join_into(b->st);
+		if (rc) return rc;
+	}
+	auto it = b->graphs.find(key);
+	if (it == b->graphs.end()) {
+		cudaGraph_t gr;
+		CK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+		int rc = 0;
+		cudaError_t ce = cudaEventRecord(b->fork, b->st);
+		for (size_t i = 0; i < b->es.size() && !rc && ce == cudaSuccess; i++) {
+			if (key[i] < 0) continue;
+			GroupBase *x = b->es[i]->g;
+			ce = cudaStreamWaitEvent(x->stream(), b->fork, 0);
+			if (ce == cudaSuccess) rc = x->enqueue_one();
+			if (ce == cudaSuccess) ce = cudaEventRecord(b->join[i], x->stream());
+			if (ce == cudaSuccess) ce = cudaStreamWaitEvent(b->st, b->join[i], 0);
+		}
+		const cudaError_t ee = cudaStreamEndCapture(b->st, &gr);
+		if (rc) return rc;
+		if (ce != cudaSuccess || ee != cudaSuccess) {
+			fprintf(stderr, "dqmc_b200: batch graph capture failed: %s\n",
+			        cudaGetErrorString(ce != cudaSuccess ? ce : ee));
+			return DQMC_E_CUDA;
+		}
+		cudaGraphExec_t ex;
+		const cudaError_t ie = cudaGraphInstantiate(&ex, gr, 0);
+		cudaGraphDestroy(gr);
+		CK(ie);
+		it = b->graphs.emplace(key, ex).first;
+	} else {
+		for (size_t i = 0; i < b->es.size(); i++)
+			if (key[i] >= 0) b->es[i]->g->advance();
+	}
+	CK(cudaGraphLaunch(it->second, b->st));
+	CK(cudaEventRecord(b->done, b->st));
+	for (dqmc_engine *e : b->es) {
+		const int rc = e->g->wait_on(b->done);
+		if (rc) return rc;
+	}
+	return 0;
+}
 
 extern "C" {
 
@@ -2153,6 +2342,55 @@ int dqmc_engine_set_hopping(dqmc_engine *e, const void *exp_Ku, const void *exp_
 	const void *m[8] = {exp_Ku, exp_Kd, inv_exp_Ku, inv_exp_Kd, exp_halfKu, exp_halfKd,
 	                    inv_exp_halfKu, inv_exp_halfKd};
 	return e->g->set_hopping(m);
+}
+
+int dqmc_batch_create(dqmc_engine *const *engines, int n, dqmc_batch **out)
+{
+	if (!engines || n < 1 || !out) return DQMC_E_ARG;
+	*out = nullptr;
+	if (getenv("DQMC_DEBUG_SYNC")) return DQMC_E_ARG;   // its eager checks cannot be captured
+	dqmc_batch *b = new (std::nothrow) dqmc_batch;
+	if (!b) return DQMC_E_NOMEM;
+	for (int i = 0; i < n; i++) {
+		if (!engines[i]) {
+			delete b;
+			return DQMC_E_ARG;
+		}
+		b->es.push_back(engines[i]);
+	}
+	b->join.assign(n, nullptr);
+	bool ok = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) == cudaSuccess &&
+	          cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) == cudaSuccess &&
+	          cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) == cudaSuccess;
+	for (int i = 0; ok && i < n; i++)
+		ok = cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming) == cudaSuccess;
+	if (!ok) {
+		delete b;
+		return DQMC_E_CUDA;
+	}
+	*out = b;
+	return 0;
+}
+
+int dqmc_batch_sweeps(dqmc_batch *b, int n_sweeps, int sync)
+{
+	if (!b || n_sweeps < 0) return DQMC_E_ARG;
+	for (int k = 0; k < n_sweeps; k++) {
+		const int rc = batch_sweep(b);
+		if (rc == 1) break;
+		if (rc) return rc;
+	}
+	if (sync) CK(cudaStreamSynchronize(b->st));
+	return 0;
+}
+
+void *dqmc_batch_stream(dqmc_batch *b) { return b ? (void *)b->st : nullptr; }
+
+void dqmc_batch_destroy(dqmc_batch *b)
+{
+	if (!b) return;
+	cudaStreamSynchronize(b->st);
+	delete b;
 }
 
 int dqmc_engine_check_g(dqmc_engine *e, int on)

@@ -14,10 +14,13 @@ namespace dq {
 // 226 KB leaves room for the kernels' static shared memory
 static const size_t SMEM_FIT = 226 * 1024;
 
+// carve: the shared-memory forms take the largest shared-memory carveout
+// (room for a GEMM CTA beside them); the global-memory forms keep the
+// default, whose L1 serves their working matrix
 template <typename K, typename Args>
-static int launch_dense(K kern, const Args &a, size_t sm, cudaStream_t st)
+static int launch_dense(K kern, const Args &a, size_t sm, cudaStream_t st, bool carve)
 {
-	if (raise_smem(kern, sm, true) != cudaSuccess) return DQMC_E_ARG;
+	if (raise_smem(kern, sm, carve) != cudaSuccess) return DQMC_E_ARG;
 	kern<<<a.batch, 512, sm, st>>>(a);
 	return 0;
 }
@@ -25,13 +28,13 @@ static int launch_dense(K kern, const Args &a, size_t sm, cudaStream_t st)
 template <typename T, int RPL, bool GM>
 static int launch_qrb_rpl(const QrArgs<T> &a, cudaStream_t st)
 {
-	return launch_dense(k_qrb<T, 16, 8, RPL, GM>, a, qrb_smem_bytes<T, 8>(a.N, GM), st);
+	return launch_dense(k_qrb<T, 16, 8, RPL, GM>, a, qrb_smem_bytes<T, 8>(a.N, GM), st, !GM);
 }
 
 template <typename T, int RPL, bool GM>
 static int launch_qrp_rpl(const QrArgs<T> &a, cudaStream_t st)
 {
-	return launch_dense(k_qrp<T, 16, 8, RPL, GM>, a, qrp_smem_bytes<T, 8>(a.N, GM), st);
+	return launch_dense(k_qrp<T, 16, 8, RPL, GM>, a, qrp_smem_bytes<T, 8>(a.N, GM), st, !GM);
 }
 
 template <typename T, bool GM>
@@ -73,7 +76,7 @@ int launch_qr_pivot(const QrArgs<T> &a, cudaStream_t st)
 template <typename T, int RPL, bool GM>
 static int launch_rec_rpl(const RecArgs<T> &a, cudaStream_t st)
 {
-	return launch_dense(k_recb<T, 16, RPL, 3, GM>, a, recb_smem_bytes<T>(a.N, GM), st);
+	return launch_dense(k_recb<T, 16, RPL, 3, GM>, a, recb_smem_bytes<T>(a.N, GM), st, !GM);
 }
 
 template <typename T, bool GM>

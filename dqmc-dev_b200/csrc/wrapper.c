@@ -701,6 +701,19 @@ int dqmc_wrapper_batch(int n_files, const char *const *sim_files, const char *lo
 		pr.t[PR_INIT] += time_wall() - t0;
 		pr.n[PR_INIT]++;
 	}
+	/* every round of all groups as one CUDA graph launch (dqmc_batch) while
+	 * every unfinished group sweeps; per-group launches otherwise */
+	dqmc_batch *batch = NULL;
+	{
+		int ok = ng > 0;
+		dqmc_engine **es = calloc(ng > 0 ? ng : 1, sizeof(dqmc_engine *));
+		for (int gi = 0; ok && gi < ng; gi++) {
+			if (gs[gi].rc || !gs[gi].e) ok = 0;
+			else es[gi] = gs[gi].e;
+		}
+		if (ok && es && dqmc_batch_create(es, ng, &batch) != 0) batch = NULL;
+		free(es);
+	}
 	for (;;) {
 		int active = 0;
 		const int64_t t0 = time_wall();
@@ -721,22 +734,32 @@ int dqmc_wrapper_batch(int n_files, const char *const *sim_files, const char *lo
 				pr.n[PR_CHECKPOINT]++;
 				if (rc) { g->rc = 6; continue; }
 			}
-			g->rc = dqmc_engine_sweeps(g->e, 1, 0);
-			if (g->rc) continue;
 			g->queued = 1;
 			active = 1;
 		}
 		if (!active) break;
+		int whole = batch != NULL;
+		for (int gi = 0; gi < ng; gi++)
+			if (!gs[gi].queued && !gs[gi].done) whole = 0;   /* stopped or failed */
+		if (whole) {
+			const int rc = dqmc_batch_sweeps(batch, 1, 1);
+			for (int gi = 0; rc && gi < ng; gi++)
+				if (gs[gi].queued) gs[gi].rc = rc;
+		} else {
+			for (int gi = 0; gi < ng; gi++)
+				if (gs[gi].queued) gs[gi].rc = dqmc_engine_sweeps(gs[gi].e, 1, 0);
+		}
 		for (int gi = 0; gi < ng; gi++) {
 			struct grp *g = &gs[gi];
-			if (!g->queued) continue;
-			g->rc = dqmc_engine_sync(g->e);
+			if (!g->queued || g->rc) continue;
+			if (!whole) g->rc = dqmc_engine_sync(g->e);
 			if (g->rc) continue;
 			for (int c = 0; c < g->n; c++) g->m[c]->sweep++;
 		}
 		pr.t[PR_SWEEPS] += time_wall() - t0;
 		pr.n[PR_SWEEPS]++;
 	}
+	dqmc_batch_destroy(batch);   /* before its engines */
 	for (int gi = 0; gi < ng; gi++) {
 		struct grp *g = &gs[gi];
 		int rc = g->rc;

@@ -5,9 +5,10 @@ per group: the lattice and its measurement maps, L and n_matmul, the
 hopping matrices, the measurement periods and the sweep counters.  U may
 differ inside a group, because exp_lambda and del are per chain.  A ragged
 batch therefore splits its chains into such groups.  Each group gets its own
-engine and CUDA stream, and each sweep queues every group's captured sweep
-graph before waiting for any of them.  Groups of different size and length
-so run concurrently, as the C drop-in's dqmc_wrapper_batch runs them.
+engine and CUDA streams, and every sweep of the whole batch is one CUDA graph
+launch (dqmc_batch_sweeps) that forks into all groups and joins back, so
+groups of different size and length run concurrently, as the C drop-in's
+dqmc_wrapper_batch runs them.
 
 The delay rank (n_delay: rank-k updates collected before they are flushed
 into G) trades per-accept work against flush traffic, and the best value
@@ -24,6 +25,9 @@ from collections import OrderedDict
 
 import numpy as np
 
+import ctypes as C
+
+from . import lib as _lib
 from .engine import INT_PARAMS, Engine, SimData
 
 # parameters a group shares (everything except U's exp_lambda and del)
@@ -78,7 +82,7 @@ class RaggedBatch:
     """Chains of any parameters advanced together; see the module docstring."""
 
     def __init__(self, sims: list[SimData], device: int = 0, autotune: bool = False,
-                 candidates=(4, 8, 16, 32)):
+                 candidates=(4, 8, 16, 32), one_graph: bool = True):
         if not sims:
             raise ValueError("no chains")
         self.sims = sims
@@ -96,19 +100,38 @@ class RaggedBatch:
         self.engines = [Engine([sims[i] for i in idx], device=device,
                                n_delay=self.delay.get(sims[idx[0]].N))
                         for idx in self.groups]
+        # one CUDA graph launch per sweep of all groups (dqmc_batch), or
+        # (one_graph False) every group's own sweep graph on its own stream
+        self.lib = self.engines[0].lib
+        self.b = None
+        if one_graph:
+            hs = (C.c_void_p * len(self.engines))(*[e.h for e in self.engines])
+            b = C.c_void_p()
+            _lib.check(self.lib.dqmc_batch_create(hs, len(self.engines), C.byref(b)),
+                       "dqmc_batch_create")
+            self.b = b
 
     def init(self):
         for e in self.engines:
             e.init()
 
-    def sweeps(self, n: int = 1):
-        """n sweeps of every chain: sweep by sweep, all groups queued before
-        any is waited for."""
-        for _ in range(n):
-            for e in self.engines:
-                e.sweeps(1, sync=False)
-            for e in self.engines:
-                e.sync()
+    def sweeps(self, n: int = 1, sync: bool = True):
+        """n sweeps of every chain, each one CUDA graph launch for all groups
+        (captured on first use for each combination of sweep kinds) on the
+        batch's stream."""
+        if self.b is None:
+            for _ in range(n):
+                for e in self.engines:
+                    e.sweeps(1, sync=False)
+                for e in self.engines:
+                    e.sync()
+            return
+        _lib.check(self.lib.dqmc_batch_sweeps(self.b, n, int(sync)), "dqmc_batch_sweeps")
+
+    def stream(self) -> int:
+        """The batch's cudaStream_t (as an integer), on which its sweeps run
+        (0 without the batch graph)."""
+        return int(self.lib.dqmc_batch_stream(self.b) or 0) if self.b is not None else 0
 
     def errors(self) -> int:
         out = 0
@@ -121,6 +144,9 @@ class RaggedBatch:
             e.pull()
 
     def close(self):
+        if getattr(self, "b", None):
+            self.lib.dqmc_batch_destroy(self.b)
+            self.b = None
         for e in self.engines:
             e.close()
         self.engines = []

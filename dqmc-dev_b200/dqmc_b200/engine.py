@@ -201,6 +201,15 @@ class Engine:
     def init(self):
         _lib.check(self.lib.dqmc_engine_init(self.h), "dqmc_engine_init")
 
+    def push(self):
+        """Upload every chain's state from its SimData again
+        (dqmc_engine_set_chain); G, the cluster products and the draws follow
+        the uploaded fields before the next sweep.  The accumulators stay."""
+        for c, s in enumerate(self.sims):
+            _lib.check(self.lib.dqmc_engine_set_chain(
+                self.h, c, s.exp_lambda.ctypes.data, s.del_.ctypes.data, s.rng.ctypes.data,
+                s.hs.ctypes.data, s.sweep), "dqmc_engine_set_chain")
+
     def sweeps(self, n: int, sync: bool = True):
         _lib.check(self.lib.dqmc_engine_sweeps(self.h, n, int(sync)), "dqmc_engine_sweeps")
 

@@ -194,6 +194,28 @@ int dqmc_engine_logdet_grad(dqmc_engine *e, double *logdet, void *S);
  * memory per chain and spin for the duration of the call. */
 int dqmc_engine_obs_grad(dqmc_engine *e, double *obs, void *Z);
 
+/* Engines advanced together (the ragged batch: one engine per parameter
+ * group, any lattice, L or hopping): every dqmc_batch_sweeps sweep of all
+ * engines that have sweeps left is ONE CUDA graph launch on the batch's own
+ * stream.  The graph of a combination of the engines' sweep kinds (warm-up,
+ * equal-time, unequal-time) is captured on first use: it forks from the
+ * batch stream into every engine and each of its lanes, holds each engine's
+ * sweep kernels, and joins back.  Fields replaced through
+ * dqmc_engine_set_chain(s) are taken up (G recomputed) before the launch,
+ * outside the graph.  Work queued afterwards on an engine (its calls, its
+ * stream) is ordered after the batch's sweeps.  The engines must belong to
+ * one device and stay alive for the batch's lifetime; dqmc_batch_create
+ * refuses while DQMC_DEBUG_SYNC is set (its per-launch host checks cannot be
+ * captured).  No counterpart in the reference, which runs one chain per
+ * process; the sweep of each engine is that of src/dqmc.c:247-386. */
+typedef struct dqmc_batch dqmc_batch;
+int dqmc_batch_create(dqmc_engine *const *engines, int n, dqmc_batch **out);
+/* n_sweeps sweeps (fewer when every engine completes); sync: wait for them */
+int dqmc_batch_sweeps(dqmc_batch *b, int n_sweeps, int sync);
+/* the batch's cudaStream_t, as void* */
+void *dqmc_batch_stream(dqmc_batch *b);
+void dqmc_batch_destroy(dqmc_batch *b);
+
 /* G drift self-check, the runtime form of the reference's compile-time
  * CHECK_G_WRP (src/dqmc.c:15-16, 277-287, 339-343): with it on, at every
  * recalculation of G the engine also wraps the previous slice's G once more

@@ -55,6 +55,43 @@ def test_ragged_batch_matches_oracle(mods, tmp_path):
     rb.close()
 
 
+def test_batch_graph_matches_separate_engines(mods):
+    """The ragged batch's one-graph sweeps (dqmc_batch_sweeps, groups of
+    different lattices and L, uneven sweep kinds: warm-up then measuring)
+    against the same groups swept engine by engine: fields, RNG state and
+    accumulators bit-identical; also after fields are replaced in the middle
+    of the run (the re-initialisation runs before the graph)."""
+    batch, engine, gen, simfile = mods
+    dicts = _ragged(gen, 7, 21)
+    a = [engine.SimData(d) for d in dicts]
+    b = [engine.SimData(d) for d in dicts]
+    rb = batch.RaggedBatch(a)
+    rb.init()
+    rb.sweeps(1)
+    rb.pull()
+    for e in rb.engines:      # replace the fields: every group re-initialises
+        e.push()
+    rb.sweeps(a[0].p["n_sweep"])
+    rb.pull()
+    assert rb.errors() == 0
+    engines = [engine.Engine([b[i] for i in idx]) for idx in rb.groups]
+    rb.close()
+    for e in engines:
+        e.init()
+        e.sweeps(1)
+        e.pull()
+        e.push()
+        e.sweeps(b[0].p["n_sweep"])
+        e.pull()
+        assert e.errors() == 0
+        e.close()
+    for c, (x, y) in enumerate(zip(a, b)):
+        assert x.sweep == y.sweep == x.p["n_sweep"], c
+        assert np.array_equal(x.hs, y.hs), c
+        assert np.array_equal(x.rng, y.rng), c
+        assert np.array_equal(x.eq_acc, y.eq_acc), c
+
+
 def test_autotuned_ragged_batch_runs(mods):
     batch, engine, gen, simfile = mods
     sims = [engine.SimData(d) for d in _ragged(gen, 5, 12)]
