@@ -15,7 +15,9 @@ into G) trades per-accept work against flush traffic, and the best value
 depends on N.  With `autotune`, each lattice size gets the candidate whose
 timed sweep of a copy of its first group is shortest.  Changing n_delay
 changes results only by rounding; without `autotune` every group keeps its
-files' value.
+files' value.  `autotune` also times every group of 32 chains or more in
+1, 2, 4 and 8 lanes (sub-batches whose launches overlap) and keeps the
+fastest; lanes never change results.
 """
 from __future__ import annotations
 
@@ -48,11 +50,13 @@ def group_key(s: SimData) -> str:
     return h.hexdigest()
 
 
-def time_sweep(sims: list[SimData], n_delay: int | None, device: int = 0) -> float:
-    """Seconds of one sweep of copies of `sims` at delay rank n_delay (after
-    one untimed sweep that also captures the sweep graph)."""
+def time_sweep(sims: list[SimData], n_delay: int | None, device: int = 0,
+               lanes: int | None = None) -> float:
+    """Seconds of one sweep of copies of `sims` at delay rank n_delay in
+    `lanes` sub-batches (after one untimed sweep that also captures the
+    sweep graph)."""
     copies = [s.clone() for s in sims]
-    e = Engine(copies, device=device, n_delay=n_delay)
+    e = Engine(copies, device=device, n_delay=n_delay, lanes=lanes)
     try:
         e.init()
         e.sweeps(1, sync=True)
@@ -61,6 +65,22 @@ def time_sweep(sims: list[SimData], n_delay: int | None, device: int = 0) -> flo
         return time.perf_counter() - t0
     finally:
         e.close()
+
+
+def autotune_lanes(sims: list[SimData], candidates=(1, 2, 4, 8), device: int = 0,
+                   n_delay: int | None = None) -> int:
+    """The lane count (sub-batches with their own streams, whose launches
+    overlap) with the shortest timed sweep of copies of all of `sims`;
+    candidates above the number of chains are skipped.  Any lane count gives
+    the same results, so the choice only changes the speed."""
+    best, best_t = None, None
+    for n in candidates:
+        if n > len(sims):
+            continue
+        t = time_sweep(sims, n_delay, device, lanes=n)
+        if best_t is None or t < best_t:
+            best, best_t = n, t
+    return best
 
 
 def autotune_delay(sims: list[SimData], candidates=(4, 8, 16, 32), device: int = 0,
@@ -97,9 +117,17 @@ class RaggedBatch:
                 n = sims[idx[0]].N
                 if n not in self.delay:
                     self.delay[n] = autotune_delay([sims[i] for i in idx], candidates, device)
+        # the lane count of every group large enough to split (lanes change
+        # only the speed, never the results)
+        self.lanes = {}
+        if autotune:
+            for g, idx in enumerate(self.groups):
+                if len(idx) >= 32:
+                    self.lanes[g] = autotune_lanes([sims[i] for i in idx], device=device,
+                                                   n_delay=self.delay.get(sims[idx[0]].N))
         self.engines = [Engine([sims[i] for i in idx], device=device,
-                               n_delay=self.delay.get(sims[idx[0]].N))
-                        for idx in self.groups]
+                               n_delay=self.delay.get(sims[idx[0]].N), lanes=self.lanes.get(g))
+                        for g, idx in enumerate(self.groups)]
         # one CUDA graph launch per sweep of all groups (dqmc_batch), or
         # (one_graph False) every group's own sweep graph on its own stream
         self.lib = self.engines[0].lib

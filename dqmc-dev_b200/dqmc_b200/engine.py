@@ -8,6 +8,7 @@ parameter set; the arithmetic all happens in libdqmc_b200.so.
 from __future__ import annotations
 
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -174,12 +175,26 @@ class SimData:
 class Engine:
     """A group of chains with one parameter set, advanced on one GPU."""
 
-    def __init__(self, sims: list[SimData], device: int = 0, n_delay: int | None = None):
+    def __init__(self, sims: list[SimData], device: int = 0, n_delay: int | None = None,
+                 lanes: int | None = None):
         """n_delay overrides the sim files' delay rank (the flush period of
         the delayed update); results then differ from the file's setting
-        only by rounding."""
+        only by rounding.  lanes overrides the number of sub-batches with
+        their own streams (else the engine's rule, or DQMC_LANES); results
+        do not depend on it."""
         if not sims:
             raise ValueError("no chains")
+        if lanes is not None:
+            old = os.environ.get("DQMC_LANES")
+            os.environ["DQMC_LANES"] = str(int(lanes))
+            try:
+                self.__init__(sims, device, n_delay, None)
+            finally:
+                if old is None:
+                    del os.environ["DQMC_LANES"]
+                else:
+                    os.environ["DQMC_LANES"] = old
+            return
         self.lib = _lib.load()
         self.sims = sims
         s0 = sims[0]

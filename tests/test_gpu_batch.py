@@ -92,6 +92,37 @@ def test_batch_graph_matches_separate_engines(mods):
         assert np.array_equal(x.eq_acc, y.eq_acc), c
 
 
+def test_autotune_lanes_picks_a_candidate_and_keeps_results(mods):
+    """The lane tuner returns one of its candidates, and an engine in the
+    chosen lanes gives bit-identical results to one lane."""
+    batch, engine, gen, simfile = mods
+    from dqmc_b200 import replicas
+    rngs = replicas.chain_streams(5, range(8))
+    base = gen.make_sim(init_rng=rngs[0], Nx=4, Ny=4, U=4.0, dt=0.1, L=20, n_matmul=5,
+                        n_delay=4, period_eqlt=5, n_sweep_warm=0, n_sweep_meas=3)
+    dicts = [base]
+    for r in rngs[1:]:
+        hs, rr = gen.initial_hs(r, 20, 16)
+        d = dict(base)
+        d["state/init_rng"], d["state/rng"], d["state/hs"] = r, rr, hs
+        dicts.append(d)
+    sims = [engine.SimData(d) for d in dicts]
+    n = batch.autotune_lanes(sims, candidates=(1, 2, 4))
+    assert n in (1, 2, 4)
+    runs = []
+    for lanes in (1, n):
+        ss = [s.clone() for s in sims]
+        e = engine.Engine(ss, lanes=lanes)
+        assert e.lanes() == lanes
+        e.init()
+        e.sweeps(3)
+        e.pull()
+        e.close()
+        runs.append(ss)
+    for a, b in zip(*runs):
+        assert np.array_equal(a.hs, b.hs) and np.array_equal(a.eq_acc, b.eq_acc)
+
+
 def test_autotuned_ragged_batch_runs(mods):
     batch, engine, gen, simfile = mods
     sims = [engine.SimData(d) for d in _ragged(gen, 5, 12)]
