@@ -65,12 +65,12 @@ static GemmArgs<T> gargs(int M, int N, int K, int batch, const T *A, Addr aA, in
 // doubles order as their bit patterns) and running sum of means; block 0
 // counts the recalculations
 template <typename T>
-__global__ void k_gdrift(int N, const T *G, const T *Gw, unsigned long long *dmax, double *dsum,
-		int *count)
+__global__ void k_gdrift(int N, const T *G, const T *Gw, long long w_stride,
+		unsigned long long *dmax, double *dsum, int *count)
 {
 	const int b = blockIdx.x;
 	const long long NN = (long long)N * N;
-	const T *g = G + b * NN, *w = Gw + b * NN;
+	const T *g = G + b * NN, *w = Gw + b * w_stride;
 	double mx = 0.0, sm = 0.0;
 	for (long long q = threadIdx.x; q < NN; q += blockDim.x) {
 		const double d = absv(g[q] - w[q]);
@@ -540,7 +540,7 @@ struct GroupBase {
 	// per chain c0 .. c0+n-1 the largest and the mean |G - G_wrapped| over
 	// the checked recalculations and both spins
 	virtual int set_check_g(int on) = 0;
-	virtual int g_drift(int c0, int n, double *mx, double *mean, int *count) = 0;
+	virtual int g_drift(int which, int c0, int n, double *mx, double *mean, int *count) = 0;
 	// one sweep of a batch graph (dqmc_batch_sweeps): the kind of the next
 	// sweep (bit 0 equal-time, bit 1 unequal-time measurements; -1 when the
 	// run is complete), the pending re-initialisation queued outside any
@@ -895,16 +895,16 @@ struct Group : GroupBase, ProfHook {
 		if (on && !Gw.p) {
 			CK(cudaDeviceSynchronize());   // the allocations' zeroing runs on the default stream
 			int rc = Gw.alloc((size_t)NB * N * N);
-			rc |= dmax.alloc(NB);
-			rc |= dsum.alloc(NB);
-			rc |= dcount.alloc(1);
+			rc |= dmax.alloc(2 * (size_t)NB);     // [0, NB): wrap check, [NB, 2 NB): unequal-time check
+			rc |= dsum.alloc(2 * (size_t)NB);
+			rc |= dcount.alloc(2);
 			CK(cudaDeviceSynchronize());
 			if (rc) return rc;
 		}
 		if (on) {
-			CK(cudaMemsetAsync(dmax.p, 0, sizeof(unsigned long long) * NB, st));
-			CK(cudaMemsetAsync(dsum.p, 0, sizeof(double) * NB, st));
-			CK(cudaMemsetAsync(dcount.p, 0, sizeof(int), st));
+			CK(cudaMemsetAsync(dmax.p, 0, sizeof(unsigned long long) * 2 * NB, st));
+			CK(cudaMemsetAsync(dsum.p, 0, sizeof(double) * 2 * NB, st));
+			CK(cudaMemsetAsync(dcount.p, 0, 2 * sizeof(int), st));
 		}
 		if ((on != 0) != check_g) {
 			// the captured sweeps follow the setting from the next sweep on
@@ -917,18 +917,18 @@ struct Group : GroupBase, ProfHook {
 		return 0;
 	}
 
-	int g_drift(int c0, int n, double *mx, double *mean, int *count) override
+	int g_drift(int which, int c0, int n, double *mx, double *mean, int *count) override
 	{
-		if (c0 < 0 || n < 0 || c0 + n > C) return DQMC_E_ARG;
+		if (c0 < 0 || n < 0 || c0 + n > C || (which != 0 && which != 1)) return DQMC_E_ARG;
 		if (!check_g || !dmax.p) return DQMC_E_ARG;
 		std::vector<unsigned long long> hm((size_t)2 * n);
 		std::vector<double> hs((size_t)2 * n);
 		int cnt = 0;
-		CK(cudaMemcpyAsync(hm.data(), dmax.p + (size_t)2 * c0, sizeof(unsigned long long) * 2 * n,
+		const size_t o = (size_t)which * NB + (size_t)2 * c0;
+		CK(cudaMemcpyAsync(hm.data(), dmax.p + o, sizeof(unsigned long long) * 2 * n,
 		                   cudaMemcpyDeviceToHost, st));
-		CK(cudaMemcpyAsync(hs.data(), dsum.p + (size_t)2 * c0, sizeof(double) * 2 * n,
-		                   cudaMemcpyDeviceToHost, st));
-		CK(cudaMemcpyAsync(&cnt, dcount.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+		CK(cudaMemcpyAsync(hs.data(), dsum.p + o, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, st));
+		CK(cudaMemcpyAsync(&cnt, dcount.p + which, sizeof(int), cudaMemcpyDeviceToHost, st));
 		CK(cudaStreamSynchronize(st));
 		for (int q = 0; q < n; q++) {
 			double a, b;
@@ -1326,6 +1326,14 @@ struct Group : GroupBase, ProfHook {
 		const size_t NN = (size_t)N * N;
 		int rc = calc_ue_g();
 		if (rc) return rc;
+		if (check_g) {
+			// the equal-time G against the (0, 0) block of G(tau, tau)
+			// (the reference's CHECK_G_UE, dqmc.c:21-22, 405-408); the
+			// stacks are slice-major, so slice 0 of item b is block b
+			k_gdrift<T><<<NB, 256, 0, st>>>(N, G.p, ue.Gtt.p, (long long)NN, dmax.p + NB,
+			                                dsum.p + NB, dcount.p + 1);
+			launch_count++;
+		}
 		// half wrap of all 3 L slices per item (dqmc.c:415-451); the B stack
 		// is free again and holds the intermediate product
 		T *stk[3] = {ue.G0t.p, ue.Gtt.p, ue.Gt0.p};
@@ -1400,7 +1408,8 @@ struct Group : GroupBase, ProfHook {
 				int rc = calc_eq_g((f + 1) % F);
 				if (rc) return rc;
 				if (check_g) {
-					k_gdrift<T><<<NB, 256, 0, st>>>(N, G.p, Gw.p, dmax.p, dsum.p, dcount.p);
+					k_gdrift<T><<<NB, 256, 0, st>>>(N, G.p, Gw.p, (long long)N * N, dmax.p, dsum.p,
+					                                dcount.p);
 					launch_count++;
 				}
 			} else {
@@ -2088,14 +2097,14 @@ struct Lanes : GroupBase {
 		return 0;
 	}
 
-	int g_drift(int first, int n, double *mx, double *mean, int *count) override
+	int g_drift(int which, int first, int n, double *mx, double *mean, int *count) override
 	{
 		if (first != 0 || n != c0s()) return DQMC_E_ARG;
 		CK(cudaStreamSynchronize(st));
 		for (size_t k = 0; k < g.size(); k++) {
 			const size_t a = c0[k], m = c0[k + 1] - c0[k];
-			const int rc = g[k]->g_drift(0, (int)m, mx ? mx + a : nullptr, mean ? mean + a : nullptr,
-			                             count);
+			const int rc = g[k]->g_drift(which, 0, (int)m, mx ? mx + a : nullptr,
+			                             mean ? mean + a : nullptr, count);
 			if (rc) return rc;
 		}
 		return 0;
@@ -2402,7 +2411,14 @@ int dqmc_engine_g_drift(dqmc_engine *e, double *max_abs, double *mean_abs, int *
 {
 	if (!e) return DQMC_E_ARG;
 	const int n = ((Lanes *)e->g)->c0s();
-	return e->g->g_drift(0, n, max_abs, mean_abs, n_recalc);
+	return e->g->g_drift(0, 0, n, max_abs, mean_abs, n_recalc);
+}
+
+int dqmc_engine_g_drift_ue(dqmc_engine *e, double *max_abs, double *mean_abs, int *n_meas)
+{
+	if (!e) return DQMC_E_ARG;
+	const int n = ((Lanes *)e->g)->c0s();
+	return e->g->g_drift(1, 0, n, max_abs, mean_abs, n_meas);
 }
 
 int dqmc_engine_profile_sweep(dqmc_engine *e, int meas_eq, int meas_ue, double *out, int n_class)

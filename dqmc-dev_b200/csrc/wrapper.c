@@ -461,6 +461,10 @@ static void log_drift(FILE *log, dqmc_engine *e, int n)
 		for (int c = 0; c < n; c++)
 			fprintf(log, "chain %d: g - gwrp over %d recalculations:\tmax %.3e\tavg %.3e\n", c, cnt,
 			        mx[c], mx[n + c]);
+	if (dqmc_engine_g_drift_ue(e, mx, mx + n, &cnt) == 0 && cnt > 0)
+		for (int c = 0; c < n; c++)
+			fprintf(log, "chain %d: g - Gtt over %d unequal-time measurements:\tmax %.3e\tavg %.3e\n",
+			        c, cnt, mx[c], mx[n + c]);
 	free(mx);
 }
 

@@ -284,15 +284,18 @@ class Engine:
         the recalculated G with the previous slice's G wrapped once more."""
         _lib.check(self.lib.dqmc_engine_check_g(self.h, int(on)), "dqmc_engine_check_g")
 
-    def g_drift(self):
-        """(max, mean, n_recalc): per chain the largest |G - G_wrapped| and its
-        mean over the entries, over the recalculations checked and both spins
-        (dqmc_engine_g_drift)."""
+    def g_drift(self, unequal_time: bool = False):
+        """(max, mean, n): per chain the largest |G - G_wrapped| and its mean
+        over the entries, over the n recalculations checked and both spins
+        (dqmc_engine_g_drift); with unequal_time, |G - G(0,0)| of the
+        unequal-time path over the n unequal-time measurements
+        (dqmc_engine_g_drift_ue)."""
         n = len(self.sims)
         mx, mean = np.zeros(n), np.zeros(n)
         cnt = C.c_int(0)
-        _lib.check(self.lib.dqmc_engine_g_drift(self.h, mx.ctypes.data, mean.ctypes.data,
-                                                C.addressof(cnt)), "dqmc_engine_g_drift")
+        fn = self.lib.dqmc_engine_g_drift_ue if unequal_time else self.lib.dqmc_engine_g_drift
+        _lib.check(fn(self.h, mx.ctypes.data, mean.ctypes.data, C.addressof(cnt)),
+                   "dqmc_engine_g_drift")
         return mx, mean, int(cnt.value)
 
     def stream(self) -> int:

@@ -232,6 +232,11 @@ void dqmc_batch_destroy(dqmc_batch *b);
  * set and writes the drift to its log. */
 int dqmc_engine_check_g(dqmc_engine *e, int on);
 int dqmc_engine_g_drift(dqmc_engine *e, double *max_abs, double *mean_abs, int *n_recalc);
+/* The same check also compares, at every unequal-time measurement, the
+ * equal-time G with the (0, 0) block of G(tau, tau) that the unequal-time
+ * path computed (the reference's CHECK_G_UE, dqmc.c:21-22, 405-408), before
+ * the half wrap; per chain as above, over the measurements checked. */
+int dqmc_engine_g_drift_ue(dqmc_engine *e, double *max_abs, double *mean_abs, int *n_meas);
 
 /* Replaces the hopping matrices of every chain (the eight exp(-+dt K) and
  * exp(-+dt K / 2) of dqmc_params, both spins) in place, without any device

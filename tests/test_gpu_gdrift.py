@@ -97,3 +97,29 @@ def test_wrapper_logs_the_drift(eng, golden, tmp_path, monkeypatch):
     assert len(lines) == 1, text
     mx = float(lines[0].split("max")[1].split()[0])
     assert 0 < mx < 1e-8
+
+
+@pytest.mark.parametrize("case", ["uneq_small", "cplx_small"])
+def test_unequal_time_check(eng, golden, case):
+    """The (0, 0) block of G(tau, tau) from the unequal-time path against the
+    equal-time G (the reference's CHECK_G_UE): one check per unequal-time
+    measurement, a small positive difference, the sweep unchanged."""
+    from dqmc_b200 import simfile
+    d = simfile.read(os.path.join(golden, case, "sim_0.h5"))
+    a, ga, _ = _run(eng, [d], 99, False)
+    sims = [eng.SimData(d)]
+    e = eng.Engine(sims)
+    e.check_g(True)
+    e.init()
+    e.sweeps(99)
+    e.pull()
+    assert e.errors() == 0
+    mx, mean, cnt = e.g_drift(unequal_time=True)
+    gu, gd, _ = e.g(0)
+    e.close()
+    s = sims[0]
+    assert np.array_equal(a[0].hs, s.hs) and np.array_equal(a[0].ue_acc, s.ue_acc)
+    assert np.array_equal(ga[0][0], gu) and np.array_equal(ga[0][1], gd)
+    assert cnt == s.ue_n > 0
+    assert np.all(np.isfinite(mx)) and np.all(mx > 0) and np.all(mx < 1e-8), mx
+    assert np.all(mean <= mx)
