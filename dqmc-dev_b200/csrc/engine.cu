@@ -1501,14 +1501,18 @@ struct Group : GroupBase, ProfHook {
 				launch_count = 0;
 				int rc = enqueue_sweep(meq, mue);
 				cudaError_t ce = cudaStreamEndCapture(st, &gr);
-				if (rc) return rc;
+				if (rc) {
+					if (ce == cudaSuccess) cudaGraphDestroy(gr);
+					return rc;
+				}
 				if (ce != cudaSuccess) {
 					fprintf(stderr, "dqmc_b200: graph capture failed: %s\n", cudaGetErrorString(ce));
 					return DQMC_E_CUDA;
 				}
 				cudaGraphExec_t ex;
-				CK(cudaGraphInstantiate(&ex, gr, 0));
+				const cudaError_t ie = cudaGraphInstantiate(&ex, gr, 0);
 				cudaGraphDestroy(gr);
+				CK(ie);
 				graphs[kind] = ex;
 				graph_launches[kind] = launch_count;
 				it = graphs.find(kind);
@@ -2200,6 +2204,7 @@ static int batch_sweep(dqmc_batch *b)
 			if (ce == cudaSuccess) ce = cudaStreamWaitEvent(b->st, b->join[i], 0);
 		}
 		const cudaError_t ee = cudaStreamEndCapture(b->st, &gr);
+		if (ee == cudaSuccess && (rc || ce != cudaSuccess)) cudaGraphDestroy(gr);
 		if (rc) return rc;
 		if (ce != cudaSuccess || ee != cudaSuccess) {
 			fprintf(stderr, "dqmc_b200: batch graph capture failed: %s\n",
