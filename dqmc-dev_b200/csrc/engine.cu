@@ -1126,7 +1126,9 @@ struct Group : GroupBase, ProfHook {
 		m.G = Gh.p;
 		m.acc = acc_eq.p; m.acc_stride = eq_size; m.n_sample = n_eq.p;
 		prof_begin(4);
-		k_meas_eqlt<T><<<C, 256, 2 * N * sizeof(T) + 64, st>>>(m);
+		// one warp per class: enough chunks of 8 warps for every class
+		const int chunks = std::max(1, std::min(32, (std::max(p.num_i, p.num_ij) + 7) / 8));
+		k_meas_eqlt<T><<<dim3(C, chunks), 256, 2 * N * sizeof(T) + 64, st>>>(m);
 		launch_count++;
 		if (eq_toggles()) {
 			k_meas_eqlt_x<T><<<C, 256, 0, st>>>(m, gs_eq.p);

@@ -105,8 +105,13 @@ __device__ inline T peierls(const T *p, int idx)
 template <typename T>
 __global__ void k_meas_eqlt(MeasArgs<T> a)
 {
-	const int c = blockIdx.x;
+	// grid (chain, class chunk): each warp sums whole classes, its lanes
+	// striding over the class's entries, reduced by a fixed butterfly (a
+	// deterministic order); the chunks split a chain's classes
+	const int c = blockIdx.x, chunk = blockIdx.y;
 	if (c >= a.nchain) return;
+	const int lane = threadIdx.x & 31, gw = chunk * (blockDim.x >> 5) + (threadIdx.x >> 5);
+	const int ngw = gridDim.y * (blockDim.x >> 5);
 	const int N = a.N;
 	const size_t NN = (size_t)N * N;
 	const T *gu = a.G + (size_t)(2 * c) * NN, *gd = gu + NN;
@@ -120,14 +125,14 @@ __global__ void k_meas_eqlt(MeasArgs<T> a)
 	const T phase = a.phase[c];
 	T *acc = a.acc + (size_t)c * a.acc_stride;
 	const int ni = a.num_i, nij = a.num_ij;
-	if (threadIdx.x == 0) {
+	if (chunk == 0 && threadIdx.x == 0) {
 		acc[0] = acc[0] + phase;
 		a.n_sample[c] += 1;
 	}
 	const T pre_i = phase / (double)a.degen_i;
-	for (int r = threadIdx.x; r < ni; r += blockDim.x) {
+	for (int r = gw; r < ni; r += ngw) {
 		T s0 = zero<T>(), s1 = zero<T>(), s2 = zero<T>(), s3 = zero<T>();
-		for (int q = a.i_off[r]; q < a.i_off[r + 1]; q++) {
+		for (int q = a.i_off[r] + lane; q < a.i_off[r + 1]; q += 32) {
 			const int i = a.i_idx[q];
 			const T guii = du[i], gdii = dd[i];
 			s0 += 2.0 - guii - gdii;
@@ -135,17 +140,23 @@ __global__ void k_meas_eqlt(MeasArgs<T> a)
 			s2 += 1.0 - gdii;
 			s3 += (1.0 - guii) * (1.0 - gdii);
 		}
-		acc[1 + r] += pre_i * s0;
-		acc[1 + ni + r] += pre_i * s1;
-		acc[1 + 2 * ni + r] += pre_i * s2;
-		acc[1 + 3 * ni + r] += pre_i * s3;
+		s0 = warp_sum(s0);
+		s1 = warp_sum(s1);
+		s2 = warp_sum(s2);
+		s3 = warp_sum(s3);
+		if (lane == 0) {
+			acc[1 + r] += pre_i * s0;
+			acc[1 + ni + r] += pre_i * s1;
+			acc[1 + 2 * ni + r] += pre_i * s2;
+			acc[1 + 3 * ni + r] += pre_i * s3;
+		}
 	}
 	const T pre = phase / (double)a.degen_ij;
 	T *a2 = acc + 1 + 4 * ni;
-	for (int r = threadIdx.x; r < nij; r += blockDim.x) {
+	for (int r = gw; r < nij; r += ngw) {
 		T g00 = zero<T>(), g00u = zero<T>(), g00d = zero<T>(), nn = zero<T>();
 		T xx = zero<T>(), zz = zero<T>(), ps = zero<T>(), vv = zero<T>(), vn = zero<T>();
-		for (int q = a.ij_off[r]; q < a.ij_off[r + 1]; q++) {
+		for (int q = a.ij_off[r] + lane; q < a.ij_off[r + 1]; q += 32) {
 			const int e = a.ij_idx[q];
 			const int i = e % N, j = e / N;
 			const double delta = (i == j) ? 1.0 : 0.0;
@@ -169,6 +180,18 @@ __global__ void k_meas_eqlt(MeasArgs<T> a)
 				vn += nun * (1.0 - gdii) + (1.0 - guii) * ndn;
 			}
 		}
+		g00 = warp_sum(g00);
+		g00u = warp_sum(g00u);
+		g00d = warp_sum(g00d);
+		nn = warp_sum(nn);
+		xx = warp_sum(xx);
+		zz = warp_sum(zz);
+		ps = warp_sum(ps);
+		if (a.energy) {
+			vv = warp_sum(vv);
+			vn = warp_sum(vn);
+		}
+		if (lane != 0) continue;
 		if (a.energy) {
 			T *ae = acc + a.lay.energy + a.num_bb + 2 * (size_t)a.num_bs;
 			ae[r] += pre * vv;
