@@ -207,9 +207,10 @@ __global__ void k_meas_eqlt(MeasArgs<T> a)
 	}
 }
 
-// grid (chain, t)
+// grid (chain, t); at most 128 registers a thread for complex (two CTAs per
+// SM instead of one at 132), 64 for real (four CTAs, as the compiler chooses)
 template <typename T>
-__global__ void k_meas_uneqlt(MeasArgs<T> a)
+__global__ void __launch_bounds__(256, is_cplx<T>::value ? 2 : 4) k_meas_uneqlt(MeasArgs<T> a)
 {
 	const int c = blockIdx.x, t = blockIdx.y;
 	if (c >= a.nchain || t >= a.L) return;
