@@ -464,6 +464,93 @@ __global__ void k_yhat(int N, int L, int NB, const T *Y, const double *dv, T *Yh
 	}
 }
 
+// ---------------------------------- checkpointed observable gradients
+//
+// Rows and columns of the space-time Green's function Gst = O^-1 without
+// forming it.  For the chain rotated by s slices (slice l' of the rotated
+// chain is slice (l' + s) mod L) the rotated O is D P O P^T D, D = -1 on
+// the slices that wrapped, so the unequal-time stacks of the rotated chain
+// hold row and column s: Gst(s, l) = sg G0t'[l - s], Gst(l, s) =
+// sg Gt0'[l - s], sg = -1 for l < s.  From O Gst = I and Gst O = I the
+// next row and column follow by one product each:
+//   Gst(m+1, .) = B_m Gst(m, .) + delta_{m+1}
+//   Gst(., m+1) = (Gst(., m) - delta_m) B_m^-1     (negated for m = L-1)
+// which the engine takes across one cluster of n_matmul slices from each
+// rotation s = c n_matmul, the within-cluster propagation of expand_g
+// (greens.c:339-469).
+
+// diagonals of the equal-time blocks G(l, l) from a slice-major stack
+// Gtt[l][item]: out[item][l N + i]
+template <typename T>
+__global__ void k_stack_diag(int N, int L, int NB, const T *Gtt, T *out)
+{
+	const long long NN = (long long)N * N, tot = (long long)NB * L * N;
+	for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot;
+	     q += (long long)gridDim.x * blockDim.x) {
+		const int i = (int)(q % N);
+		const long long bl = q / N;
+		const int l = (int)(bl % L), b = (int)(bl / L);
+		out[q] = Gtt[((size_t)l * NB + b) * NN + (long long)i * (N + 1)];
+	}
+}
+
+// row s (R_b, N x NL, block l at columns l N) and column s (X_b, NL x N,
+// block l at rows l N) of Gst from the rotated chain's stacks
+template <typename T>
+__global__ void k_seed_rowcol(int N, int L, int NB, int s, const T *G0t, const T *Gt0, T *R, T *X)
+{
+	const long long NN = (long long)N * N, NL = (long long)N * L, tot = NN * L * NB;
+	for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot;
+	     q += (long long)gridDim.x * blockDim.x) {
+		const long long e = q % NN, bl = q / NN;
+		const int l = (int)(bl % L), b = (int)(bl / L);
+		const int r = (int)(e % N), c = (int)(e / N);
+		const size_t src = ((size_t)((l - s + L) % L) * NB + b) * NN + e;
+		const double sg = l < s ? -1.0 : 1.0;
+		R[(size_t)b * NN * L + (size_t)l * NN + e] = G0t[src] * sg;
+		X[(size_t)b * NN * L + (size_t)l * N + r + NL * c] = Gt0[src] * sg;
+	}
+}
+
+// A_b[i step] += v for i < N, item stride s: the identity added to one
+// N x N block of a row (step N + 1) or a column (step N L + 1)
+template <typename T>
+__global__ void k_shift_diag(int N, int NB, T *A, long long s, long long step, double v)
+{
+	for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < (long long)N * NB;
+	     q += (long long)gridDim.x * blockDim.x) {
+		T *p = A + (q / N) * s + (q % N) * step;
+		*p = *p + v;
+	}
+}
+
+// Yh_b += s_m diag(d_m) Y_b over nb = k NB matrices, d_m the slice-m field
+// diagonal of item b % NB, s_m = -1 at m = L-1 (the corner's sign)
+template <typename T>
+__global__ void k_yacc(int N, int L, int NB, int nb, int m, const T *Y, const double *dv, T *Yh)
+{
+	const long long NN = (long long)N * N;
+	for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < NN * nb;
+	     q += (long long)gridDim.x * blockDim.x) {
+		const int b = (int)(q / NN) % NB, i = (int)((q % NN) % N);
+		const double f = dv[((size_t)b * L + m) * N + i] * (m == L - 1 ? -1.0 : 1.0);
+		Yh[q] = Yh[q] + Y[q] * f;
+	}
+}
+
+// per-slice vectors rotated by s slices: dst[b][l] = src[b][(l + s) mod L]
+__global__ void k_rotate_slices(int N, int L, int NB, int s, const double *src, double *dst)
+{
+	const long long tot = (long long)NB * L * N;
+	for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot;
+	     q += (long long)gridDim.x * blockDim.x) {
+		const int i = (int)(q % N);
+		const long long bl = q / N;
+		const int l = (int)(bl % L), b = (int)(bl / L);
+		dst[q] = src[((size_t)b * L + (l + s) % L) * N + i];
+	}
+}
+
 // The delayed update runs as one CTA per chain with G in global memory
 // (k_update).  DQMC_UPDATE=cluster selects the form with G held in shared
 // memory (k_update_cl, one CTA per chain and spin in clusters of two) where
@@ -623,6 +710,21 @@ struct Group : GroupBase, ProfHook {
 			wb.release();
 		}
 	} og;
+	// checkpointed observable-gradient work (per item: row and column of
+	// Gst, each N x NL, two rows and four columns), allocated by the first
+	// checkpointed obs_grad; the unequal-time state ue is allocated with it
+	// when the engine measures no unequal-time quantities
+	struct ObsCkptWork {
+		DevBuf<T> R, X, Y, Yh, Cl, dg;
+		DevBuf<double> dv, dvi, w, ones;
+		void release()
+		{
+			DevBuf<T> *b[] = {&R, &X, &Y, &Yh, &Cl, &dg};
+			for (auto *x : b) x->release();
+			DevBuf<double> *d[] = {&dv, &dvi, &w, &ones};
+			for (auto *x : d) x->release();
+		}
+	} ok;
 	DevBuf<T> Pr;                  // pair products C_{(m+1)%F} C_m, F >= 2
 	DevBuf<double> dR, ldet;       // UDT scales; log |det(I + B...B)| per item
 	DevBuf<int> pvt;
@@ -652,6 +754,7 @@ struct Group : GroupBase, ProfHook {
 		                     &bond2s};
 		for (auto *b : ib) b->release();
 		og.release();
+		ok.release();
 		Gw.release(); dmax.release(); dsum.release(); dcount.release();
 		el.release(); del.release(); dv.release(); dvi.release(); dR.release(); ldet.release();
 		rng.release(); rng_ckpt.release(); order.release(); ubuf.release(); err.release();
@@ -1625,15 +1728,170 @@ struct Group : GroupBase, ProfHook {
 	// slices, and for each the matrices Z (per spin) with d obs / d theta =
 	// sum_spin tr[Z D_theta]: Z = sum_m s_m exp(V_m) Y_m exp(-dt K),
 	// Y_m = sum_l Gst(m, l) W_l Gst(l, m+1), Gst = O^-1 the space-time Green's
-	// function (bsofi with one slice per block) and W_l the observable's
-	// weights at slice l.  obs[chain][2], Z[chain][obs][spin][N*N].
+	// function and W_l the observable's weights at slice l.
+	// obs[chain][2], Z[chain][obs][spin][N*N].  The checkpointed form holds
+	// one row and one column of Gst per item at a time (O(N^2 L) memory);
+	// the dense form (DQMC_OBS_GRAD=dense, and the sizes the unequal-time
+	// kernels do not take) inverts the whole N L x N L matrix.
 	int obs_grad(double *obs_out, void *Z_out) override
 	{
-		const size_t NN = (size_t)N * N, NL = (size_t)N * L, NL2 = NL * NL;
 		if (need_init) {
 			const int rc = init();
 			if (rc) return rc;
 		}
+		const char *ev = getenv("DQMC_OBS_GRAD");
+		if ((ev && !strcmp(ev, "dense")) || !UneqState<T>::supported(N, F, L))
+			return obs_grad_dense(obs_out, Z_out);
+		return obs_grad_ckpt(obs_out, Z_out);
+	}
+
+	// <n> and <docc> of every chain from the equal-time diagonals hd
+	// [item][N L] of both spins; w (when given) receives the weights W_l of
+	// observable o (0: n, 1: docc) as [item][N L]
+	void obs_values(const std::vector<T> &hd, double *obs_out, int o, double *w) const
+	{
+		const size_t NL = (size_t)N * L;
+		const double inv = 1.0 / (double)NL;
+		if (obs_out)
+			for (int c = 0; c < C; c++) {
+				double n = 0.0, d2 = 0.0;
+				for (size_t r = 0; r < NL; r++) {
+					const double nu = 1.0 - re(hd[(2 * c) * NL + r]), nd = 1.0 - re(hd[(2 * c + 1) * NL + r]);
+					n += nu + nd;
+					d2 += nu * nd;
+				}
+				obs_out[2 * c] = n * inv;
+				obs_out[2 * c + 1] = d2 * inv;
+			}
+		if (w)
+			for (int b = 0; b < NB; b++)
+				for (size_t r = 0; r < NL; r++)
+					w[b * NL + r] = o == 0 ? -inv : -inv * (1.0 - re(hd[(b ^ 1) * NL + r]));
+	}
+
+	// Z[chain][obs][spin] from the device sums Zb[obs][item]
+	int z_out(const T *Zb, void *Z_out)
+	{
+		const size_t NN = (size_t)N * N;
+		std::vector<T> hz(2 * NB * NN);
+		CK(cudaMemcpyAsync(hz.data(), Zb, sizeof(T) * 2 * NB * NN, cudaMemcpyDeviceToHost, st));
+		CK(cudaStreamSynchronize(st));
+		if (Z_out)
+			for (int c = 0; c < C; c++)
+				for (int o = 0; o < 2; o++)
+					for (int sp = 0; sp < 2; sp++)
+						memcpy((T *)Z_out + ((size_t)(c * 2 + o) * 2 + sp) * NN,
+						       hz.data() + ((size_t)o * NB + 2 * c + sp) * NN, sizeof(T) * NN);
+		return 0;
+	}
+
+	// the checkpointed form: the stabilised unequal-time Green's functions
+	// (calc_ue_g) of the chain rotated to each cluster boundary s = c n_matmul
+	// give Gst(s, .) and Gst(., s); the rows and columns of the cluster's
+	// other slices follow by one B_m or B_m^-1 product each.  Per item: two
+	// rows and four columns of N x N L (the current and next column and the
+	// next column weighted by each observable's W), beside the unequal-time
+	// stacks.  The engine's G, clusters and fields are left as they were.
+	int obs_grad_ckpt(double *obs_out, void *Z_out)
+	{
+		const size_t NN = (size_t)N * N, NL = (size_t)N * L, RS = NN * L;
+		const long long rs = (long long)RS, nn = (long long)NN;
+		ObsCkptWork &k = ok;
+		int rc = 0;
+		if (!k.R.p) {
+			const bool had_ue = ue.G0t.p != nullptr;
+			rc |= k.R.alloc(2 * NB * RS); rc |= k.X.alloc(4 * NB * RS);
+			rc |= k.Y.alloc(2 * NB * NN); rc |= k.Yh.alloc(2 * NB * NN);
+			rc |= k.Cl.alloc((size_t)NB * F * NN); rc |= k.dg.alloc(NB * NL);
+			rc |= k.dv.alloc((size_t)NB * L * N); rc |= k.dvi.alloc((size_t)NB * L * N);
+			rc |= k.w.alloc(2 * NB * NL); rc |= k.ones.alloc(2 * NB * NL);
+			if (!rc && !had_ue && ue.alloc(N, L, F, NB)) {
+				ue.release();
+				rc = DQMC_E_NOMEM;
+			}
+			if (rc) { k.release(); return DQMC_E_NOMEM; }
+			std::vector<double> one1(2 * NB * NL, 1.0);
+			CK(cudaMemcpy(k.ones.p, one1.data(), sizeof(double) * one1.size(), cudaMemcpyHostToDevice));
+			// zeroed on the legacy default stream, which the engine's
+			// non-blocking stream does not wait for
+			CK(cudaDeviceSynchronize());
+		}
+		// the chain as it is: the equal-time diagonals give the observables
+		// and their weights
+		rc = calc_ue_g();
+		if (rc) return rc;
+		k_stack_diag<T><<<grid_for((long long)NB * NL), 256, 0, st>>>(N, L, NB, ue.Gtt.p, k.dg.p);
+		std::vector<T> hd(NB * NL);
+		CK(cudaMemcpyAsync(hd.data(), k.dg.p, sizeof(T) * NB * NL, cudaMemcpyDeviceToHost, st));
+		CK(cudaStreamSynchronize(st));
+		obs_values(hd, obs_out, 0, nullptr);
+		std::vector<double> w(2 * NB * NL);
+		obs_values(hd, nullptr, 0, w.data());
+		obs_values(hd, nullptr, 1, w.data() + NB * NL);
+		CK(cudaMemcpyAsync(k.w.p, w.data(), sizeof(double) * w.size(), cudaMemcpyHostToDevice, st));
+		CK(cudaMemsetAsync(k.Yh.p, 0, sizeof(T) * 2 * NB * NN, st));
+		T *R0 = k.R.p, *R1 = k.R.p + NB * RS;
+		T *Xc = k.X.p, *Xu = k.X.p + NB * RS, *Xw = k.X.p + 2 * NB * RS;
+		const size_t cl_pitch = sizeof(T) * F * NN;
+		for (int c = 0; c < F; c++) {
+			const int s = c * nmul;
+			if (c > 0) {
+				// the rotated chain: fields shifted by s slices, its clusters
+				// the chain's shifted by c (the same products, so no rebuild)
+				k_rotate_slices<<<grid_for((long long)NB * L * N), 256, 0, st>>>(N, L, NB, s, dv.p, k.dv.p);
+				k_rotate_slices<<<grid_for((long long)NB * L * N), 256, 0, st>>>(N, L, NB, s, dvi.p, k.dvi.p);
+				CK(cudaMemcpy2DAsync(k.Cl.p, cl_pitch, Cl.p + (size_t)c * NN, cl_pitch,
+				                     sizeof(T) * (F - c) * NN, NB, cudaMemcpyDeviceToDevice, st));
+				CK(cudaMemcpy2DAsync(k.Cl.p + (size_t)(F - c) * NN, cl_pitch, Cl.p, cl_pitch,
+				                     sizeof(T) * c * NN, NB, cudaMemcpyDeviceToDevice, st));
+				std::swap(dv.p, k.dv.p); std::swap(dvi.p, k.dvi.p); std::swap(Cl.p, k.Cl.p);
+				rc = calc_ue_g();
+				std::swap(dv.p, k.dv.p); std::swap(dvi.p, k.dvi.p); std::swap(Cl.p, k.Cl.p);
+				if (rc) return rc;
+			}
+			k_seed_rowcol<T><<<grid_for((long long)NB * RS), 256, 0, st>>>(N, L, NB, s, ue.G0t.p, ue.Gt0.p,
+			                                                              R0, Xc);
+			for (int j = 0; j < nmul; j++) {
+				const int m = s + j;
+				// slice j of the rotated stacks is slice m
+				const T *Bm = ue.Bs.p + (size_t)j * NB * NN, *iBm = ue.iBs.p + (size_t)j * NB * NN;
+				const T sg = from_re<T>(m == L - 1 ? -1.0 : 1.0);
+				// column m+1, plain and weighted by W_l of both observables
+				k_shift_diag<T><<<grid_for((long long)NB * N), 256, 0, st>>>(N, NB, Xc + (size_t)m * N, rs,
+				                                                            (long long)NL + 1, -1.0);
+				gemm(gargs<T>((int)NL, N, N, NB, Xc, per_item(rs), (int)NL, iBm, per_item(nn), N, Xu,
+				              per_item(rs), (int)NL, sg));
+				GemmArgs<T> gw = gargs<T>((int)NL, N, N, 2 * NB, Xc, Addr{0, rs, NB}, (int)NL, iBm,
+				                          Addr{0, nn, NB}, N, Xw, per_item(rs), (int)NL, sg, zero<T>(), GM_A_DD);
+				gw.d = k.w.p; gw.dinv = k.ones.p; gw.aD = per_item((long long)NL);
+				gemm(gw);
+				// Y_m = Gst(m, .) W Gst(., m+1) of both observables
+				gemm(gargs<T>(N, N, (int)NL, 2 * NB, R0, Addr{0, rs, NB}, N, Xw, per_item(rs), (int)NL, k.Y.p,
+				              per_item(nn), N));
+				k_yacc<T><<<grid_for(2LL * NB * nn), 256, 0, st>>>(N, L, NB, 2 * NB, m, k.Y.p, dv.p, k.Yh.p);
+				// row m+1
+				if (j + 1 < nmul) {
+					gemm(gargs<T>(N, (int)NL, N, NB, Bm, per_item(nn), N, R0, per_item(rs), N, R1, per_item(rs), N));
+					k_shift_diag<T><<<grid_for((long long)NB * N), 256, 0, st>>>(N, NB, R1 + (size_t)(m + 1) * NN,
+					                                                            rs, (long long)N + 1, 1.0);
+					std::swap(R0, R1);
+				}
+				std::swap(Xc, Xu);
+			}
+		}
+		// Z = Yh exp(-dt K) of both observables
+		gemm(gargs<T>(N, N, N, 2 * NB, k.Yh.p, per_item(nn), N, expK.p, per_spin(nn), N, k.Y.p, per_item(nn), N));
+		rc = z_out(k.Y.p, Z_out);
+		if (rc) return rc;
+		CK(cudaGetLastError());
+		watchdog("obs_grad");
+		return sync();
+	}
+
+	// the dense form: Gst from bsofi with one slice per block
+	int obs_grad_dense(double *obs_out, void *Z_out)
+	{
+		const size_t NN = (size_t)N * N, NL = (size_t)N * L, NL2 = NL * NL;
 		// the work buffers are allocated by the first call and kept, so that
 		// repeated evaluations (new hopping, same fields) allocate nothing
 		DevBuf<T> &O = og.O, &Gr = og.Gr, &Qh = og.Qh, &Tw = og.Tw, &Rw = og.Rw, &Yh = og.Yh,
@@ -1643,39 +1901,28 @@ struct Group : GroupBase, ProfHook {
 		if (!O.p) {
 			rc |= O.alloc(NB * NL2); rc |= Gr.alloc(NB * NL2);
 			rc |= Qh.alloc((size_t)NB * std::max(L - 1, 1) * 4 * NN); rc |= Tw.alloc((size_t)NB * L * NN);
-			rc |= Rw.alloc((size_t)NB * NL * 2 * N); rc |= Yh.alloc(NB * NN); rc |= Zb.alloc(NB * NN);
+			rc |= Rw.alloc((size_t)NB * NL * 2 * N); rc |= Yh.alloc(NB * NN); rc |= Zb.alloc(2 * NB * NN);
 			rc |= dg.alloc(NB * NL); rc |= wb.alloc(NB * NL);
 			if (rc) { og.release(); return DQMC_E_NOMEM; }
 			// zeroed on the legacy default stream, which the engine's
 			// non-blocking stream does not wait for
 			CK(cudaDeviceSynchronize());
 		}
-		auto release = [&]() {};
 		CK(cudaMemsetAsync(O.p, 0, sizeof(T) * NB * NL2, st));
 		k_add_diag<T><<<grid_for((long long)NL * NB), 256, 0, st>>>((int)NL, NB, O.p, (long long)NL2);
 		k_build_o<T><<<grid_for((long long)NN * L * NB), 256, 0, st>>>(N, L, NB, expK.p, dv.p, O.p);
 		rc = bsofi(L, O.p, Gr.p, Qh.p, Tw.p, Rw.p);
-		if (rc) { release(); return rc; }
+		if (rc) return rc;
 		k_diag_of<T><<<grid_for((long long)NL * NB), 256, 0, st>>>((long long)NL, NB, Gr.p, dg.p);
 		std::vector<T> hd(NB * NL);
 		CK(cudaMemcpyAsync(hd.data(), dg.p, sizeof(T) * NB * NL, cudaMemcpyDeviceToHost, st));
 		CK(cudaStreamSynchronize(st));
-		const double inv = 1.0 / (double)NL;
-		for (int c = 0; c < C; c++) {
-			double n = 0.0, d2 = 0.0;
-			for (size_t r = 0; r < NL; r++) {
-				const double nu = 1.0 - re(hd[(2 * c) * NL + r]), nd = 1.0 - re(hd[(2 * c + 1) * NL + r]);
-				n += nu + nd;
-				d2 += nu * nd;
-			}
-			if (obs_out) { obs_out[2 * c] = n * inv; obs_out[2 * c + 1] = d2 * inv; }
-		}
+		obs_values(hd, obs_out, 0, nullptr);
 		std::vector<double> w(NB * NL);
 		for (int o = 0; o < 2; o++) {
-			for (int b = 0; b < NB; b++)
-				for (size_t r = 0; r < NL; r++)
-					w[b * NL + r] = o == 0 ? -inv : -inv * (1.0 - re(hd[(b ^ 1) * NL + r]));
-			// stream-ordered after the previous observable's use of wb
+			obs_values(hd, nullptr, o, w.data());
+			// stream-ordered after the previous observable's use of wb; a
+			// copy from pageable memory returns once w has been staged
 			CK(cudaMemcpyAsync(wb.p, w.data(), sizeof(double) * NB * NL, cudaMemcpyHostToDevice, st));
 			k_rowscale<T><<<grid_for((long long)NL2 * NB), 256, 0, st>>>((long long)NL, NB, Gr.p, wb.p, O.p);
 			// Y_m = Gst(m-row) (W Gst)((m+1)-column): m < L-1 at once, then m = L-1
@@ -1688,19 +1935,11 @@ struct Group : GroupBase, ProfHook {
 			              per_item((long long)(L * NN)), N));
 			k_yhat<T><<<grid_for((long long)NN * NB), 256, 0, st>>>(N, L, NB, Tw.p, dv.p, Yh.p);
 			gemm(gargs<T>(N, N, N, NB, Yh.p, per_item((long long)NN), N, expK.p, per_spin((long long)NN), N,
-			              Zb.p, per_item((long long)NN), N));
-			std::vector<T> hz(NB * NN);
-			CK(cudaMemcpyAsync(hz.data(), Zb.p, sizeof(T) * NB * NN, cudaMemcpyDeviceToHost, st));
-			CK(cudaStreamSynchronize(st));
-			if (Z_out)
-				for (int c = 0; c < C; c++)
-					for (int sp = 0; sp < 2; sp++)
-						memcpy((T *)Z_out + ((size_t)(c * 2 + o) * 2 + sp) * NN, hz.data() + (2 * c + sp) * NN,
-						       sizeof(T) * NN);
+			              Zb.p + (size_t)o * NB * NN, per_item((long long)NN), N));
 		}
-		CK(cudaStreamSynchronize(st));
+		rc = z_out(Zb.p, Z_out);
+		if (rc) return rc;
 		CK(cudaGetLastError());
-		release();
 		return sync();
 	}
 

@@ -188,10 +188,17 @@ int dqmc_engine_logdet_grad(dqmc_engine *e, double *logdet, void *S);
  * and Z[chain][obs][spin] (N x N, column-major num) with
  * d obs / d theta = sum_spin tr[Z_spin D_theta], D_theta as for
  * dqmc_engine_logdet_grad.  Z comes from the space-time Green's function
- * O^-1 (bsofi with one slice per block): Z = sum_m s_m exp(V_m) Y_m
- * exp(-dt K), Y_m = sum_l O^-1(m, l) W_l O^-1(l, m+1), s_m = -1 for the
- * corner block m = L-1 and +1 otherwise.  Needs 2 (N L)^2 nums of device
- * memory per chain and spin for the duration of the call. */
+ * O^-1 (src/greens.c:247-264 with one slice per block): Z = sum_m s_m
+ * exp(V_m) Y_m exp(-dt K), Y_m = sum_l O^-1(m, l) W_l O^-1(l, m+1),
+ * s_m = -1 for the corner block m = L-1 and +1 otherwise.  O^-1 is never
+ * formed: at each cluster boundary s = c n_matmul the stabilised
+ * unequal-time Green's functions of the chain rotated by s slices
+ * (src/greens.c:247-494) give row and column s of O^-1, and one B_m or
+ * B_m^-1 product per slice gives the rows and columns in between.  Device
+ * work per chain and spin: 11 N^2 L nums (the unequal-time stacks and the
+ * rows and columns), kept for the next call.  DQMC_OBS_GRAD=dense, and the
+ * sizes the unequal-time kernels do not take (N above 160 real / 112
+ * complex), invert the whole N L x N L matrix instead: 2 (N L)^2 nums. */
 int dqmc_engine_obs_grad(dqmc_engine *e, double *obs, void *Z);
 
 /* Engines advanced together (the ragged batch: one engine per parameter

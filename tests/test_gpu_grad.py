@@ -156,3 +156,62 @@ def test_observables_autograd(grad):
     want = (wts.numpy()[:, :, None] * g).sum((0, 1))
     np.testing.assert_allclose(theta.grad.numpy(), want, rtol=1e-12, atol=1e-14)
     m.close()
+
+
+def test_full_size_observable_gradients(grad):
+    """8x8, L = 40, n_matmul = 8 (five rotations, eight slices propagated from
+    each): <n>, <docc> and their derivatives along t, t', mu and three bond
+    hoppings against the explicit space-time Green's functions."""
+    import fermion_matrix as fm
+    fields = _fields(1, 40, 64, 17)
+    m = grad.SquareModel(8, 8, U=4.0, dt=0.1, L=40, fields=fields, n_matmul=8)
+    theta = np.concatenate([[1.0, -0.2, -0.3], np.zeros(128)])
+    obs, g = m.evaluate_obs(theta)
+    m.close()
+    idx = [0, 1, 2, 3, 40, 130]
+    dK = [m.dK[k] for k in idx]
+    ox, gx = fm.obs_grad(m.K(theta), dK, m.U, m.dt, m.L, fields[0])
+    np.testing.assert_allclose(obs[0], ox, rtol=1e-10)
+    for o in range(2):
+        np.testing.assert_allclose(g[0, o, idx], gx[o], rtol=GRAD_RTOL, atol=GRAD_RTOL * np.abs(gx[o]).max())
+
+
+def test_checkpointed_form_matches_dense_form(grad, monkeypatch):
+    """The rotated unequal-time rows and columns against the whole inverse of
+    the N L x N L matrix (DQMC_OBS_GRAD=dense), three configurations."""
+    fields = _fields(3, 24, 36, 29)
+    rng = np.random.default_rng(5)
+    theta = np.concatenate([[1.0, -0.25, -0.5], 0.05 * rng.standard_normal(72)])
+    m = grad.SquareModel(6, 6, U=6.0, dt=0.1, L=24, fields=fields, n_matmul=6)
+    obs, g = m.evaluate_obs(theta)
+    monkeypatch.setenv("DQMC_OBS_GRAD", "dense")
+    obs_d, g_d = m.evaluate_obs(theta)
+    m.close()
+    np.testing.assert_allclose(obs, obs_d, rtol=1e-11)
+    np.testing.assert_allclose(g, g_d, rtol=1e-9, atol=1e-9 * np.abs(g_d).max())
+
+
+def test_observable_gradients_at_batched_lattice_size(grad):
+    """12x12, beta = 6, dtau = 0.05 (L = 120, N L = 17280), mu = -1: the dense
+    inverse would take 2 (N L)^2 numbers (4.8 GB) per configuration and spin;
+    the checkpointed form stays within a few hundred MB for two
+    configurations, and its derivatives along mu and t match central
+    differences (h = 1e-5)."""
+    import torch
+    fields = _fields(2, 120, 144, 31)
+    theta = np.concatenate([[1.0, 0.0, -1.0], np.zeros(288)])
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    m = grad.SquareModel(12, 12, U=4.0, dt=0.05, L=120, fields=fields, n_matmul=10)
+    obs, g = m.evaluate_obs(theta)
+    used = free0 - torch.cuda.mem_get_info()[0]
+    assert used < 2.0e9, used
+    assert np.all(np.isfinite(g)) and np.all((obs[:, 0] > 0) & (obs[:, 0] < 2))
+    h = 1e-5
+    for k in (2, 0):
+        tp, tm = theta.copy(), theta.copy()
+        tp[k] += h
+        tm[k] -= h
+        fd = (m.evaluate_obs(tp)[0] - m.evaluate_obs(tm)[0]) / (2 * h)
+        np.testing.assert_allclose(g[:, :, k], fd, rtol=FD_RTOL, atol=FD_RTOL * np.abs(g[:, :, k]).max())
+    m.close()
