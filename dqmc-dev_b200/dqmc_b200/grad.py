@@ -26,6 +26,10 @@ double occupancy (evaluate_obs): with Gst = O^-1 the space-time Green's
 function, d <X> = sum_l tr[W_l dGst(l, l)] and dGst = -Gst dO Gst collapse to
 tr[Z D_theta] with Z = sum_m s_m exp(V_m) Y_m exp(-dt K) and
 Y_m = sum_l Gst(m, l) W_l Gst(l, m+1) (W_l the observable's weights).
+The engine never forms Gst: the stabilised unequal-time Green's functions
+of the chain rotated to each cluster boundary s give row and column s of
+Gst, and one B_m or B_m^-1 product per slice gives the rows and columns in
+between, so the device memory is O(N^2 L) per configuration.
 
 LogDet and Observables wrap the log-determinant and (<n>, <docc>) in
 torch.autograd.Functions: the forward runs the engine and keeps the
