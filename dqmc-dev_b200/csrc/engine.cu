@@ -621,6 +621,9 @@ struct GroupBase {
 	virtual int profile(int meq, int mue, double *out, int ncls) = 0;
 	virtual int logdet_grad(double *logdet, void *S) = 0;
 	virtual int obs_grad(double *obs, void *Z) = 0;
+	// one gradient evaluation (0: logdet_grad, 1: obs_grad) with per-launch
+	// events: class sums as profile(), and the kernels it launched
+	virtual int profile_grad(int which, double *out, int ncls, int *launches) = 0;
 	// the eight hopping matrices exp(-+dt K), exp(-+dt K / 2) of both spins
 	virtual int set_hopping(const void *const *m) = 0;
 	// G drift self-check: on / off (resets the counters when turned on), and
@@ -1668,8 +1671,15 @@ struct Group : GroupBase, ProfHook {
 			out[PC_UPDATE * 4 + 2] = 2.0 * cx * a * (2.0 * N * N + 2.0 * N * (kd - 1));
 			out[PC_UPDATE * 4 + 3] = 2.0 * 2.0 * sizeof(T) * (double)N * N * C * L;
 		}
-		// calc_eq_g records nest the gemm records: count gemms inside a
-		// calc_eq_g window only under class 2
+		fold_records(out, ncls);
+		return 0;
+	}
+
+	// add the recorded launches to the class sums out[4 c + k] (the
+	// update's FLOPs and bytes are counted from its accepts instead) and
+	// release the events
+	void fold_records(double *out, int ncls)
+	{
 		for (size_t i = 0; i < precs.size(); i++) {
 			const PRec &r = precs[i];
 			float ms = 0.f;
@@ -1686,7 +1696,25 @@ struct Group : GroupBase, ProfHook {
 		for (cudaEvent_t e : pev) cudaEventDestroy(e);
 		pev.clear();
 		precs.clear();
-		return 0;
+	}
+
+	int profile_grad(int which, double *out, int ncls, int *launches) override
+	{
+		if (need_init) {
+			const int rc = init();
+			if (rc) return rc;
+		}
+		CK(cudaStreamSynchronize(st));
+		for (int i = 0; i < ncls * 4; i++) out[i] = 0.0;
+		profiling = true;
+		precs.clear();
+		launch_count = 0;
+		const int rc = which ? obs_grad(nullptr, nullptr) : logdet_grad(nullptr, nullptr);
+		profiling = false;
+		if (launches) *launches = launch_count;
+		cudaStreamSynchronize(st);
+		fold_records(out, ncls);
+		return rc;
 	}
 
 	// log |det(I + B_{L-1} ... B_0)| of every item and the sums
@@ -1708,6 +1736,7 @@ struct Group : GroupBase, ProfHook {
 		CK(cudaMemsetAsync(Sg.p, 0, sizeof(T) * NB * NN, st));
 		for (int l = 0; l < L; l++) {
 			k_grad_acc<T><<<grid_for((long long)NB * NN), 256, 0, st>>>(N, NB, L, l, G.p, dv.p, dvi.p, Sg.p);
+			launch_count++;
 			if ((l + 1) % nmul == 0) {
 				const int rc = calc_eq_g((l / nmul + 1) % F);
 				if (rc) return rc;
@@ -1821,6 +1850,7 @@ struct Group : GroupBase, ProfHook {
 		rc = calc_ue_g();
 		if (rc) return rc;
 		k_stack_diag<T><<<grid_for((long long)NB * NL), 256, 0, st>>>(N, L, NB, ue.Gtt.p, k.dg.p);
+		launch_count++;
 		std::vector<T> hd(NB * NL);
 		CK(cudaMemcpyAsync(hd.data(), k.dg.p, sizeof(T) * NB * NL, cudaMemcpyDeviceToHost, st));
 		CK(cudaStreamSynchronize(st));
@@ -1840,6 +1870,7 @@ struct Group : GroupBase, ProfHook {
 				// the chain's shifted by c (the same products, so no rebuild)
 				k_rotate_slices<<<grid_for((long long)NB * L * N), 256, 0, st>>>(N, L, NB, s, dv.p, k.dv.p);
 				k_rotate_slices<<<grid_for((long long)NB * L * N), 256, 0, st>>>(N, L, NB, s, dvi.p, k.dvi.p);
+				launch_count += 2;
 				CK(cudaMemcpy2DAsync(k.Cl.p, cl_pitch, Cl.p + (size_t)c * NN, cl_pitch,
 				                     sizeof(T) * (F - c) * NN, NB, cudaMemcpyDeviceToDevice, st));
 				CK(cudaMemcpy2DAsync(k.Cl.p + (size_t)(F - c) * NN, cl_pitch, Cl.p, cl_pitch,
@@ -1851,6 +1882,7 @@ struct Group : GroupBase, ProfHook {
 			}
 			k_seed_rowcol<T><<<grid_for((long long)NB * RS), 256, 0, st>>>(N, L, NB, s, ue.G0t.p, ue.Gt0.p,
 			                                                              R0, Xc);
+			launch_count++;
 			for (int j = 0; j < nmul; j++) {
 				const int m = s + j;
 				// slice j of the rotated stacks is slice m
@@ -1859,6 +1891,7 @@ struct Group : GroupBase, ProfHook {
 				// column m+1, plain and weighted by W_l of both observables
 				k_shift_diag<T><<<grid_for((long long)NB * N), 256, 0, st>>>(N, NB, Xc + (size_t)m * N, rs,
 				                                                            (long long)NL + 1, -1.0);
+				launch_count++;
 				gemm(gargs<T>((int)NL, N, N, NB, Xc, per_item(rs), (int)NL, iBm, per_item(nn), N, Xu,
 				              per_item(rs), (int)NL, sg));
 				GemmArgs<T> gw = gargs<T>((int)NL, N, N, 2 * NB, Xc, Addr{0, rs, NB}, (int)NL, iBm,
@@ -1869,11 +1902,13 @@ struct Group : GroupBase, ProfHook {
 				gemm(gargs<T>(N, N, (int)NL, 2 * NB, R0, Addr{0, rs, NB}, N, Xw, per_item(rs), (int)NL, k.Y.p,
 				              per_item(nn), N));
 				k_yacc<T><<<grid_for(2LL * NB * nn), 256, 0, st>>>(N, L, NB, 2 * NB, m, k.Y.p, dv.p, k.Yh.p);
+				launch_count++;
 				// row m+1
 				if (j + 1 < nmul) {
 					gemm(gargs<T>(N, (int)NL, N, NB, Bm, per_item(nn), N, R0, per_item(rs), N, R1, per_item(rs), N));
 					k_shift_diag<T><<<grid_for((long long)NB * N), 256, 0, st>>>(N, NB, R1 + (size_t)(m + 1) * NN,
 					                                                            rs, (long long)N + 1, 1.0);
+					launch_count++;
 					std::swap(R0, R1);
 				}
 				std::swap(Xc, Xu);
@@ -1911,9 +1946,11 @@ struct Group : GroupBase, ProfHook {
 		CK(cudaMemsetAsync(O.p, 0, sizeof(T) * NB * NL2, st));
 		k_add_diag<T><<<grid_for((long long)NL * NB), 256, 0, st>>>((int)NL, NB, O.p, (long long)NL2);
 		k_build_o<T><<<grid_for((long long)NN * L * NB), 256, 0, st>>>(N, L, NB, expK.p, dv.p, O.p);
+		launch_count += 2;
 		rc = bsofi(L, O.p, Gr.p, Qh.p, Tw.p, Rw.p);
 		if (rc) return rc;
 		k_diag_of<T><<<grid_for((long long)NL * NB), 256, 0, st>>>((long long)NL, NB, Gr.p, dg.p);
+		launch_count++;
 		std::vector<T> hd(NB * NL);
 		CK(cudaMemcpyAsync(hd.data(), dg.p, sizeof(T) * NB * NL, cudaMemcpyDeviceToHost, st));
 		CK(cudaStreamSynchronize(st));
@@ -1925,6 +1962,7 @@ struct Group : GroupBase, ProfHook {
 			// copy from pageable memory returns once w has been staged
 			CK(cudaMemcpyAsync(wb.p, w.data(), sizeof(double) * NB * NL, cudaMemcpyHostToDevice, st));
 			k_rowscale<T><<<grid_for((long long)NL2 * NB), 256, 0, st>>>((long long)NL, NB, Gr.p, wb.p, O.p);
+			launch_count++;
 			// Y_m = Gst(m-row) (W Gst)((m+1)-column): m < L-1 at once, then m = L-1
 			if (L > 1)
 				gemm(gargs<T>(N, N, (int)NL, NB * (L - 1), Gr.p, Addr{(long long)NL2, (long long)N, L - 1},
@@ -1934,6 +1972,7 @@ struct Group : GroupBase, ProfHook {
 			              O.p, per_item((long long)NL2), (int)NL, Tw.p + (size_t)(L - 1) * NN,
 			              per_item((long long)(L * NN)), N));
 			k_yhat<T><<<grid_for((long long)NN * NB), 256, 0, st>>>(N, L, NB, Tw.p, dv.p, Yh.p);
+			launch_count++;
 			gemm(gargs<T>(N, N, N, NB, Yh.p, per_item((long long)NN), N, expK.p, per_spin((long long)NN), N,
 			              Zb.p + (size_t)o * NB * NN, per_item((long long)NN), N));
 		}
@@ -2236,6 +2275,24 @@ struct Lanes : GroupBase {
 			if (rc) return rc;
 			for (int i = 0; i < ncls * 4; i++) out[i] += part[i];
 		}
+		return 0;
+	}
+
+	// class sums and launches over the lanes, each profiled alone
+	int profile_grad(int which, double *out, int ncls, int *launches) override
+	{
+		CK(cudaStreamSynchronize(st));
+		std::vector<double> part(ncls * 4);
+		for (int i = 0; i < ncls * 4; i++) out[i] = 0.0;
+		int total = 0;
+		for (GroupBase *x : g) {
+			int n = 0;
+			const int rc = x->profile_grad(which, part.data(), ncls, &n);
+			if (rc) return rc;
+			for (int i = 0; i < ncls * 4; i++) out[i] += part[i];
+			total += n;
+		}
+		if (launches) *launches = total;
 		return 0;
 	}
 
@@ -2670,6 +2727,12 @@ int dqmc_engine_g_drift_ue(dqmc_engine *e, double *max_abs, double *mean_abs, in
 int dqmc_engine_profile_sweep(dqmc_engine *e, int meas_eq, int meas_ue, double *out, int n_class)
 {
 	return (e && out && n_class > 0) ? e->g->profile(meas_eq, meas_ue, out, n_class) : DQMC_E_ARG;
+}
+
+int dqmc_engine_profile_grad(dqmc_engine *e, int which, double *out, int n_class, int *launches)
+{
+	if (!e || !out || n_class <= 0 || (which != 0 && which != 1)) return DQMC_E_ARG;
+	return e->g->profile_grad(which, out, n_class, launches);
 }
 
 

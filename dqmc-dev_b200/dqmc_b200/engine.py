@@ -249,6 +249,18 @@ class Engine:
         names = self.PROFILE_CLASSES
         return {names[c]: tuple(out[4 * c:4 * c + 4]) for c in range(n_class)}
 
+    def profile_grad(self, which: str, n_class: int = 7):
+        """One gradient evaluation ("logdet" or "obs") with per-launch CUDA
+        events, its results discarded; returns ({class: (ms, launches, flops,
+        bytes)}, kernels launched) (dqmc_engine_profile_grad)."""
+        out = (C.c_double * (4 * n_class))()
+        n = C.c_int(0)
+        _lib.check(self.lib.dqmc_engine_profile_grad(self.h, {"logdet": 0, "obs": 1}[which], out,
+                                                     n_class, C.byref(n)),
+                   "dqmc_engine_profile_grad")
+        names = self.PROFILE_CLASSES
+        return {names[c]: tuple(out[4 * c:4 * c + 4]) for c in range(n_class)}, n.value
+
     def logdet_grad(self):
         """(logdet per chain, S per chain and spin as N x N arrays): see
         dqmc_engine_logdet_grad; fields, RNG and sweep counts stay."""

@@ -169,6 +169,15 @@ int dqmc_engine_launches_per_sweep(dqmc_engine *e, int meas_eq, int meas_ue);
  * of G per slice, chain and spin. */
 int dqmc_engine_profile_sweep(dqmc_engine *e, int meas_eq, int meas_ue, double *out,
 		int n_class);
+/* One gradient evaluation, its results discarded (which = 0:
+ * dqmc_engine_logdet_grad, 1: dqmc_engine_obs_grad), with CUDA events around
+ * the engine's recorded launches; out as for dqmc_engine_profile_sweep
+ * (the gradient paths' GEMMs under class 0, calc_eq_g's QRs and recombine
+ * under 2, 5 and 6, the unequal-time kernels under 3), lanes profiled one
+ * after another.  *launches (may be null) receives the number of kernels
+ * the evaluation launched. */
+int dqmc_engine_profile_grad(dqmc_engine *e, int which, double *out, int n_class,
+		int *launches);
 
 /* Fixed-field log-determinant and its gradient sums (no counterpart in the
  * reference, whose sweep only samples).  For every chain: logdet[chain] =

@@ -215,3 +215,22 @@ def test_observable_gradients_at_batched_lattice_size(grad):
         fd = (m.evaluate_obs(tp)[0] - m.evaluate_obs(tm)[0]) / (2 * h)
         np.testing.assert_allclose(g[:, :, k], fd, rtol=FD_RTOL, atol=FD_RTOL * np.abs(g[:, :, k]).max())
     m.close()
+
+
+def test_gradient_profile_counts_launches_and_keeps_results(grad):
+    """dqmc_engine_profile_grad: one evaluation of each kind with per-launch
+    events; the GEMM class carries time and FLOPs, the launch count is
+    positive, and the evaluations after it give what they gave before."""
+    fields = _fields(2, 8, 16, 37)
+    m = grad.SquareModel(4, 4, U=4.0, dt=0.1, L=8, fields=fields, n_matmul=4)
+    theta = np.concatenate([[1.0, -0.2, -0.3], np.zeros(32)])
+    before = m.evaluate(theta) + m.evaluate_obs(theta)
+    eng = m.engine(m.K(theta))
+    for which in ("logdet", "obs"):
+        prof, n = eng.profile_grad(which)
+        assert n > 0
+        assert prof["gemm"][0] > 0 and prof["gemm"][1] > 0 and prof["gemm"][2] > 0
+    after = m.evaluate(theta) + m.evaluate_obs(theta)
+    m.close()
+    for a, b in zip(before, after):
+        np.testing.assert_allclose(a, b, rtol=1e-13, atol=1e-14)
