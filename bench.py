@@ -412,41 +412,48 @@ def roofline(prof, items, workload, peak, ms_per_step):
                       "note": "counted FLOPs of every class over the timed ms_per_step"}}
 
 
-def e2e_rate(eng, sims, steps, world):
+def e2e_rate(engs, steps, world, sweep_all):
     """chain-sweeps/s through the C ABI with host buffers: per step, every
-    chain's state goes from pinned host memory to the device in one batched
-    call (dqmc_engine_set_chains), one sweep runs, and state plus
-    accumulators come back in one call (dqmc_engine_get_chains); the
-    downloaded state is the next step's input."""
+    engine's chains go from pinned host memory to the device in one batched
+    call each (dqmc_engine_set_chains), one sweep of all of them runs
+    (sweep_all, synchronised), and state plus accumulators come back in one
+    call per engine (dqmc_engine_get_chains); the downloaded state is the
+    next step's input."""
     import torch
-    eng.pull()          # host copies of the state the device now holds
-    n = len(sims)
 
     def pinned(a):
         return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
 
-    el_h, dl_h, rg_h, hs_h = (pinned(a) for a in eng.state_arrays())
-    rg_o, hs_o = pinned(np.zeros_like(rg_h)), pinned(np.zeros_like(hs_h))
-    eqn_o = pinned(np.zeros(n, np.int32))
-    eq_o = pinned(np.zeros((n,) + sims[0].eq_acc.shape, sims[0].eq_acc.dtype))
-    ue = sims[0].p["period_uneqlt"] > 0
-    uen_o = pinned(np.zeros(n, np.int32)) if ue else None
-    ue_o = pinned(np.zeros((n,) + sims[0].ue_acc.shape, sims[0].ue_acc.dtype)) if ue else None
-    sweep = sims[0].sweep
-    h2d = el_h.nbytes + dl_h.nbytes + rg_h.nbytes + hs_h.nbytes
-    d2h = rg_o.nbytes + hs_o.nbytes + eqn_o.nbytes + eq_o.nbytes
-    if ue:
-        d2h += uen_o.nbytes + ue_o.nbytes
+    legs, h2d, d2h, n_all = [], 0, 0, 0
+    for eng in engs:
+        eng.pull()          # host copies of the state the device now holds
+        sims = eng.sims
+        n = len(sims)
+        el_h, dl_h, rg_h, hs_h = (pinned(a) for a in eng.state_arrays())
+        rg_o, hs_o = pinned(np.zeros_like(rg_h)), pinned(np.zeros_like(hs_h))
+        eqn_o = pinned(np.zeros(n, np.int32))
+        eq_o = pinned(np.zeros((n,) + sims[0].eq_acc.shape, sims[0].eq_acc.dtype))
+        ue = sims[0].p["period_uneqlt"] > 0
+        uen_o = pinned(np.zeros(n, np.int32)) if ue else None
+        ue_o = pinned(np.zeros((n,) + sims[0].ue_acc.shape, sims[0].ue_acc.dtype)) if ue else None
+        h2d += el_h.nbytes + dl_h.nbytes + rg_h.nbytes + hs_h.nbytes
+        d2h += rg_o.nbytes + hs_o.nbytes + eqn_o.nbytes + eq_o.nbytes
+        if ue:
+            d2h += uen_o.nbytes + ue_o.nbytes
+        legs.append([eng, el_h, dl_h, rg_h, hs_h, rg_o, hs_o, eqn_o, eq_o, uen_o, ue_o, sims[0].sweep])
+        n_all += n
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(steps):
-        eng.set_chains(el_h, dl_h, rg_h, hs_h, sweep)
-        eng.sweeps(1, sync=True)
-        sweep = eng.get_chains(rg_o, hs_o, eqn_o, eq_o, uen_o, ue_o)
-        rg_h, rg_o = rg_o, rg_h
-        hs_h, hs_o = hs_o, hs_h
+        for lg in legs:
+            lg[0].set_chains(lg[1], lg[2], lg[3], lg[4], lg[11])
+        sweep_all()
+        for lg in legs:
+            lg[11] = lg[0].get_chains(lg[5], lg[6], lg[7], lg[8], lg[9], lg[10])
+            lg[3], lg[5] = lg[5], lg[3]
+            lg[4], lg[6] = lg[6], lg[4]
     t = max_over_ranks((time.perf_counter() - t0) / steps, world)
-    return {"value": n * world / t, "unit": METRIC, "h2d_bytes_per_step": h2d,
+    return {"value": n_all * world / t, "unit": METRIC, "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "steps": steps}
 
 
@@ -495,7 +502,7 @@ def run_engine_workload(args, rank, world, local):
     launches = int(round(args.steps * (kinds[0] * (1 - 1 / pu) + kinds[1] / pu))) if pu > 0 \
         else kinds[0] * args.steps
 
-    e2e = e2e_rate(eng, sims, e2e_steps, world)
+    e2e = e2e_rate([eng], e2e_steps, world, lambda: eng.sweeps(1, sync=True))
     log("e2e done")
     prof, items = profile_one_lane(sims, local, pu)
     log("profile sweep done")
@@ -556,12 +563,14 @@ def _ragged64(n_sweep):
 def run_ragged(args, rank, world, local):
     """The ragged mix as parameter groups (one engine each), every sweep of
     all groups one CUDA graph launch on the batch's stream (dqmc_batch): K
-    sweeps of every chain, timed with CUDA events on that stream."""
+    sweeps of every chain, timed with CUDA events on that stream; then the
+    end-to-end leg (host state up, one batch sweep, host state down) and one
+    profiled eager sweep of every group for the roofline."""
     import torch
     torch.cuda.set_device(local)
     from dqmc_b200 import batch
     from dqmc_b200 import engine
-    dicts, desc = _ragged64(args.warmup + args.steps + 2)
+    dicts, desc = _ragged64(args.warmup + args.steps + args.e2e_steps + 3)
     sims = [engine.SimData(d) for d in dicts]
     log(f"generated {len(sims)} chains")
     rb = batch.RaggedBatch(sims, device=local, autotune=True)
@@ -581,6 +590,14 @@ def run_ragged(args, rank, world, local):
     assert rb.errors() == 0, "device error word set"
     t_max = max_over_ranks(t, world)
     launches = sum(e.launches_per_sweep(True, False) for e in rb.engines) * args.steps
+    e2e = e2e_rate(rb.engines, args.e2e_steps, world, lambda: rb.sweeps(1, sync=True))
+    # class sums of one eager sweep of every group, each launch timed alone
+    profs = [e.profile_sweep(True, False) for e in rb.engines]
+    prof = {k: tuple(sum(p[k][i] for p in profs) for i in range(4)) for k in profs[0]}
+    rl = roofline(prof, 2 * len(sims), args.workload, fp64_peak(), 1e3 * t_max / args.steps) \
+        if rank == 0 else None
+    forms = {str(n): f for n, f in rb.update.items()}
+    lanes = {str(g): n for g, n in rb.lanes.items()}
     rb.close()
     if rank == 0:
         print(json.dumps({
@@ -590,9 +607,10 @@ def run_ragged(args, rank, world, local):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": desc, "chains_per_gpu": len(sims), "groups": len(rb.groups),
                        "delay_rank": {str(k): v for k, v in rb.delay.items()},
+                       "update_form": forms, "lanes": lanes,
                        "timing": "CUDA events on the batch stream around the graph launches "
                                  "(one per sweep of all groups)"},
-            "gpu_launches": launches, "e2e": None, "roofline": None,
+            "gpu_launches": launches, "e2e": e2e, "roofline": rl,
             "clocks": clk.summary(), "cpu_baseline": None,
         }))
 

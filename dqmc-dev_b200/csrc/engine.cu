@@ -624,6 +624,8 @@ struct GroupBase {
 	// one gradient evaluation (0: logdet_grad, 1: obs_grad) with per-launch
 	// events: class sums as profile(), and the kernels it launched
 	virtual int profile_grad(int which, double *out, int ncls, int *launches) = 0;
+	// whether the delayed update holds G on chip (k_update_cl)
+	virtual bool update_on_chip() = 0;
 	// the eight hopping matrices exp(-+dt K), exp(-+dt K / 2) of both spins
 	virtual int set_hopping(const void *const *m) = 0;
 	// G drift self-check: on / off (resets the counters when turned on), and
@@ -1698,6 +1700,8 @@ struct Group : GroupBase, ProfHook {
 		precs.clear();
 	}
 
+	bool update_on_chip() override { return upd_cl; }
+
 	int profile_grad(int which, double *out, int ncls, int *launches) override
 	{
 		if (need_init) {
@@ -2278,6 +2282,8 @@ struct Lanes : GroupBase {
 		return 0;
 	}
 
+	bool update_on_chip() override { return g[0]->update_on_chip(); }
+
 	// class sums and launches over the lanes, each profiled alone
 	int profile_grad(int which, double *out, int ncls, int *launches) override
 	{
@@ -2727,6 +2733,11 @@ int dqmc_engine_g_drift_ue(dqmc_engine *e, double *max_abs, double *mean_abs, in
 int dqmc_engine_profile_sweep(dqmc_engine *e, int meas_eq, int meas_ue, double *out, int n_class)
 {
 	return (e && out && n_class > 0) ? e->g->profile(meas_eq, meas_ue, out, n_class) : DQMC_E_ARG;
+}
+
+int dqmc_engine_update_on_chip(dqmc_engine *e)
+{
+	return e ? (e->g->update_on_chip() ? 1 : 0) : DQMC_E_ARG;
 }
 
 int dqmc_engine_profile_grad(dqmc_engine *e, int which, double *out, int n_class, int *launches)

@@ -17,7 +17,11 @@ timed sweep of a copy of its first group is shortest.  Changing n_delay
 changes results only by rounding; without `autotune` every group keeps its
 files' value.  `autotune` also times every group of 32 chains or more in
 1, 2, 4 and 8 lanes (sub-batches whose launches overlap) and keeps the
-fastest; lanes never change results.
+fastest, and for each lattice size it times the delayed update's two forms
+on the first group of that size: G in device memory with one CTA per chain
+and 8-column flush tiles per warp (k_update), or G on chip in a cluster of
+two CTAs per chain, one per spin (k_update_cl, where one spin's G and panels
+fit in shared memory).  Neither lanes nor the update form change results.
 """
 from __future__ import annotations
 
@@ -51,20 +55,42 @@ def group_key(s: SimData) -> str:
 
 
 def time_sweep(sims: list[SimData], n_delay: int | None, device: int = 0,
-               lanes: int | None = None) -> float:
-    """Seconds of one sweep of copies of `sims` at delay rank n_delay in
-    `lanes` sub-batches (after one untimed sweep that also captures the
-    sweep graph)."""
+               lanes: int | None = None, update: str | None = None, n: int = 1) -> float:
+    """Seconds per sweep of copies of `sims` at delay rank n_delay in
+    `lanes` sub-batches with the given update form, over n sweeps (after
+    one untimed sweep that also captures the sweep graph)."""
     copies = [s.clone() for s in sims]
-    e = Engine(copies, device=device, n_delay=n_delay, lanes=lanes)
+    e = Engine(copies, device=device, n_delay=n_delay, lanes=lanes, update=update)
     try:
         e.init()
         e.sweeps(1, sync=True)
         t0 = time.perf_counter()
-        e.sweeps(1, sync=True)
-        return time.perf_counter() - t0
+        e.sweeps(n, sync=True)
+        return (time.perf_counter() - t0) / n
     finally:
         e.close()
+
+
+def update_forms(sims: list[SimData], n_delay: int | None = None, device: int = 0) -> list[str]:
+    """The delayed-update forms these chains can take: "global" always,
+    "cluster" where the engine places one spin's G and panels on chip."""
+    e = Engine([sims[0].clone()], device=device, n_delay=n_delay, update="cluster")
+    try:
+        return ["global", "cluster"] if e.update_form == "cluster" else ["global"]
+    finally:
+        e.close()
+
+
+def autotune_update(sims: list[SimData], device: int = 0, n_delay: int | None = None,
+                    lanes: int | None = None) -> str:
+    """The delayed-update form ("global" or "cluster") with the shorter
+    timed sweeps of copies of all of `sims`.  Both forms do the same
+    arithmetic in the same order, so the choice only changes the speed."""
+    forms = update_forms(sims, n_delay, device)
+    if len(forms) == 1:
+        return forms[0]
+    t = {f: time_sweep(sims, n_delay, device, lanes=lanes, update=f, n=2) for f in forms}
+    return min(forms, key=lambda f: t[f])
 
 
 def autotune_lanes(sims: list[SimData], candidates=(1, 2, 4, 8), device: int = 0,
@@ -125,8 +151,19 @@ class RaggedBatch:
                 if len(idx) >= 32:
                     self.lanes[g] = autotune_lanes([sims[i] for i in idx], device=device,
                                                    n_delay=self.delay.get(sims[idx[0]].N))
+        # the delayed update's form per lattice size, on the first group of
+        # that size (the form changes only the speed)
+        self.update = {}
+        if autotune:
+            for g, idx in enumerate(self.groups):
+                n = sims[idx[0]].N
+                if n not in self.update:
+                    self.update[n] = autotune_update([sims[i] for i in idx], device=device,
+                                                     n_delay=self.delay.get(n),
+                                                     lanes=self.lanes.get(g))
         self.engines = [Engine([sims[i] for i in idx], device=device,
-                               n_delay=self.delay.get(sims[idx[0]].N), lanes=self.lanes.get(g))
+                               n_delay=self.delay.get(sims[idx[0]].N), lanes=self.lanes.get(g),
+                               update=self.update.get(sims[idx[0]].N))
                         for g, idx in enumerate(self.groups)]
         # one CUDA graph launch per sweep of all groups (dqmc_batch), or
         # (one_graph False) every group's own sweep graph on its own stream

@@ -176,24 +176,37 @@ class Engine:
     """A group of chains with one parameter set, advanced on one GPU."""
 
     def __init__(self, sims: list[SimData], device: int = 0, n_delay: int | None = None,
-                 lanes: int | None = None):
+                 lanes: int | None = None, update: str | None = None):
         """n_delay overrides the sim files' delay rank (the flush period of
         the delayed update); results then differ from the file's setting
         only by rounding.  lanes overrides the number of sub-batches with
-        their own streams (else the engine's rule, or DQMC_LANES); results
-        do not depend on it."""
+        their own streams (else the engine's rule, or DQMC_LANES).  update
+        selects the delayed update's form: "global" (G in device memory, one
+        CTA per chain, k_update) or "cluster" (G on chip in a cluster of two
+        CTAs per chain, one per spin, k_update_cl, where one spin's G and
+        panels fit in shared memory; else "global"), else DQMC_UPDATE
+        decides.  Results depend on neither lanes nor update: every form
+        does the same arithmetic in the same order."""
         if not sims:
             raise ValueError("no chains")
+        env = {}
         if lanes is not None:
-            old = os.environ.get("DQMC_LANES")
-            os.environ["DQMC_LANES"] = str(int(lanes))
+            env["DQMC_LANES"] = str(int(lanes))
+        if update is not None:
+            if update not in ("global", "cluster"):
+                raise ValueError(f"update form {update!r}: 'global' or 'cluster'")
+            env["DQMC_UPDATE"] = update
+        if env:
+            old = {k: os.environ.get(k) for k in env}
+            os.environ.update(env)
             try:
-                self.__init__(sims, device, n_delay, None)
+                self.__init__(sims, device, n_delay)
             finally:
-                if old is None:
-                    del os.environ["DQMC_LANES"]
-                else:
-                    os.environ["DQMC_LANES"] = old
+                for k, v in old.items():
+                    if v is None:
+                        os.environ.pop(k, None)
+                    else:
+                        os.environ[k] = v
             return
         self.lib = _lib.load()
         self.sims = sims
@@ -248,6 +261,14 @@ class Engine:
                                                       n_class), "dqmc_engine_profile_sweep")
         names = self.PROFILE_CLASSES
         return {names[c]: tuple(out[4 * c:4 * c + 4]) for c in range(n_class)}
+
+    @property
+    def update_form(self) -> str:
+        """"cluster" when the delayed update holds G on chip (k_update_cl),
+        else "global" (dqmc_engine_update_on_chip)."""
+        r = self.lib.dqmc_engine_update_on_chip(self.h)
+        _lib.check(min(r, 0), "dqmc_engine_update_on_chip")
+        return "cluster" if r == 1 else "global"
 
     def profile_grad(self, which: str, n_class: int = 7):
         """One gradient evaluation ("logdet" or "obs") with per-launch CUDA

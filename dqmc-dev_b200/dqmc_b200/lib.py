@@ -28,7 +28,8 @@ EXPORTS = [
     "dqmc_engine_get_chain", "dqmc_engine_get_acc", "dqmc_engine_get_g",
     "dqmc_engine_accepts", "dqmc_engine_stream", "dqmc_engine_lanes",
     "dqmc_engine_set_chains", "dqmc_engine_get_chains", "dqmc_engine_launches_per_sweep",
-    "dqmc_engine_profile_sweep", "dqmc_engine_profile_grad", "dqmc_engine_logdet_grad",
+    "dqmc_engine_profile_sweep", "dqmc_engine_profile_grad", "dqmc_engine_update_on_chip",
+    "dqmc_engine_logdet_grad",
     "dqmc_engine_obs_grad",
     "dqmc_engine_set_hopping", "dqmc_engine_check_g", "dqmc_engine_g_drift",
     "dqmc_engine_g_drift_ue",
@@ -104,6 +105,7 @@ def load(path: str | None = None):
         "dqmc_engine_launches_per_sweep": (i, [vp, i, i]),
         "dqmc_engine_profile_sweep": (i, [vp, i, i, C.POINTER(C.c_double), i]),
         "dqmc_engine_profile_grad": (i, [vp, i, C.POINTER(C.c_double), i, vp]),
+        "dqmc_engine_update_on_chip": (i, [vp]),
         "dqmc_engine_logdet_grad": (i, [vp, vp, vp]),
         "dqmc_engine_obs_grad": (i, [vp, vp, vp]),
         "dqmc_engine_set_hopping": (i, [vp] * 9),

@@ -155,6 +155,11 @@ int dqmc_engine_accepts(dqmc_engine *e, int chain, long long *n);
 /* CUDA stream the engine queues on, as an opaque handle (cudaStream_t):
  * every sweep forks from it to the lanes' streams and joins back to it */
 void *dqmc_engine_stream(dqmc_engine *e);
+/* 1 when the engine's delayed update holds G on chip (k_update_cl: a
+ * cluster of two CTAs per chain, one per spin, chosen by DQMC_UPDATE=cluster
+ * at creation where one spin's G and panels fit in shared memory), 0 when G
+ * stays in device memory (k_update); both give bit-identical results */
+int dqmc_engine_update_on_chip(dqmc_engine *e);
 /* number of kernels one sweep of the given kind launches */
 int dqmc_engine_launches_per_sweep(dqmc_engine *e, int meas_eq, int meas_ue);
 /* Runs one sweep eagerly with CUDA events around every launch (it advances

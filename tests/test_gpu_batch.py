@@ -129,6 +129,9 @@ def test_autotuned_ragged_batch_runs(mods):
     rb = batch.RaggedBatch(sims, autotune=True, candidates=(2, 4, 8))
     assert set(rb.delay) == {s.N for s in sims}
     assert all(v in (2, 4, 8) for v in rb.delay.values())
+    assert set(rb.update) == {s.N for s in sims}
+    for g, idx in enumerate(rb.groups):
+        assert rb.engines[g].update_form == rb.update[sims[idx[0]].N]
     rb.init()
     rb.sweeps(2)
     rb.pull()
@@ -272,3 +275,41 @@ def test_batched_state_calls_match_per_chain(mods, monkeypatch):
     assert e1.errors() == 0 and e2.errors() == 0
     e1.close()
     e2.close()
+
+
+def test_update_form_option_and_autotune(mods):
+    """Engine(update=...) selects the delayed update's form (G on chip in a
+    two-CTA cluster, or in device memory), both give bit-identical chains,
+    the tuner returns a form the chains can take, and a lattice whose G does
+    not fit on chip offers only the device-memory form."""
+    batch, engine, gen, simfile = mods
+    from dqmc_b200 import replicas
+    rngs = replicas.chain_streams(9, range(4))
+    base = gen.make_sim(init_rng=rngs[0], Nx=6, Ny=6, U=4.0, dt=0.1, L=20, n_matmul=5,
+                        n_delay=8, period_eqlt=5, n_sweep_warm=0, n_sweep_meas=3)
+    dicts = [base]
+    for r in rngs[1:]:
+        hs, rr = gen.initial_hs(r, 20, 36)
+        d = dict(base)
+        d["state/init_rng"], d["state/rng"], d["state/hs"] = r, rr, hs
+        dicts.append(d)
+    sims = [engine.SimData(d) for d in dicts]
+    assert batch.update_forms(sims) == ["global", "cluster"]
+    runs = []
+    for form in ("global", "cluster"):
+        ss = [s.clone() for s in sims]
+        e = engine.Engine(ss, update=form)
+        assert e.update_form == form
+        e.init()
+        e.sweeps(3)
+        e.pull()
+        assert e.errors() == 0
+        e.close()
+        runs.append(ss)
+    for a, b in zip(*runs):
+        assert np.array_equal(a.hs, b.hs) and np.array_equal(a.rng, b.rng)
+        assert np.array_equal(a.eq_acc, b.eq_acc)
+    assert batch.autotune_update(sims) in ("global", "cluster")
+    big = engine.SimData(gen.make_sim(Nx=16, Ny=16, U=4.0, dt=0.1, L=10, n_matmul=5, n_delay=8,
+                                      period_eqlt=5, n_sweep_warm=0, n_sweep_meas=1))
+    assert batch.update_forms([big]) == ["global"]
