@@ -552,17 +552,21 @@ __global__ void k_rotate_slices(int N, int L, int NB, int s, const double *src, 
 }
 
 // The delayed update runs as one CTA per chain with G in global memory
-// (k_update).  DQMC_UPDATE=cluster selects the form with G held in shared
-// memory (k_update_cl, one CTA per chain and spin in clusters of two) where
-// one spin's G and panels fit there.  That form cuts the latency of a slice
-// by about 30% (12 x 12, 64 chains) but holds a whole SM per CTA and pays a
-// cross-CTA exchange per accept, so at 256 chains it takes 2.8 times the
-// SM-time of k_update and the whole sweep ran 13% slower; it stays opt-in.
-// (read when an engine is created, or a seam called)
-static bool update_cl_requested()
+// (k_update), or with G held in shared memory (k_update_cl, one CTA per
+// chain and spin in clusters of two) where one spin's G and panels fit
+// there.  Both do the same arithmetic in the same order.  The on-chip form
+// cuts the latency of a slice but holds a whole SM per CTA and pays a
+// cross-CTA exchange per accept.  Engines of real scalars with N >= 96 and
+// at most 64 chains take it: the 12 x 12 lattice at L = 120 ran 15% faster
+// from 1 to 64 chains (one chain 15.3 -> 17.7 chain-sweeps/s), 10 x 10 2%
+// faster, while 128 chains of 12 x 12 ran 5% slower and 4 x 4 and 8 x 8
+// 5-8% slower at every count.  DQMC_UPDATE=cluster or =global overrides
+// the rule (read when an engine is created, or a seam called).
+static bool update_cl_wanted(bool cplx, int N, int chains)
 {
 	const char *v = getenv("DQMC_UPDATE");
-	return v && strcmp(v, "cluster") == 0;
+	if (v && *v) return strcmp(v, "cluster") == 0;
+	return !cplx && N >= 96 && chains <= 64;
 }
 
 template <typename T>
@@ -846,7 +850,8 @@ struct Group : GroupBase, ProfHook {
 		return p.meas_gen_suscept || p.meas_chiral || p.meas_energy_corr || p.meas_local_JQ;
 	}
 
-	int create(const dqmc_params &pp, int nchain)
+	// nchain chains of an engine of engine_chains (the update form's rule)
+	int create(const dqmc_params &pp, int nchain, int engine_chains)
 	{
 		p = pp;
 		C = nchain;
@@ -922,7 +927,7 @@ struct Group : GroupBase, ProfHook {
 		kd = p.n_delay < 1 ? 1 : p.n_delay;
 		ldp = (N + 15) / 16 * 16 + 4;
 		while (kd > 1 && update_smem_bytes<T>(N, kd, ldp) > 200 * 1024) kd /= 2;
-		upd_cl = update_cl_requested() && update_cl_fits<T>(N, kd);
+		upd_cl = update_cl_wanted(is_cplx<T>::value, N, engine_chains) && update_cl_fits<T>(N, kd);
 		CK(update_attr<T>(N, kd, update_smem_bytes<T>(N, kd, ldp), upd_cl));
 		CK(cudaDeviceSynchronize());
 		return 0;
@@ -2122,11 +2127,11 @@ struct Lanes : GroupBase {
 			int rc;
 			if (p.cplx) {
 				auto *gg = new Group<zd>();
-				rc = gg->create(p, n);
+				rc = gg->create(p, n, n_chain);
 				x = gg;
 			} else {
 				auto *gg = new Group<double>();
-				rc = gg->create(p, n);
+				rc = gg->create(p, n, n_chain);
 				x = gg;
 			}
 			if (rc) {
@@ -2806,7 +2811,7 @@ static int seam_update(int batch, int N, int n_delay, const double *del, uint64_
 	int kd = n_delay;
 	const int ldp = (N + 15) / 16 * 16 + 4;
 	while (kd > 1 && update_smem_bytes<T>(N, kd, ldp) > 200 * 1024) kd /= 2;
-	const bool cl = update_cl_requested() && update_cl_fits<T>(N, kd);
+	const bool cl = update_cl_wanted(is_cplx<T>::value, N, batch) && update_cl_fits<T>(N, kd);
 	CK(update_attr<T>(N, kd, update_smem_bytes<T>(N, kd, ldp), cl));
 	Scratch<T> sc;
 	uint64_t *ck = sc.template get<uint64_t>((size_t)batch * 17);

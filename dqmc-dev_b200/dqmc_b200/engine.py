@@ -185,8 +185,9 @@ class Engine:
         CTA per chain, k_update) or "cluster" (G on chip in a cluster of two
         CTAs per chain, one per spin, k_update_cl, where one spin's G and
         panels fit in shared memory; else "global"), else DQMC_UPDATE
-        decides.  Results depend on neither lanes nor update: every form
-        does the same arithmetic in the same order."""
+        decides, else the engine's rule (on chip for real scalars with
+        N >= 96 and at most 64 chains).  Results depend on neither lanes nor
+        update: every form does the same arithmetic in the same order."""
         if not sims:
             raise ValueError("no chains")
         env = {}

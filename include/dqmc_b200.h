@@ -156,9 +156,12 @@ int dqmc_engine_accepts(dqmc_engine *e, int chain, long long *n);
  * every sweep forks from it to the lanes' streams and joins back to it */
 void *dqmc_engine_stream(dqmc_engine *e);
 /* 1 when the engine's delayed update holds G on chip (k_update_cl: a
- * cluster of two CTAs per chain, one per spin, chosen by DQMC_UPDATE=cluster
- * at creation where one spin's G and panels fit in shared memory), 0 when G
- * stays in device memory (k_update); both give bit-identical results */
+ * cluster of two CTAs per chain, one per spin), 0 when G stays in device
+ * memory (k_update); both give bit-identical results.  Chosen at creation:
+ * DQMC_UPDATE=cluster or =global when set, else on chip for real scalars
+ * with N >= 96 and at most 64 chains; on chip only where one spin's G and
+ * panels fit in shared memory.  dqmc_gpu_update_delayed applies the same
+ * rule to its batch. */
 int dqmc_engine_update_on_chip(dqmc_engine *e);
 /* number of kernels one sweep of the given kind launches */
 int dqmc_engine_launches_per_sweep(dqmc_engine *e, int meas_eq, int meas_ue);

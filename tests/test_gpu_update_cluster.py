@@ -1,8 +1,8 @@
 """The delayed update with G held in shared memory (k_update_cl, selected
-with DQMC_UPDATE=cluster when the engine is created) against the default
-form (k_update): both do the arithmetic of src/updates.c:7-84 in the same
-order, so fields, RNG states, G and measurements must be bit-identical, and
-the fields equal the oracle's."""
+with DQMC_UPDATE=cluster when the engine is created) against the form with
+G in device memory (k_update, DQMC_UPDATE=global): both do the arithmetic of
+src/updates.c:7-84 in the same order, so fields, RNG states, G and
+measurements must be bit-identical, and the fields equal the oracle's."""
 import os
 import shutil
 
@@ -58,7 +58,7 @@ def _cases(golden):
 def test_cluster_update_bit_identical(eng, golden, case, monkeypatch, tmp_path):
     dicts = _cases(golden)[case]
     n = 2
-    a, ga = _run(eng, dicts, n, monkeypatch, None)
+    a, ga = _run(eng, dicts, n, monkeypatch, "global")
     b, gb = _run(eng, dicts, n, monkeypatch, "cluster")
     for c in range(len(dicts)):
         assert np.array_equal(a[c].hs, b[c].hs)
