@@ -223,16 +223,19 @@ static int eq_gemm(const GemmArgs<T> &g, cudaStream_t st, int *count, ProfHook *
 }
 
 // G = (I + C_{l0-1} ... C_{l0})^-1 over the F clusters (cyclic), grouped two
-// clusters at a time as calc_eq_g(l0, N, F, 2, C, ...) does (greens.c:69-208)
+// clusters at a time as calc_eq_g(l0, N, F, 2, C, ...) does (greens.c:69-208),
+// or one at a time (group 1: calc_eq_g(l0, N, L, 1, B, ...), a QR after every
+// factor, as the reference's CHECK_G_ACC calls it, dqmc.c:283-287)
 template <typename T>
 static int run_calc_eq_g(const EqWork<T> &w, int l0, cudaStream_t st, int *count,
-		ProfHook *ph = nullptr)
+		ProfHook *ph = nullptr, int group = 2)
 {
 	const int N = w.N, F = w.F, NB = w.NB;
 	const size_t NN = (size_t)N * N;
 	const Addr aCl = Addr{w.cl_stride, 0, 1}, aI = Addr{(long long)NN, 0, 1};
 	auto clu = [&](int f) { return w.Cl + (size_t)(((f % F) + F) % F) * NN; };
-	int m = (l0 + 1 + (F - 1) % 2) % F;
+	if (group != 1 && group != 2) return DQMC_E_ARG;
+	int m = (l0 + 1 + (F - 1) % group) % F;
 	QrArgs<T> q;
 	memset(&q, 0, sizeof(q));
 	q.N = N; q.batch = NB; q.err = w.err;
@@ -241,7 +244,8 @@ static int run_calc_eq_g(const EqWork<T> &w, int l0, cudaStream_t st, int *count
 	q.qdet = w.qdet;
 	q.pvt = w.pvt; q.p_stride = N;
 	q.work = w.W; q.w_stride = NN;     // free while a QR runs
-	const int first = (F == 1) ? 1 : ((F - 1) % 2 == 1 ? 2 : 1);
+	// factors in the first group: 1 + (F - 1) % group
+	const int first = 1 + (F - 1) % group;
 	if (first == 2 && w.Pr) {
 		q.X = w.Pr + (size_t)l0 * NN; q.x_stride = w.pr_stride;
 	} else if (first == 2) {
@@ -259,8 +263,10 @@ static int run_calc_eq_g(const EqWork<T> &w, int l0, cudaStream_t st, int *count
 	if (count) (*count)++;
 	T *Tc = w.Tm, *Tn = w.Tm2;
 	while (m != l0) {
-		const int next = (m + 2) % F;
-		if (w.Pr) {
+		const int next = (m + group) % F;
+		if (group == 1) {
+			eq_gemm(gargs<T>(N, N, N, NB, clu(m), aCl, N, w.Qm, aI, N, w.X, aI, N), st, count, ph, w.err);
+		} else if (w.Pr) {
 			eq_gemm(gargs<T>(N, N, N, NB, w.Pr + (size_t)m * NN, Addr{w.pr_stride, 0, 1}, N, w.Qm, aI, N,
 			                 w.X, aI, N), st, count, ph, w.err);
 		} else {
@@ -400,6 +406,21 @@ __global__ void k_grad_acc(int N, int NB, int L, int l, const T *G, const double
 		const T g = G[q];
 		const T x = (i == j) ? one<T>() - g : -g;
 		S[q] = S[q] + x * (dv[o + i] * dvi[o + j]);
+	}
+}
+
+// B_l = exp_K diag(d_l) of every slice and item, item-major (out[item][l],
+// N x N each): the single-slice factors of the accurate recalculation
+// check (the reference's CHECK_G_ACC builds them as calcBu, dqmc.c:29-59)
+template <typename T>
+__global__ void k_build_b_items(int N, int L, int NB, const T *expK, const double *dv, T *out)
+{
+	const long long NN = (long long)N * N, tot = NN * L * NB;
+	for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot;
+	     q += (long long)gridDim.x * blockDim.x) {
+		const long long e = q % NN, bl = q / NN;   // bl = item L + l
+		const int item = (int)(bl / L), c = (int)(e / N);
+		out[q] = expK[(long long)(item & 1) * NN + e] * dv[bl * N + c];
 	}
 }
 
@@ -747,6 +768,13 @@ struct Group : GroupBase, ProfHook {
 	DevBuf<unsigned long long> dmax;   // [item] running max |G - G_wrapped| (bits)
 	DevBuf<double> dsum;               // [item] running sum of mean |G - G_wrapped|
 	DevBuf<int> dcount;                // recalculations checked
+	// the accurate recalculation check (the reference's CHECK_G_ACC,
+	// dqmc.c:18-19, 283-287, 345-349): at every recalculation G again from
+	// the L single-slice factors with a QR after each, against the G of the
+	// cluster chain; the third slot of dmax / dsum / dcount
+	bool check_acc = false;
+	DevBuf<T> Bacc, Gacc, phacc;       // [item][L] factors, [item] G and phase
+	DevBuf<double> ldacc;              // [item] log |det| of that recalculation
 
 	~Group() override
 	{
@@ -765,6 +793,7 @@ struct Group : GroupBase, ProfHook {
 		og.release();
 		ok.release();
 		Gw.release(); dmax.release(); dsum.release(); dcount.release();
+		Bacc.release(); Gacc.release(); phacc.release(); ldacc.release();
 		el.release(); del.release(); dv.release(); dvi.release(); dR.release(); ldet.release();
 		rng.release(); rng_ckpt.release(); order.release(); ubuf.release(); err.release();
 		ue.release();
@@ -1002,38 +1031,76 @@ struct Group : GroupBase, ProfHook {
 		return 0;
 	}
 
+	// on: 0 off; else the wrap and unequal-time checks, and with bit 1 the
+	// accurate recalculation check too
 	int set_check_g(int on) override
 	{
 		CK(cudaStreamSynchronize(st));
+		const bool acc = on != 0 && (on & 2) != 0;
 		if (on && !Gw.p) {
 			CK(cudaDeviceSynchronize());   // the allocations' zeroing runs on the default stream
 			int rc = Gw.alloc((size_t)NB * N * N);
-			rc |= dmax.alloc(2 * (size_t)NB);     // [0, NB): wrap check, [NB, 2 NB): unequal-time check
-			rc |= dsum.alloc(2 * (size_t)NB);
-			rc |= dcount.alloc(2);
+			// [0, NB): wrap check, [NB, 2 NB): unequal-time, [2 NB, 3 NB): accurate
+			rc |= dmax.alloc(3 * (size_t)NB);
+			rc |= dsum.alloc(3 * (size_t)NB);
+			rc |= dcount.alloc(3);
 			CK(cudaDeviceSynchronize());
 			if (rc) return rc;
 		}
-		if (on) {
-			CK(cudaMemsetAsync(dmax.p, 0, sizeof(unsigned long long) * 2 * NB, st));
-			CK(cudaMemsetAsync(dsum.p, 0, sizeof(double) * 2 * NB, st));
-			CK(cudaMemsetAsync(dcount.p, 0, 2 * sizeof(int), st));
+		if (acc && !Bacc.p) {
+			CK(cudaDeviceSynchronize());
+			int rc = Bacc.alloc((size_t)NB * L * N * N);
+			rc |= Gacc.alloc((size_t)NB * N * N);
+			rc |= phacc.alloc((size_t)NB);
+			rc |= ldacc.alloc((size_t)NB);
+			CK(cudaDeviceSynchronize());
+			if (rc) {
+				Bacc.release(); Gacc.release(); phacc.release(); ldacc.release();
+				return DQMC_E_NOMEM;
+			}
 		}
-		if ((on != 0) != check_g) {
+		if (on) {
+			CK(cudaMemsetAsync(dmax.p, 0, sizeof(unsigned long long) * 3 * NB, st));
+			CK(cudaMemsetAsync(dsum.p, 0, sizeof(double) * 3 * NB, st));
+			CK(cudaMemsetAsync(dcount.p, 0, 3 * sizeof(int), st));
+		}
+		if ((on != 0) != check_g || acc != check_acc) {
 			// the captured sweeps follow the setting from the next sweep on
 			for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
 			graphs.clear();
 			graph_launches.clear();
 			check_g = on != 0;
+			check_acc = acc;
 		}
 		CK(cudaStreamSynchronize(st));
 		return 0;
 	}
 
+	// G at slice l0 from the L single-slice factors, a QR after each
+	// (calc_eq_g(l0, N, L, 1, B, ...), dqmc.c:283-287), into Gacc; the
+	// cluster chain's scratch is free again once its G is done
+	int calc_eq_g_acc(int l0)
+	{
+		const size_t NN = (size_t)N * N;
+		k_build_b_items<T><<<grid_for((long long)NB * L * NN), 256, 0, st>>>(N, L, NB, expK.p, dv.p,
+		                                                                   Bacc.p);
+		launch_count++;
+		EqWork<T> w = eq_work();
+		w.F = L;
+		w.Cl = Bacc.p; w.cl_stride = (long long)L * NN;
+		w.Pr = nullptr;
+		w.G = Gacc.p; w.g_stride = (long long)NN;
+		w.phi = phacc.p;
+		w.logdet = ldacc.p;
+		const int rc = run_calc_eq_g<T>(w, l0, st, &launch_count, nullptr, 1);
+		watchdog("calc_eq_g (accurate check)");
+		return rc;
+	}
+
 	int g_drift(int which, int c0, int n, double *mx, double *mean, int *count) override
 	{
-		if (c0 < 0 || n < 0 || c0 + n > C || (which != 0 && which != 1)) return DQMC_E_ARG;
-		if (!check_g || !dmax.p) return DQMC_E_ARG;
+		if (c0 < 0 || n < 0 || c0 + n > C || which < 0 || which > 2) return DQMC_E_ARG;
+		if (!check_g || !dmax.p || (which == 2 && !check_acc)) return DQMC_E_ARG;
 		std::vector<unsigned long long> hm((size_t)2 * n);
 		std::vector<double> hs((size_t)2 * n);
 		int cnt = 0;
@@ -1525,6 +1592,13 @@ struct Group : GroupBase, ProfHook {
 				if (check_g) {
 					k_gdrift<T><<<NB, 256, 0, st>>>(N, G.p, Gw.p, (long long)N * N, dmax.p, dsum.p,
 					                                dcount.p);
+					launch_count++;
+				}
+				if (check_acc) {
+					rc = calc_eq_g_acc((l + 1) % L);
+					if (rc) return rc;
+					k_gdrift<T><<<NB, 256, 0, st>>>(N, G.p, Gacc.p, (long long)N * N, dmax.p + 2 * NB,
+					                                dsum.p + 2 * NB, dcount.p + 2);
 					launch_count++;
 				}
 			} else {
@@ -2733,6 +2807,13 @@ int dqmc_engine_g_drift_ue(dqmc_engine *e, double *max_abs, double *mean_abs, in
 	if (!e) return DQMC_E_ARG;
 	const int n = ((Lanes *)e->g)->c0s();
 	return e->g->g_drift(1, 0, n, max_abs, mean_abs, n_meas);
+}
+
+int dqmc_engine_g_drift_acc(dqmc_engine *e, double *max_abs, double *mean_abs, int *n_recalc)
+{
+	if (!e) return DQMC_E_ARG;
+	const int n = ((Lanes *)e->g)->c0s();
+	return e->g->g_drift(2, 0, n, max_abs, mean_abs, n_recalc);
 }
 
 int dqmc_engine_profile_sweep(dqmc_engine *e, int meas_eq, int meas_ue, double *out, int n_class)

@@ -435,9 +435,10 @@ static int engine_from(struct sim **sims, int n, dqmc_engine **out)
 {
 	int rc = dqmc_engine_create(&sims[0]->p, n, 0, out);
 	if (rc) return rc;
-	/* the runtime form of the reference's CHECK_G_WRP (dqmc.c:15-16) */
+	/* the runtime forms of the reference's CHECK_G_WRP and CHECK_G_UE
+	 * (dqmc.c:15-22), and with DQMC_CHECK_G=acc also CHECK_G_ACC */
 	if (getenv("DQMC_CHECK_G")) {
-		rc = dqmc_engine_check_g(*out, 1);
+		rc = dqmc_engine_check_g(*out, strcmp(getenv("DQMC_CHECK_G"), "acc") == 0 ? 3 : 1);
 		if (rc) return rc;
 	}
 	for (int c = 0; c < n; c++) {
@@ -465,6 +466,10 @@ static void log_drift(FILE *log, dqmc_engine *e, int n)
 		for (int c = 0; c < n; c++)
 			fprintf(log, "chain %d: g - Gtt over %d unequal-time measurements:\tmax %.3e\tavg %.3e\n",
 			        c, cnt, mx[c], mx[n + c]);
+	if (dqmc_engine_g_drift_acc(e, mx, mx + n, &cnt) == 0)
+		for (int c = 0; c < n; c++)
+			fprintf(log, "chain %d: g - gacc over %d recalculations:\tmax %.3e\tavg %.3e\n", c, cnt,
+			        mx[c], mx[n + c]);
 	free(mx);
 }
 

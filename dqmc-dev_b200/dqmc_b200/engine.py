@@ -312,22 +312,27 @@ class Engine:
         _lib.check(self.lib.dqmc_engine_set_hopping(self.h, *[c.ctypes.data for c in col]),
                    "dqmc_engine_set_hopping")
 
-    def check_g(self, on: bool = True):
+    def check_g(self, on: bool = True, accurate: bool = False):
         """G drift self-check on or off (dqmc_engine_check_g; the runtime form
-        of the reference's CHECK_G_WRP): every recalculation also compares
-        the recalculated G with the previous slice's G wrapped once more."""
-        _lib.check(self.lib.dqmc_engine_check_g(self.h, int(on)), "dqmc_engine_check_g")
+        of the reference's CHECK_G_WRP and CHECK_G_UE): every recalculation
+        also compares the recalculated G with the previous slice's G wrapped
+        once more.  With accurate, every recalculation also computes G from
+        the L single-slice factors with a QR after each (CHECK_G_ACC)."""
+        flag = (1 | (2 if accurate else 0)) if on else 0
+        _lib.check(self.lib.dqmc_engine_check_g(self.h, flag), "dqmc_engine_check_g")
 
-    def g_drift(self, unequal_time: bool = False):
+    def g_drift(self, unequal_time: bool = False, accurate: bool = False):
         """(max, mean, n): per chain the largest |G - G_wrapped| and its mean
         over the entries, over the n recalculations checked and both spins
         (dqmc_engine_g_drift); with unequal_time, |G - G(0,0)| of the
         unequal-time path over the n unequal-time measurements
-        (dqmc_engine_g_drift_ue)."""
+        (dqmc_engine_g_drift_ue); with accurate, |G - G_acc| of the
+        single-slice recalculation (dqmc_engine_g_drift_acc)."""
         n = len(self.sims)
         mx, mean = np.zeros(n), np.zeros(n)
         cnt = C.c_int(0)
-        fn = self.lib.dqmc_engine_g_drift_ue if unequal_time else self.lib.dqmc_engine_g_drift
+        fn = (self.lib.dqmc_engine_g_drift_acc if accurate else
+              self.lib.dqmc_engine_g_drift_ue if unequal_time else self.lib.dqmc_engine_g_drift)
         _lib.check(fn(self.h, mx.ctypes.data, mean.ctypes.data, C.addressof(cnt)),
                    "dqmc_engine_g_drift")
         return mx, mean, int(cnt.value)

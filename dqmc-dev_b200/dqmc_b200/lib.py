@@ -32,7 +32,7 @@ EXPORTS = [
     "dqmc_engine_logdet_grad",
     "dqmc_engine_obs_grad",
     "dqmc_engine_set_hopping", "dqmc_engine_check_g", "dqmc_engine_g_drift",
-    "dqmc_engine_g_drift_ue",
+    "dqmc_engine_g_drift_ue", "dqmc_engine_g_drift_acc",
     "dqmc_batch_create", "dqmc_batch_sweeps", "dqmc_batch_stream", "dqmc_batch_destroy",
     "dqmc_gpu_gemm", "dqmc_gpu_calc_eq_g", "dqmc_gpu_update_delayed", "dqmc_gpu_mul_seq",
     "dqmc_gpu_calc_eq_g_noalloc",
@@ -112,6 +112,7 @@ def load(path: str | None = None):
         "dqmc_engine_check_g": (i, [vp, i]),
         "dqmc_engine_g_drift": (i, [vp, vp, vp, vp]),
         "dqmc_engine_g_drift_ue": (i, [vp, vp, vp, vp]),
+        "dqmc_engine_g_drift_acc": (i, [vp, vp, vp, vp]),
         "dqmc_batch_create": (i, [vp, i, vp]),
         "dqmc_batch_sweeps": (i, [vp, i, i]),
         "dqmc_batch_stream": (vp, [vp]),

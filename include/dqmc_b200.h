@@ -248,6 +248,8 @@ void dqmc_batch_destroy(dqmc_batch *b);
  * dqmc_engine_check_g turns it on (and clears the counters) or off; it costs
  * one wrap and one N x N comparison per recalculation and N x N nums of
  * device memory per chain and spin.  The results leave the sweep unchanged.
+ * With bit 1 of `on` set (on = 3) the accurate recalculation check runs
+ * too (dqmc_engine_g_drift_acc).
  * dqmc_engine_g_drift gives per chain (arrays of n_chain) the largest
  * |G - G_wrapped| over the checked recalculations and both spins, and its
  * mean over the entries averaged over the recalculations and spins, and the
@@ -261,6 +263,15 @@ int dqmc_engine_g_drift(dqmc_engine *e, double *max_abs, double *mean_abs, int *
  * path computed (the reference's CHECK_G_UE, dqmc.c:21-22, 405-408), before
  * the half wrap; per chain as above, over the measurements checked. */
 int dqmc_engine_g_drift_ue(dqmc_engine *e, double *max_abs, double *mean_abs, int *n_meas);
+/* The accurate recalculation check, the runtime form of the reference's
+ * compile-time CHECK_G_ACC (src/dqmc.c:18-19, 283-287, 345-349): at every
+ * recalculation G is computed again from the L single-slice factors B_l
+ * with a QR after each one (calc_eq_g(l, N, L, 1, B, ...)) and compared
+ * with the G of the cluster chain.  It costs a calc_eq_g of L factors per
+ * recalculation and L N x N nums of device memory per chain and spin, and
+ * leaves the sweep unchanged; per chain as above, over the recalculations
+ * checked, DQMC_E_ARG unless the check was turned on with bit 1. */
+int dqmc_engine_g_drift_acc(dqmc_engine *e, double *max_abs, double *mean_abs, int *n_recalc);
 
 /* Replaces the hopping matrices of every chain (the eight exp(-+dt K) and
  * exp(-+dt K / 2) of dqmc_params, both spins) in place, without any device

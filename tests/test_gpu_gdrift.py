@@ -123,3 +123,58 @@ def test_unequal_time_check(eng, golden, case):
     assert cnt == s.ue_n > 0
     assert np.all(np.isfinite(mx)) and np.all(mx > 0) and np.all(mx < 1e-8), mx
     assert np.all(mean <= mx)
+
+
+@pytest.mark.parametrize("case", ["c1_small", "cplx_small", "headline"])
+def test_accurate_recalculation_check(eng, golden, case):
+    """G from the L single-slice factors with a QR after each (the
+    reference's CHECK_G_ACC, calc_eq_g(l, N, L, 1, B, ...)) against the G of
+    the cluster chain at every recalculation: one check per recalculation
+    beside the wrap check, a small positive difference, the sweep
+    unchanged (a golden case, a complex one with flux, and two chains of the
+    12x12, L = 120 benchmark shape)."""
+    from dqmc_b200 import simfile
+    if case == "headline":
+        dicts, sweeps = _headline_dicts(2), 2
+    else:
+        dicts, sweeps = [simfile.read(os.path.join(golden, case, "sim_0.h5"))], 3
+    a, ga, _ = _run(eng, dicts, sweeps, False)
+    sims = [eng.SimData(d) for d in dicts]
+    e = eng.Engine(sims)
+    e.check_g(True, accurate=True)
+    e.init()
+    e.sweeps(sweeps)
+    e.pull()
+    assert e.errors() == 0
+    mx, mean, cnt = e.g_drift(accurate=True)
+    _, _, cnt_w = e.g_drift()
+    gs = [e.g(c) for c in range(len(sims))]
+    e.close()
+    for sa, sb in zip(a, sims):
+        assert np.array_equal(sa.hs, sb.hs) and np.array_equal(sa.rng, sb.rng)
+        assert np.array_equal(sa.eq_acc, sb.eq_acc)
+    for x, y in zip(ga, gs):
+        assert np.array_equal(x[0], y[0]) and np.array_equal(x[1], y[1])
+    F = sims[0].p["L"] // sims[0].p["n_matmul"]
+    done = sims[0].sweep - int(np.asarray(dicts[0]["state/sweep"]).reshape(-1)[0])
+    assert done > 0 and cnt == cnt_w == F * done
+    bound = 1e-7 if case == "headline" else 1e-8
+    assert np.all(np.isfinite(mx)) and np.all(mx > 0) and np.all(mx < bound), mx
+    assert np.all(mean <= mx)
+
+
+def test_wrapper_logs_the_accurate_check(eng, golden, tmp_path, monkeypatch):
+    from dqmc_b200 import lib
+    for f in ("sim_0.h5", "sim.h5.params"):
+        shutil.copy(os.path.join(golden, "c1_small", f), tmp_path)
+    monkeypatch.setenv("DQMC_CHECK_G", "acc")
+    log = tmp_path / "log"
+    rc = lib.load().dqmc_wrapper(str(tmp_path / "sim_0.h5").encode(), str(log).encode(), 0,
+                                 False, True)
+    text = open(log).read()
+    assert rc == 0, text
+    for key in ("g - gwrp", "g - gacc"):
+        lines = [ln for ln in text.splitlines() if key in ln]
+        assert len(lines) == 1, text
+        mx = float(lines[0].split("max")[1].split()[0])
+        assert 0 < mx < 1e-8
