@@ -86,6 +86,7 @@ class SquareModel:
         dK[2] -= np.eye(N)
         self.dK = dK
         self._eng = None
+        self._K = None
         self._dK_dev = None
 
     def K(self, theta: np.ndarray) -> np.ndarray:
@@ -128,18 +129,25 @@ class SquareModel:
     def engine(self, K: np.ndarray) -> Engine:
         """The model's engine with hopping K: created (and its device buffers
         allocated) by the first evaluation, then only its hopping matrices
-        change (dqmc_engine_set_hopping)."""
+        change (dqmc_engine_set_hopping).  The same K as the previous call
+        keeps everything: neither gradient evaluation changes the fields,
+        the clusters or the hopping, so its successor reads the same state
+        that a re-initialisation would rebuild."""
+        if self._eng is not None and self._K is not None and np.array_equal(K, self._K):
+            return self._eng
         mats = self._hopping(K)
         if self._eng is None:
             self._eng = Engine(self._sims(K, mats), device=self.device)
         else:
             self._eng.set_hopping(mats)
+        self._K = np.array(K, copy=True)
         return self._eng
 
     def close(self):
         if self._eng is not None:
             self._eng.close()
             self._eng = None
+        self._K = None
 
     def __del__(self):
         try:
