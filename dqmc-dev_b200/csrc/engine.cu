@@ -741,7 +741,7 @@ struct Group : GroupBase, ProfHook {
 		}
 	} og;
 	// checkpointed observable-gradient work (per item: row and column of
-	// Gst, each N x NL, two rows and four columns), allocated by the first
+	// Gst, each N x NL, two rows and three columns), allocated by the first
 	// checkpointed obs_grad; the unequal-time state ue is allocated with it
 	// when the engine measures no unequal-time quantities
 	struct ObsCkptWork {
@@ -1900,10 +1900,12 @@ struct Group : GroupBase, ProfHook {
 	// the checkpointed form: the stabilised unequal-time Green's functions
 	// (calc_ue_g) of the chain rotated to each cluster boundary s = c n_matmul
 	// give Gst(s, .) and Gst(., s); the rows and columns of the cluster's
-	// other slices follow by one B_m or B_m^-1 product each.  Per item: two
-	// rows and four columns of N x N L (the current and next column and the
-	// next column weighted by each observable's W), beside the unequal-time
-	// stacks.  The engine's G, clusters and fields are left as they were.
+	// other slices follow by one B_m or B_m^-1 product each.  W_l of <n> is
+	// -1/(N L) I and of <docc> -1/(N L) diag(1 - n_{-sigma}), so both Y_m take
+	// alpha = -1/(N L) and only the <docc> column is weighted.  Per item: two
+	// rows and three columns of N x N L (the current and next column and the
+	// next column weighted for <docc>), beside the unequal-time stacks.  The
+	// engine's G, clusters and fields are left as they were.
 	int obs_grad_ckpt(double *obs_out, void *Z_out)
 	{
 		const size_t NN = (size_t)N * N, NL = (size_t)N * L, RS = NN * L;
@@ -1912,17 +1914,17 @@ struct Group : GroupBase, ProfHook {
 		int rc = 0;
 		if (!k.R.p) {
 			const bool had_ue = ue.G0t.p != nullptr;
-			rc |= k.R.alloc(2 * NB * RS); rc |= k.X.alloc(4 * NB * RS);
+			rc |= k.R.alloc(2 * NB * RS); rc |= k.X.alloc(3 * NB * RS);
 			rc |= k.Y.alloc(2 * NB * NN); rc |= k.Yh.alloc(2 * NB * NN);
 			rc |= k.Cl.alloc((size_t)NB * F * NN); rc |= k.dg.alloc(NB * NL);
 			rc |= k.dv.alloc((size_t)NB * L * N); rc |= k.dvi.alloc((size_t)NB * L * N);
-			rc |= k.w.alloc(2 * NB * NL); rc |= k.ones.alloc(2 * NB * NL);
+			rc |= k.w.alloc(NB * NL); rc |= k.ones.alloc(NB * NL);
 			if (!rc && !had_ue && ue.alloc(N, L, F, NB)) {
 				ue.release();
 				rc = DQMC_E_NOMEM;
 			}
 			if (rc) { k.release(); return DQMC_E_NOMEM; }
-			std::vector<double> one1(2 * NB * NL, 1.0);
+			std::vector<double> one1(NB * NL, 1.0);
 			CK(cudaMemcpy(k.ones.p, one1.data(), sizeof(double) * one1.size(), cudaMemcpyHostToDevice));
 			// zeroed on the legacy default stream, which the engine's
 			// non-blocking stream does not wait for
@@ -1938,10 +1940,12 @@ struct Group : GroupBase, ProfHook {
 		CK(cudaMemcpyAsync(hd.data(), k.dg.p, sizeof(T) * NB * NL, cudaMemcpyDeviceToHost, st));
 		CK(cudaStreamSynchronize(st));
 		obs_values(hd, obs_out, 0, nullptr);
-		std::vector<double> w(2 * NB * NL);
-		obs_values(hd, nullptr, 0, w.data());
-		obs_values(hd, nullptr, 1, w.data() + NB * NL);
+		// the <docc> weights without their -1/(N L): 1 - n of the other spin
+		std::vector<double> w(NB * NL);
+		for (int b = 0; b < NB; b++)
+			for (size_t r = 0; r < NL; r++) w[b * NL + r] = 1.0 - re(hd[(b ^ 1) * NL + r]);
 		CK(cudaMemcpyAsync(k.w.p, w.data(), sizeof(double) * w.size(), cudaMemcpyHostToDevice, st));
+		const T a_obs = from_re<T>(-1.0 / (double)NL);
 		CK(cudaMemsetAsync(k.Yh.p, 0, sizeof(T) * 2 * NB * NN, st));
 		T *R0 = k.R.p, *R1 = k.R.p + NB * RS;
 		T *Xc = k.X.p, *Xu = k.X.p + NB * RS, *Xw = k.X.p + 2 * NB * RS;
@@ -1971,19 +1975,20 @@ struct Group : GroupBase, ProfHook {
 				// slice j of the rotated stacks is slice m
 				const T *Bm = ue.Bs.p + (size_t)j * NB * NN, *iBm = ue.iBs.p + (size_t)j * NB * NN;
 				const T sg = from_re<T>(m == L - 1 ? -1.0 : 1.0);
-				// column m+1, plain and weighted by W_l of both observables
+				// column m+1, plain and weighted for <docc>
 				k_shift_diag<T><<<grid_for((long long)NB * N), 256, 0, st>>>(N, NB, Xc + (size_t)m * N, rs,
 				                                                            (long long)NL + 1, -1.0);
 				launch_count++;
 				gemm(gargs<T>((int)NL, N, N, NB, Xc, per_item(rs), (int)NL, iBm, per_item(nn), N, Xu,
 				              per_item(rs), (int)NL, sg));
-				GemmArgs<T> gw = gargs<T>((int)NL, N, N, 2 * NB, Xc, Addr{0, rs, NB}, (int)NL, iBm,
-				                          Addr{0, nn, NB}, N, Xw, per_item(rs), (int)NL, sg, zero<T>(), GM_A_DD);
+				GemmArgs<T> gw = gargs<T>((int)NL, N, N, NB, Xc, per_item(rs), (int)NL, iBm, per_item(nn), N,
+				                          Xw, per_item(rs), (int)NL, sg, zero<T>(), GM_A_DD);
 				gw.d = k.w.p; gw.dinv = k.ones.p; gw.aD = per_item((long long)NL);
 				gemm(gw);
-				// Y_m = Gst(m, .) W Gst(., m+1) of both observables
-				gemm(gargs<T>(N, N, (int)NL, 2 * NB, R0, Addr{0, rs, NB}, N, Xw, per_item(rs), (int)NL, k.Y.p,
-				              per_item(nn), N));
+				// Y_m = Gst(m, .) W Gst(., m+1) of both observables: items
+				// [0, NB) take the plain column, [NB, 2 NB) the weighted one
+				gemm(gargs<T>(N, N, (int)NL, 2 * NB, R0, Addr{0, rs, NB}, N, Xu, Addr{(long long)(Xw - Xu), rs, NB},
+				              (int)NL, k.Y.p, per_item(nn), N, a_obs));
 				k_yacc<T><<<grid_for(2LL * NB * nn), 256, 0, st>>>(N, L, NB, 2 * NB, m, k.Y.p, dv.p, k.Yh.p);
 				launch_count++;
 				// row m+1

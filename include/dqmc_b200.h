@@ -212,7 +212,7 @@ int dqmc_engine_logdet_grad(dqmc_engine *e, double *logdet, void *S);
  * unequal-time Green's functions of the chain rotated by s slices
  * (src/greens.c:247-494) give row and column s of O^-1, and one B_m or
  * B_m^-1 product per slice gives the rows and columns in between.  Device
- * work per chain and spin: 11 N^2 L nums (the unequal-time stacks and the
+ * work per chain and spin: 10 N^2 L nums (the unequal-time stacks and the
  * rows and columns), kept for the next call.  DQMC_OBS_GRAD=dense, and the
  * sizes the unequal-time kernels do not take (N above 160 real / 112
  * complex), invert the whole N L x N L matrix instead: 2 (N L)^2 nums. */
