@@ -284,6 +284,63 @@ def cpu_procs():
     return max(1, (os.cpu_count() or 2) // 2)
 
 
+def ragged_reference_rate(n_proc, sweeps):
+    """Aggregate chain-sweeps/s of the reference C build on a bounded sample
+    of the ragged mix: n_proc chains spread evenly over the 64 (the same
+    generator and seed as the GPU line), one dqmc_1_r process each (2
+    OpenMP threads, OpenBLAS 1 thread), `sweeps` sweeps each.  The rate is
+    the sum over the processes of sweeps / own wall time: the steady rate of
+    independent processes that each keep running chains of their size.  The
+    files take the reference generator's layout (a params file per chain,
+    linked)."""
+    from dqmc_b200 import simfile
+    exe = os.path.join(ROOT, "oracle", "_ref", "dqmc_1_r")
+    if not os.path.exists(exe):
+        raise RuntimeError(f"reference build missing: {exe}")
+    dicts, _ = _ragged64(sweeps)
+    step = max(1, len(dicts) // n_proc)
+    dicts = dicts[::step][:n_proc]
+    tmp = tempfile.mkdtemp()
+    cwd = os.getcwd()
+    os.chdir(tmp)
+    try:
+        paths = []
+        for c, d in enumerate(dicts):
+            rel = f"r{c}.h5.params"
+            simfile.write(rel, {k: v for k, v in d.items() if k.startswith(("metadata/", "params/"))})
+            sim = {k: v for k, v in d.items() if not k.startswith(("metadata/", "params/"))}
+            sim["params_file"] = rel
+            sim["metadata"] = simfile.Link(rel)
+            sim["params"] = simfile.Link(rel)
+            simfile.write(f"r{c}.h5", sim)
+            paths.append(f"r{c}.h5")
+        env = dict(os.environ, OPENBLAS_NUM_THREADS="1", OMP_NUM_THREADS="2")
+        t0 = time.perf_counter()
+        procs = [subprocess.Popen([exe, "-b", "-l", f"{p}.log", p], env=env,
+                                  stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+                 for p in paths]
+        ends = [None] * len(procs)
+        while any(e is None for e in ends):
+            for i, p in enumerate(procs):
+                if ends[i] is None and p.poll() is not None:
+                    ends[i] = time.perf_counter() - t0
+            time.sleep(0.005)
+        t = max(ends)
+        rcs = [p.returncode for p in procs]
+        if any(rcs):
+            raise RuntimeError(f"reference runs failed: {rcs}")
+        sides = sorted({int(round(float(np.sqrt(int(np.asarray(d["params/N"]).reshape(-1)[0])))))
+                        for d in dicts})
+    finally:
+        os.chdir(cwd)
+        shutil.rmtree(tmp, ignore_errors=True)
+    n = len(paths)
+    sample = (f"{n} chains spread over the ragged mix (sides {sides}), one process of the "
+              f"reference dqmc_1_r each x {sweeps} sweeps (2 OpenMP threads, OpenBLAS 1 "
+              f"thread), {min(ends):.1f}-{t:.1f} s per process; rate = sum of sweeps / own time")
+    return sum(sweeps / e for e in ends), t, sample
+
+
 def ref_sample(wl, n_proc, sweeps, t):
     cplx = wl["cfg"].get("nflux", 0) != 0
     c = wl["cfg"]
@@ -305,6 +362,21 @@ def run_reference_arm(args, rank, world):
             "config": {"workload": GRAD_DESC, "cpu": True}, "cpu_baseline": from_grad,
             "e2e": {"value": from_grad["value"], "unit": "grad evals/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}))
+        return
+    if args.workload == "ragged64":
+        n_proc = cpu_procs()
+        sweeps = max(1, args.steps)
+        rate, t, sample = ragged_reference_rate(n_proc, sweeps)
+        print(json.dumps({
+            "metric": METRIC, "value": rate, "unit": METRIC, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / sweeps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": _ragged64(1)[1], "chains": n_proc, "cpu": True},
+            "cpu_baseline": {"value": rate, "unit": METRIC, "cores": n_proc * 2,
+                             "kind": "reference", "sample": sample},
+            "e2e": {"value": rate, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }))
         return
     wl = WORKLOADS.get(args.workload, WORKLOADS["batch256"])
     n_proc = cpu_procs()
@@ -599,6 +671,12 @@ def run_ragged(args, rank, world, local):
     forms = {str(n): f for n, f in rb.update.items()}
     lanes = {str(g): n for g, n in rb.lanes.items()}
     rb.close()
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        n_proc = cpu_procs()
+        rate, _, sample = ragged_reference_rate(n_proc, 3)
+        cpu = {"value": rate, "unit": METRIC, "cores": n_proc * 2, "kind": "reference",
+               "sample": sample}
     if rank == 0:
         print(json.dumps({
             "metric": METRIC, "value": len(sims) * args.steps * world / t_max, "unit": METRIC,
@@ -611,7 +689,7 @@ def run_ragged(args, rank, world, local):
                        "timing": "CUDA events on the batch stream around the graph launches "
                                  "(one per sweep of all groups)"},
             "gpu_launches": launches, "e2e": e2e, "roofline": rl,
-            "clocks": clk.summary(), "cpu_baseline": None,
+            "clocks": clk.summary(), "cpu_baseline": cpu,
         }))
 
 
