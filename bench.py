@@ -289,10 +289,11 @@ def ragged_reference_rate(n_proc, sweeps):
     of the ragged mix: n_proc chains spread evenly over the 64 (the same
     generator and seed as the GPU line), one dqmc_1_r process each (2
     OpenMP threads, OpenBLAS 1 thread), `sweeps` sweeps each.  The rate is
-    the sum over the processes of sweeps / own wall time: the steady rate of
-    independent processes that each keep running chains of their size.  The
-    files take the reference generator's layout (a params file per chain,
-    linked)."""
+    that of a farm of these n_proc processes working through the mix: n_proc
+    over the mean time a process spends on one chain-sweep (each process's
+    wall time over its sweeps), so large and small chains weigh by their
+    cost.  The files take the reference generator's layout (a params file
+    per chain, linked)."""
     from dqmc_b200 import simfile
     exe = os.path.join(ROOT, "oracle", "_ref", "dqmc_1_r")
     if not os.path.exists(exe):
@@ -337,8 +338,9 @@ def ragged_reference_rate(n_proc, sweeps):
     n = len(paths)
     sample = (f"{n} chains spread over the ragged mix (sides {sides}), one process of the "
               f"reference dqmc_1_r each x {sweeps} sweeps (2 OpenMP threads, OpenBLAS 1 "
-              f"thread), {min(ends):.1f}-{t:.1f} s per process; rate = sum of sweeps / own time")
-    return sum(sweeps / e for e in ends), t, sample
+              f"thread), {min(ends):.1f}-{t:.1f} s per process; rate = processes / mean "
+              f"seconds per chain-sweep")
+    return n * sweeps / (sum(ends) / n), t, sample
 
 
 def ref_sample(wl, n_proc, sweeps, t):
