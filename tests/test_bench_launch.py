@@ -19,3 +19,26 @@ def test_gpus_flag_spawns_ranks():
     assert p.returncode == 0, p.stderr[-2000:]
     lines = [json.loads(x) for x in p.stdout.splitlines() if x.startswith("{")]
     assert lines == [{"n_gpus": 2, "max_rank": 1.0}]
+
+
+def test_reference_arm_times_the_ragged_mix():
+    """`--impl reference --workload ragged64` runs the reference build on
+    chains of the ragged mix (not the 256-chain model) and prints one line
+    with its rate, the CPU baseline and an e2e of zero copies."""
+    import pytest
+    if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "dqmc_1_r")):
+        pytest.skip("reference build not present")
+    env = {k: v for k, v in os.environ.items()
+           if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK", "MASTER_ADDR", "MASTER_PORT")}
+    env["CUDA_VISIBLE_DEVICES"] = ""
+    p = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
+                        "--workload", "ragged64", "--steps", "1", "--warmup", "0"],
+                       env=env, capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr[-2000:]
+    lines = [json.loads(x) for x in p.stdout.splitlines() if x.startswith("{")]
+    assert len(lines) == 1
+    d = lines[0]
+    assert d["impl"] == "reference" and d["value"] > 0
+    assert d["config"]["workload"].startswith("64 ragged chains")
+    assert "ragged mix" in d["cpu_baseline"]["sample"]
+    assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["value"] == d["value"]
