@@ -91,6 +91,11 @@ ROOFLINE_KERNELS = {
 # items of a launch; other workloads report null
 TRAFFIC_PER_ITEM = {"batch256": {"gemm": 172580, "qr_presort": 168068, "qr_pivot": 166916,
                                  "recombine": 333636, "update": 170852}}
+# the reference build's FLOPs per chain-sweep of each single-model workload,
+# counted call by call with LAPACK-standard counts (python oracle/flop_tally.py
+# after make -C oracle tally; averaged over an unequal-time cycle)
+REF_FLOPS_PER_CHAIN_SWEEP = {"batch256": 8308315008.0, "c1": 4082880.0,
+                             "uneq8x8": 700769877.3, "complex64": 14984803733.3}
 
 T0 = time.time()
 
@@ -458,10 +463,11 @@ def profile_mix(eng, period_uneqlt):
     return {k: tuple((1 - w) * a + w * b for a, b in zip(prof[k], ue[k])) for k in prof}
 
 
-def roofline(prof, items, workload, peak, ms_per_step):
+def roofline(prof, items, workload, peak, ms_per_step, chains=None):
     """The dominant launch class by event time among those with counted
     FLOPs: its FLOPs over its time against the FP64 DGEMM peak, and the
-    whole sweep's FLOPs over the timed sweep."""
+    whole sweep's FLOPs over the timed sweep, by the engine's count and (for
+    `chains` chains of a workload with a tally) by the reference build's."""
     cls = [k for k in ROOFLINE_KERNELS if prof[k][0] > 0 and prof[k][2] > 0]
     dom = max(cls, key=lambda k: prof[k][0])
     d_ms, d_n, d_fl, _ = prof[dom]
@@ -469,7 +475,7 @@ def roofline(prof, items, workload, peak, ms_per_step):
     traffic = TRAFFIC_PER_ITEM.get(workload, {}).get(dom)
     sweep_fl = sum(prof[k][2] for k in ROOFLINE_KERNELS)
     sweep_tf = sweep_fl / (ms_per_step / 1e3) / 1e12
-    return {"bound": "tensor", "kernel": ROOFLINE_KERNELS[dom], "class": dom,
+    out = {"bound": "tensor", "kernel": ROOFLINE_KERNELS[dom], "class": dom,
             "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
             "frac": achieved / peak if peak else None,
             "traffic": traffic * items if traffic else None,
@@ -484,6 +490,15 @@ def roofline(prof, items, workload, peak, ms_per_step):
             "sweep": {"flops": sweep_fl, "achieved": sweep_tf,
                       "frac": sweep_tf / peak if peak else None,
                       "note": "counted FLOPs of every class over the timed ms_per_step"}}
+    ref = REF_FLOPS_PER_CHAIN_SWEEP.get(workload)
+    if ref and chains:
+        ref_tf = ref * chains / (ms_per_step / 1e3) / 1e12
+        out["sweep"].update({
+            "reference_flops": ref * chains, "reference_achieved": ref_tf,
+            "reference_frac": ref_tf / peak if peak else None,
+            "reference_note": "the reference build's LAPACK-standard FLOPs per chain-sweep "
+                              "(oracle/flop_tally.py) times the chains, over ms_per_step"})
+    return out
 
 
 def e2e_rate(engs, steps, world, sweep_all):
@@ -581,7 +596,7 @@ def run_engine_workload(args, rank, world, local):
     prof, items = profile_one_lane(sims, local, pu)
     log("profile sweep done")
     peak = fp64_peak()
-    rl = roofline(prof, items, args.workload, peak, 1e3 * t_max / args.steps)
+    rl = roofline(prof, items, args.workload, peak, 1e3 * t_max / args.steps, chains=nch)
 
     plain = None
     if args.workload == "batch256":

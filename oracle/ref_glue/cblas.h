@@ -12,12 +12,22 @@ enum CBLAS_UPLO { CblasUpper = 121, CblasLower = 122 };
 enum CBLAS_DIAG { CblasNonUnit = 131, CblasUnit = 132 };
 enum CBLAS_SIDE { CblasLeft = 141, CblasRight = 142 };
 
+#ifdef DQ_FLOP_TALLY
+/* the tally variant: counting wrappers (flop_tally.c) in front of OpenBLAS */
+#define cblas_dgemm dq_tally_dgemm
+#define cblas_dgemv dq_tally_dgemv
+#define cblas_dtrmm dq_tally_dtrmm
+#define cblas_zgemm dq_tally_zgemm
+#define cblas_zgemv dq_tally_zgemv
+#define cblas_ztrmm dq_tally_ztrmm
+#else
 #define cblas_dgemm scipy_cblas_dgemm
 #define cblas_dgemv scipy_cblas_dgemv
 #define cblas_dtrmm scipy_cblas_dtrmm
 #define cblas_zgemm scipy_cblas_zgemm
 #define cblas_zgemv scipy_cblas_zgemv
 #define cblas_ztrmm scipy_cblas_ztrmm
+#endif
 
 void cblas_dgemm(enum CBLAS_ORDER, enum CBLAS_TRANSPOSE, enum CBLAS_TRANSPOSE,
 		int m, int n, int k, double alpha, const double *a, int lda,

@@ -35,6 +35,53 @@ void scipy_zunmqr_(const char *, const char *, const int *, const int *, const i
 void scipy_ztrtri_(const char *, const char *, const int *, void *, const int *, int *,
 		size_t, size_t);
 
+#ifdef DQ_FLOP_TALLY
+void dq_tally_dgetrf(const int *, const int *, double *, const int *, int *, int *);
+void dq_tally_dgetri(const int *, double *, const int *, const int *, double *, const int *, int *);
+void dq_tally_dgetrs(const char *, const int *, const int *, const double *, const int *,
+		const int *, double *, const int *, int *, size_t);
+void dq_tally_dgeqp3(const int *, const int *, double *, const int *, int *, double *,
+		double *, const int *, int *);
+void dq_tally_dgeqrf(const int *, const int *, double *, const int *, double *, double *,
+		const int *, int *);
+void dq_tally_dormqr(const char *, const char *, const int *, const int *, const int *,
+		const double *, const int *, const double *, double *, const int *,
+		double *, const int *, int *, size_t, size_t);
+void dq_tally_dtrtri(const char *, const char *, const int *, double *, const int *, int *,
+		size_t, size_t);
+
+void dq_tally_zgetrf(const int *, const int *, void *, const int *, int *, int *);
+void dq_tally_zgetri(const int *, void *, const int *, const int *, void *, const int *, int *);
+void dq_tally_zgetrs(const char *, const int *, const int *, const void *, const int *,
+		const int *, void *, const int *, int *, size_t);
+void dq_tally_zgeqp3(const int *, const int *, void *, const int *, int *, void *,
+		void *, const int *, double *, int *);
+void dq_tally_zgeqrf(const int *, const int *, void *, const int *, void *, void *,
+		const int *, int *);
+void dq_tally_zunmqr(const char *, const char *, const int *, const int *, const int *,
+		const void *, const int *, const void *, void *, const int *,
+		void *, const int *, int *, size_t, size_t);
+void dq_tally_ztrtri(const char *, const char *, const int *, void *, const int *, int *,
+		size_t, size_t);
+#endif
+
+#ifdef DQ_FLOP_TALLY
+/* the tally variant: counting wrappers (flop_tally.c) in front of OpenBLAS */
+#define LAPACK_dgetrf(...) dq_tally_dgetrf(__VA_ARGS__)
+#define LAPACK_dgetri(...) dq_tally_dgetri(__VA_ARGS__)
+#define LAPACK_dgetrs(...) dq_tally_dgetrs(__VA_ARGS__, 1)
+#define LAPACK_dgeqp3(...) dq_tally_dgeqp3(__VA_ARGS__)
+#define LAPACK_dgeqrf(...) dq_tally_dgeqrf(__VA_ARGS__)
+#define LAPACK_dormqr(...) dq_tally_dormqr(__VA_ARGS__, 1, 1)
+#define LAPACK_dtrtri(...) dq_tally_dtrtri(__VA_ARGS__, 1, 1)
+#define LAPACK_zgetrf(...) dq_tally_zgetrf(__VA_ARGS__)
+#define LAPACK_zgetri(...) dq_tally_zgetri(__VA_ARGS__)
+#define LAPACK_zgetrs(...) dq_tally_zgetrs(__VA_ARGS__, 1)
+#define LAPACK_zgeqp3(...) dq_tally_zgeqp3(__VA_ARGS__)
+#define LAPACK_zgeqrf(...) dq_tally_zgeqrf(__VA_ARGS__)
+#define LAPACK_zunmqr(...) dq_tally_zunmqr(__VA_ARGS__, 1, 1)
+#define LAPACK_ztrtri(...) dq_tally_ztrtri(__VA_ARGS__, 1, 1)
+#else
 #define LAPACK_dgetrf(...) scipy_dgetrf_(__VA_ARGS__)
 #define LAPACK_dgetri(...) scipy_dgetri_(__VA_ARGS__)
 #define LAPACK_dgetrs(...) scipy_dgetrs_(__VA_ARGS__, 1)
@@ -49,3 +96,4 @@ void scipy_ztrtri_(const char *, const char *, const int *, void *, const int *,
 #define LAPACK_zgeqrf(...) scipy_zgeqrf_(__VA_ARGS__)
 #define LAPACK_zunmqr(...) scipy_zunmqr_(__VA_ARGS__, 1, 1)
 #define LAPACK_ztrtri(...) scipy_ztrtri_(__VA_ARGS__, 1, 1)
+#endif

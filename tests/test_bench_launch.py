@@ -42,3 +42,23 @@ def test_reference_arm_times_the_ragged_mix():
     assert d["config"]["workload"].startswith("64 ragged chains")
     assert "ragged mix" in d["cpu_baseline"]["sample"]
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["value"] == d["value"]
+
+
+def test_roofline_carries_the_reference_flop_tally():
+    """bench.roofline on a synthetic per-class profile: the dominant class,
+    the engine-counted sweep fraction, and for a workload with a reference
+    tally the same step measured in the reference build's FLOPs."""
+    sys.path.insert(0, ROOT)
+    import bench
+    names = ["gemm", "update", "qr_pivot", "uneqlt_g", "meas", "qr_presort", "recombine"]
+    prof = {k: (0.0, 0.0, 0.0, 0.0) for k in names}
+    prof["gemm"] = (50.0, 800.0, 1.2e12, 0.0)
+    prof["qr_presort"] = (60.0, 60.0, 0.3e12, 0.0)
+    rl = bench.roofline(prof, 512, "batch256", 35.0, 200.0, chains=256)
+    assert rl["class"] == "qr_presort" and abs(rl["achieved"] - 5.0) < 1e-9
+    assert abs(rl["sweep"]["achieved"] - 7.5) < 1e-9
+    ref = bench.REF_FLOPS_PER_CHAIN_SWEEP["batch256"] * 256 / 0.2 / 1e12
+    assert abs(rl["sweep"]["reference_achieved"] - ref) < 1e-9
+    assert abs(rl["sweep"]["reference_frac"] - ref / 35.0) < 1e-12
+    rl2 = bench.roofline(prof, 128, "ragged64", 35.0, 200.0)
+    assert "reference_flops" not in rl2["sweep"]
