@@ -9,6 +9,7 @@
   (oracle/_ref, outputs committed as ref_out.npz) on the golden cases.
 """
 import ctypes as C
+import json
 import os
 import shutil
 
@@ -85,3 +86,27 @@ def test_kagome_exact_g_fixture(golden, tmp_path):
     assert np.array_equal(o.hs.reshape(o.L, o.N), z["hs"])
     err = max(np.max(np.abs(gu - z["gu"])), np.max(np.abs(gd - z["gd"])))
     assert 1e-10 < err < 1e-8
+
+
+def test_flop_tally_of_the_reference_build():
+    """oracle/flop_tally.py on the c1 model (4x4, L = 40, n_matmul = 5,
+    n_delay = 8): the reference build's BLAS / LAPACK calls of one sweep,
+    counted with LAPACK-standard formulas, land near the analytic estimate
+    (wraps 4(L-F), mul_seq 2(L-F), calc_eq_g F(3.2F + 5) and the update's
+    flushes and panel products, in units of N^3 per spin), and the count is
+    deterministic."""
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    if not os.path.exists(os.path.join(root, "oracle", "_ref", "dqmc_1_r_tally")):
+        pytest.skip("tally build not present (make -C oracle tally)")
+    runs = []
+    for _ in range(2):
+        p = subprocess.run([sys.executable, os.path.join(root, "oracle", "flop_tally.py"), "c1"],
+                           capture_output=True, text=True, timeout=300)
+        assert p.returncode == 0, p.stderr[-2000:]
+        runs.append(json.loads(p.stdout.strip().splitlines()[-1])["c1"])
+    assert runs[0] == runs[1]
+    N, L, F = 16, 40, 8
+    estimate = 2 * N ** 3 * (4 * (L - F) + 2 * (L - F) + F * (3.2 * F + 5))
+    assert 0.5 * estimate < runs[0] < 2.0 * estimate, (runs[0], estimate)
